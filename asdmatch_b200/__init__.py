@@ -1,0 +1,404 @@
+"""ASDMatch-B200: the matching and counting path of ASDMatch on the B200.
+
+A thin ctypes binding over ``libasdm_b200.so`` (C ABI in ``include/asdm.h``).
+Names follow the reference's own interface so code written against it reads
+the same:
+
+* :func:`load_graph_from_text_file`  — ``Graph::loadGraphFromTextFile`` (relation/graph.cpp:68-148)
+* :class:`CandidateSpace`            — ``CandidateSpace`` + ``buildCandCFL`` (relation/candidate_space.cpp)
+* :func:`leapfrog_join`              — ``ComputeSetIntersection::LeapfrogJoin`` (utility/compute_set_intersection.cpp:193-233)
+* :func:`adaptive_share_join`        — ``adaptiveShareJoin`` with the ALL_LEVEL / LOCAL_COUNT /
+  COLLECT_RESULT outputs (matching/adaptive.cpp:1179-2279)
+
+All compute runs on the GPU; there is no CPU fallback.  If the shared library
+is missing, importing this package raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libasdm_b200.so")
+BIN_DIR = os.path.join(_PKG, "bin")
+
+OK, ERR_INVALID, ERR_IO, ERR_CUDA, ERR_OOM, ERR_OVERFLOW, ERR_TIMEOUT, ERR_CAPACITY, ERR_INTERNAL = range(9)
+MODE_COUNT, MODE_LOCAL, MODE_EMBED = 0, 1, 2
+
+_ERR_NAMES = {ERR_INVALID: "invalid", ERR_IO: "io", ERR_CUDA: "cuda", ERR_OOM: "oom", ERR_OVERFLOW: "overflow",
+              ERR_TIMEOUT: "timeout", ERR_CAPACITY: "capacity", ERR_INTERNAL: "internal"}
+
+
+class AsdmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s (%s)" % (msg, _ERR_NAMES.get(code, code)))
+        self.code = code
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("libasdm_b200.so not built: run `python -m asdmatch_b200.build` (%s)" % LIB_PATH)
+_lib = C.CDLL(LIB_PATH)
+
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_vp = C.c_void_p
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("budget_bytes", C.c_uint64), ("time_limit_s", C.c_double),
+                ("local_counts", _u64p), ("embeddings", _u32p), ("emb_capacity", C.c_uint64)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("emb_rows", C.c_uint64), ("intersections", C.c_uint64),
+                ("list_bytes", C.c_uint64), ("tasks", C.c_uint64), ("kernel_ms", C.c_double)]
+
+
+def _sig(name, res, args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+_last_error = _sig("asdm_last_error", C.c_char_p, [])
+_version = _sig("asdm_version", C.c_char_p, [])
+_hg_load = _sig("asdm_host_graph_load", C.c_int, [C.c_char_p, C.POINTER(_vp)])
+_hg_from_edges = _sig("asdm_host_graph_from_edges", C.c_int, [C.c_uint32, _u32p, C.c_uint64, _u32p, C.POINTER(_vp)])
+_hg_info = _sig("asdm_host_graph_info", C.c_int, [_vp, _u32p, _u64p, _u32p])
+_hg_csr = _sig("asdm_host_graph_csr", C.c_int, [_vp, C.POINTER(_u32p), C.POINTER(_u32p), C.POINTER(_u32p)])
+_hg_write = _sig("asdm_host_graph_write", C.c_int, [_vp, C.c_char_p])
+_hg_free = _sig("asdm_host_graph_free", None, [_vp])
+_gen_cl = _sig("asdm_gen_chung_lu", C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_uint32, C.c_double, C.c_uint64,
+                                              C.POINTER(_vp)])
+_gen_q = _sig("asdm_gen_query", C.c_int, [_vp, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_vp)])
+_g_upload = _sig("asdm_graph_upload", C.c_int, [_u32p, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_uint32,
+                                                C.POINTER(_vp)])
+_g_free = _sig("asdm_graph_free", C.c_int, [_vp])
+_cs_build = _sig("asdm_candidate_space", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(_vp),
+                                                   C.POINTER(C.c_int)])
+_cs_sizes = _sig("asdm_cs_sizes", C.c_int, [_vp, _u32p])
+_cs_read = _sig("asdm_cs_read", C.c_int, [_vp, C.c_uint32, _u32p, C.c_uint32])
+_cs_read_edges = _sig("asdm_cs_read_edges", C.c_int, [_vp, C.c_uint32, C.c_uint32, _u32p, _u32p, C.c_uint64, _u64p])
+_cs_free = _sig("asdm_cs_free", C.c_int, [_vp])
+_intersect = _sig("asdm_intersect_batch", C.c_int, [_u32p, _u64p, C.c_uint64, _u32p, C.c_uint32, _u64p, _u32p, _u32p])
+_plan_create = _sig("asdm_plan_create", C.c_int, [_vp, _u32p, C.POINTER(_vp)])
+_plan_order = _sig("asdm_plan_order", C.c_int, [_vp, _u32p])
+_plan_free = _sig("asdm_plan_free", C.c_int, [_vp])
+_run_plan = _sig("asdm_run_plan", C.c_int, [_vp, _vp, C.POINTER(RunOpts), C.POINTER(RunStats)])
+_count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(RunOpts),
+                                                  C.POINTER(RunStats)])
+_run_batch = _sig("asdm_run_batch", C.c_int, [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p,
+                                              C.c_double, _u64p, C.POINTER(C.c_int)])
+
+
+def _check(rc: int, what: str = ""):
+    if rc != OK:
+        msg = (_last_error() or b"").decode(errors="replace")
+        raise AsdmError(rc, ("%s: %s" % (what, msg)) if what else msg)
+
+
+def _ptr(a: np.ndarray, ty=_u32p):
+    return a.ctypes.data_as(ty)
+
+
+def version() -> str:
+    return _version().decode()
+
+
+class HostGraph:
+    """Host CSR in the reference's layout: neighbours sorted by (label, id)."""
+
+    def __init__(self, handle):
+        self._h = _vp(handle)
+        n, m2, nl = C.c_uint32(), C.c_uint64(), C.c_uint32()
+        _check(_hg_info(self._h, C.byref(n), C.byref(m2), C.byref(nl)))
+        self.n, self.m2, self.nlabels = n.value, m2.value, nl.value
+        o, b, l = _u32p(), _u32p(), _u32p()
+        _check(_hg_csr(self._h, C.byref(o), C.byref(b), C.byref(l)))
+        # zero-copy views, valid while this object lives
+        self.offsets = np.ctypeslib.as_array(o, shape=(self.n + 1,)) if self.n + 1 else np.zeros(1, np.uint32)
+        self.nbrs = np.ctypeslib.as_array(b, shape=(self.m2,)) if self.m2 else np.zeros(0, np.uint32)
+        self.labels = np.ctypeslib.as_array(l, shape=(self.n,)) if self.n else np.zeros(0, np.uint32)
+
+    @classmethod
+    def load(cls, path: str) -> "HostGraph":
+        h = _vp()
+        _check(_hg_load(path.encode(), C.byref(h)), path)
+        return cls(h.value)
+
+    @classmethod
+    def from_edges(cls, n: int, labels: Sequence[int], edges) -> "HostGraph":
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        e = np.ascontiguousarray(np.asarray(edges, dtype=np.uint32).reshape(-1))
+        h = _vp()
+        _check(_hg_from_edges(n, _ptr(lab), len(e) // 2, _ptr(e), C.byref(h)), "from_edges")
+        return cls(h.value)
+
+    @classmethod
+    def chung_lu(cls, n: int, m: int, gamma: float, nlabels: int, zipf_s: float, seed: int) -> "HostGraph":
+        h = _vp()
+        _check(_gen_cl(n, m, gamma, nlabels, zipf_s, seed, C.byref(h)), "chung_lu")
+        return cls(h.value)
+
+    def random_walk_query(self, size: int, seed: int, density: int = 0) -> "HostGraph":
+        """density: 0 any, 1 dense (avg degree >= 3), 2 sparse (< 3)."""
+        h = _vp()
+        _check(_gen_q(self._h, size, density, seed, C.byref(h)), "query")
+        return HostGraph(h.value)
+
+    def write(self, path: str):
+        _check(_hg_write(self._h, path.encode()), path)
+
+    def degree(self, v: int) -> int:
+        return int(self.offsets[v + 1] - self.offsets[v])
+
+    def edges(self) -> np.ndarray:
+        src = np.repeat(np.arange(self.n, dtype=np.uint32), np.diff(self.offsets.astype(np.int64)))
+        keep = src < self.nbrs
+        return np.stack([src[keep], self.nbrs[keep]], axis=1)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _hg_free(h)
+            self._h = _vp()
+
+
+def load_graph_from_text_file(path: str) -> HostGraph:
+    """Graph::loadGraphFromTextFile (relation/graph.cpp:68-148)."""
+    return HostGraph.load(path)
+
+
+class DeviceGraph:
+    """Data graph resident in HBM (CSR + label-run index)."""
+
+    def __init__(self, g: HostGraph):
+        h = _vp()
+        _check(_g_upload(_ptr(g.offsets), _ptr(g.nbrs), _ptr(g.labels), g.n, g.m2, max(g.nlabels, 1), C.byref(h)),
+               "upload")
+        self._h = h
+        self.n = g.n
+        self.host = g
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            _g_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CandidateSpace:
+    """CFL candidate space on the device (CandidateSpace::buildCandCFL)."""
+
+    def __init__(self, dg: DeviceGraph, q: HostGraph):
+        h = _vp()
+        ne = C.c_int()
+        _check(_cs_build(dg._h, _ptr(q.offsets), _ptr(q.nbrs), _ptr(q.labels), q.n, C.byref(h), C.byref(ne)),
+               "candidate space")
+        self._h = h
+        self.q = q
+        self.dg = dg
+        self.nonempty = bool(ne.value)
+
+    def build_cand_cfl(self) -> bool:
+        """The reference's return value: False when some candidate set is empty."""
+        return self.nonempty
+
+    def sizes(self) -> np.ndarray:
+        out = np.zeros(self.q.n, np.uint32)
+        _check(_cs_sizes(self._h, _ptr(out)))
+        return out
+
+    def candidate_set(self, u: int) -> np.ndarray:
+        n = int(self.sizes()[u])
+        out = np.zeros(max(n, 1), np.uint32)
+        _check(_cs_read(self._h, u, _ptr(out), n))
+        return out[:n]
+
+    def candidate_edge(self, u: int, u2: int):
+        """(offsets, neighbour ids) of candidateEdge[u][v][u2] for v in C(u)."""
+        n = int(self.sizes()[u])
+        off = np.zeros(n + 1, np.uint32)
+        total = C.c_uint64()
+        # first call with capacity 0 only learns the size
+        rc = _cs_read_edges(self._h, u, u2, _ptr(off), None, 0, C.byref(total))
+        if rc not in (OK, ERR_CAPACITY):
+            _check(rc)
+        vals = np.zeros(max(total.value, 1), np.uint32)
+        _check(_cs_read_edges(self._h, u, u2, _ptr(off), _ptr(vals), total.value, C.byref(total)))
+        return off, vals[:total.value]
+
+    def write_to_stream(self) -> str:
+        """Text dump: 'C u n v...' lines, then CandidateSpace::writeToStream (candidate_space.cpp:489-505)."""
+        q = self.q
+        lines = []
+        for u in range(q.n):
+            c = self.candidate_set(u)
+            lines.append("C %d %d%s" % (u, len(c), "".join(" %d" % v for v in c)))
+        for u in range(q.n):
+            c = self.candidate_set(u)
+            for e in range(int(q.offsets[u]), int(q.offsets[u + 1])):
+                u2 = int(q.nbrs[e])
+                lines.append("# %d %d" % (u, u2))
+                off, vals = self.candidate_edge(u, u2)
+                for i, v in enumerate(c):
+                    for w in vals[off[i]:off[i + 1]]:
+                        lines.append("%d %d" % (v, w))
+        return "\n".join(lines) + "\n"
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            _cs_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    def __init__(self, cs: CandidateSpace, order: Optional[Sequence[int]] = None):
+        h = _vp()
+        o = None
+        if order is not None:
+            arr = np.ascontiguousarray(order, dtype=np.uint32)
+            o = _ptr(arr)
+        _check(_plan_create(cs._h, o, C.byref(h)), "plan")
+        self._h = h
+        self.n = cs.q.n
+
+    def order(self) -> List[int]:
+        out = np.zeros(self.n, np.uint32)
+        _check(_plan_order(self._h, _ptr(out)))
+        return out.tolist()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _plan_free(h)
+            self._h = None
+
+
+@dataclass
+class MatchResult:
+    count: int
+    local_counts: Optional[np.ndarray] = None   # |Vg| x |Vq| uint64
+    embeddings: Optional[np.ndarray] = None     # rows x |Vq| uint32, lexicographically sorted
+    intersections: int = 0
+    list_bytes: int = 0
+    tasks: int = 0
+    kernel_ms: float = 0.0
+    nonempty: bool = True
+
+
+def adaptive_share_join(cs: CandidateSpace, plan: Optional[Plan] = None, mode: int = MODE_COUNT,
+                        emb_capacity: int = 0, budget_bytes: int = 0, time_limit_s: float = 0.0) -> MatchResult:
+    """Exact enumeration of one query: count, local counts (MODE_LOCAL), embeddings (MODE_EMBED)."""
+    n = cs.q.n
+    opts = RunOpts()
+    opts.mode = mode
+    opts.budget_bytes = budget_bytes
+    opts.time_limit_s = time_limit_s
+    local = emb = None
+    if mode & MODE_LOCAL:
+        local = np.zeros((cs.dg.n, n), np.uint64)
+        opts.local_counts = _ptr(local, _u64p)
+    if mode & MODE_EMBED:
+        emb = np.zeros((max(emb_capacity, 1), n), np.uint32)
+        opts.embeddings = _ptr(emb)
+        opts.emb_capacity = emb_capacity
+    st = RunStats()
+    if cs.nonempty and plan is None:
+        plan = Plan(cs)
+    _check(_run_plan(cs._h, plan._h if plan is not None else None, C.byref(opts), C.byref(st)), "run")
+    if emb is not None:
+        emb = emb[:st.emb_rows]
+    return MatchResult(st.count, local, emb, st.intersections, st.list_bytes, st.tasks, st.kernel_ms, cs.nonempty)
+
+
+def match(dg: DeviceGraph, q: HostGraph, mode: int = MODE_COUNT, order: Optional[Sequence[int]] = None,
+          time_limit_s: float = 0.0) -> MatchResult:
+    """Candidate space + plan + enumeration for one query; embeddings sized by a counting pass."""
+    cs = CandidateSpace(dg, q)
+    try:
+        if not cs.nonempty:
+            local = np.zeros((dg.n, q.n), np.uint64) if mode & MODE_LOCAL else None
+            emb = np.zeros((0, q.n), np.uint32) if mode & MODE_EMBED else None
+            return MatchResult(0, local, emb, nonempty=False)
+        plan = Plan(cs, order)
+        cap = 0
+        if mode & MODE_EMBED:
+            cap = adaptive_share_join(cs, plan, MODE_COUNT, time_limit_s=time_limit_s).count
+        return adaptive_share_join(cs, plan, mode, emb_capacity=cap, time_limit_s=time_limit_s)
+    finally:
+        cs.close()
+
+
+def count_query(dg: DeviceGraph, q: HostGraph, time_limit_s: float = 0.0) -> MatchResult:
+    """One-call count (asdm_count_query)."""
+    opts = RunOpts()
+    opts.mode = MODE_COUNT
+    opts.time_limit_s = time_limit_s
+    st = RunStats()
+    _check(_count_query(dg._h, _ptr(q.offsets), _ptr(q.nbrs), _ptr(q.labels), q.n, C.byref(opts), C.byref(st)),
+           "count")
+    return MatchResult(st.count, intersections=st.intersections, list_bytes=st.list_bytes, tasks=st.tasks,
+                       kernel_ms=st.kernel_ms)
+
+
+def leapfrog_join(lists_per_set: Sequence[Sequence[np.ndarray]]) -> List[np.ndarray]:
+    """Batched k-way sorted intersection on the device (LeapfrogJoin)."""
+    vals, loff, first, ooff = [], [0], [0], [0]
+    for lists in lists_per_set:
+        mn = 0
+        for l in lists:
+            a = np.ascontiguousarray(l, dtype=np.uint32)
+            vals.append(a)
+            loff.append(loff[-1] + len(a))
+        if lists:
+            mn = min(len(l) for l in lists)
+        first.append(first[-1] + len(lists))
+        ooff.append(ooff[-1] + mn)
+    values = np.concatenate(vals) if vals else np.zeros(1, np.uint32)
+    if len(values) == 0:
+        values = np.zeros(1, np.uint32)
+    loff_a = np.asarray(loff, np.uint64)
+    first_a = np.asarray(first, np.uint32)
+    ooff_a = np.asarray(ooff, np.uint64)
+    out = np.zeros(max(int(ooff_a[-1]), 1), np.uint32)
+    cnt = np.zeros(max(len(lists_per_set), 1), np.uint32)
+    _check(_intersect(_ptr(values), _ptr(loff_a, _u64p), len(loff) - 1, _ptr(first_a), len(lists_per_set),
+                      _ptr(ooff_a, _u64p), _ptr(out), _ptr(cnt)), "intersect")
+    return [out[ooff[i]:ooff[i] + cnt[i]].copy() for i in range(len(lists_per_set))]
+
+
+def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):
+    """Counts for many queries against one resident graph; returns (counts, status)."""
+    nq = len(queries)
+    sizes = np.asarray([q.n for q in queries], np.uint32)
+    offs = np.concatenate([q.offsets for q in queries]).astype(np.uint32)
+    nbrs = np.concatenate([q.nbrs for q in queries] + [np.zeros(1, np.uint32)]).astype(np.uint32)
+    labs = np.concatenate([q.labels for q in queries]).astype(np.uint32)
+    ob = np.cumsum([0] + [q.n + 1 for q in queries[:-1]]).astype(np.uint64)
+    nb = np.cumsum([0] + [q.m2 for q in queries[:-1]]).astype(np.uint64)
+    lb = np.cumsum([0] + [q.n for q in queries[:-1]]).astype(np.uint64)
+    counts = np.zeros(nq, np.uint64)
+    status = np.zeros(nq, np.int32)
+    rc = _run_batch(dg._h, nq, _ptr(sizes), _ptr(ob, _u64p), _ptr(offs), _ptr(nb, _u64p), _ptr(nbrs),
+                    _ptr(lb, _u64p), _ptr(labs), time_limit_s, _ptr(counts, _u64p),
+                    status.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc == ERR_CUDA:
+        _check(rc, "batch")
+    return counts, status

@@ -1,0 +1,34 @@
+// Candidate space of one query on the device (the product of K1-K3).
+#pragma once
+
+#include "device.cuh"
+
+struct asdm_cs {
+    asdm_graph *g = nullptr;
+    asdm::QueryGraph q;
+    bool nonempty = false;
+    uint32_t root = 0;                     // CFL root (selectCFLRoot)
+    std::vector<uint32_t> bfs_order;       // CFL BFS order (buildCFLBFSTree)
+    std::vector<uint32_t> ncand;           // |C(u)|
+    std::vector<uint64_t> cand_base;       // C(u) = d_cand + cand_base[u], sorted vertex ids
+    uint32_t *d_cand = nullptr;
+    // Directed query edge e = q.off[u] + k (u -> q.nbr[e]): for the i-th
+    // candidate of u, the candidates of u2 adjacent to it are
+    // d_elist[elist_base[e] + off[i] .. elist_base[e] + off[i+1]) with
+    // off = d_eoff + eoff_base[e] (ncand[u] + 1 entries, relative to the edge),
+    // stored as ascending indices into C(u2).
+    std::vector<uint64_t> eoff_base;
+    std::vector<uint64_t> elist_base;
+    std::vector<uint64_t> etotal;          // entries per directed edge
+    uint32_t *d_eoff = nullptr;
+    uint32_t *d_elist = nullptr;
+    uint64_t build_bytes = 0;              // algorithmic bytes of K1-K3 (roofline)
+    float build_ms = 0.f;                  // device time of K1-K3
+};
+
+struct asdm_plan {
+    std::vector<uint32_t> order;                                   // level -> query vertex
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> back;  // level -> (earlier level j, edge u_j -> u_k)
+    std::vector<std::vector<uint32_t>> conf;                       // level -> earlier same-label, non-adjacent levels
+    double cost = 0.0;                                             // planner's estimate
+};

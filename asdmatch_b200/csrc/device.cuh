@@ -1,0 +1,124 @@
+// Device-side structures and helpers shared by the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "internal.h"
+
+#define ASDM_CUDA(call)                                                                              \
+    do {                                                                                             \
+        cudaError_t e__ = (call);                                                                    \
+        if (e__ != cudaSuccess)                                                                      \
+            return ::asdm::fail(e__ == cudaErrorMemoryAllocation ? ASDM_ERR_OOM : ASDM_ERR_CUDA,     \
+                                "%s: %s (%s:%d)", #call, cudaGetErrorString(e__), __FILE__, __LINE__); \
+    } while (0)
+
+#define ASDM_TRY(call)                   \
+    do {                                 \
+        int rc__ = (call);               \
+        if (rc__ != ASDM_OK) return rc__; \
+    } while (0)
+
+namespace asdm {
+
+// Device view of a data graph.  Adjacency lists are sorted by (label, id);
+// each list is split into label runs (run_lab ascending, run_start the first
+// edge of the run, the run ends at the next run's start or at off[v+1]).
+struct DevGraph {
+    uint32_t n = 0, nlabels = 0;
+    uint64_t m2 = 0, nruns = 0;
+    const uint32_t *off = nullptr;           // n + 1
+    const uint32_t *nbr = nullptr;           // m2
+    const uint32_t *lab = nullptr;           // n
+    const uint32_t *pos_in_label = nullptr;  // n: rank of v among vertices of its label
+    const uint32_t *vbl_off = nullptr;       // nlabels + 1
+    const uint32_t *vbl = nullptr;           // n: vertices grouped by label, id order
+    const uint32_t *run_off = nullptr;       // n + 1
+    const uint32_t *run_lab = nullptr;       // nruns
+    const uint32_t *run_start = nullptr;     // nruns
+};
+
+// [b, e) edge range of label l in w's adjacency (empty if w has no such neighbour).
+__device__ __forceinline__ void label_run(const DevGraph &g, uint32_t w, uint32_t l, uint32_t &b, uint32_t &e) {
+    uint32_t lo = g.run_off[w], hi = g.run_off[w + 1];
+    const uint32_t end = hi;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (g.run_lab[mid] < l) lo = mid + 1; else hi = mid;
+    }
+    if (lo < end && g.run_lab[lo] == l) {
+        b = g.run_start[lo];
+        e = (lo + 1 < end) ? g.run_start[lo + 1] : g.off[w + 1];
+    } else {
+        b = e = 0;
+    }
+}
+
+// First index in [lo, n) with a[i] >= x: exponential probe from lo, then
+// binary search (the leapfrog seek of the leapfrog-triejoin paper).
+__device__ __forceinline__ uint32_t gallop_lb(const uint32_t *__restrict__ a, uint32_t lo, uint32_t n, uint32_t x) {
+    if (lo >= n || a[lo] >= x) return lo;
+    uint32_t prev = lo, step = 1, hi = n;
+    while (true) {
+        uint32_t nxt = prev + step;
+        if (nxt >= n) { hi = n; break; }
+        if (a[nxt] >= x) { hi = nxt; break; }
+        prev = nxt;
+        step <<= 1;
+    }
+    lo = prev + 1;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Exclusive prefix sum of n values (uint32 or uint64 input) into uint64
+// output; out[n] receives the total when out has n + 1 slots and
+// with_total is set.  Temporary memory comes from the stream-ordered pool.
+int scan_exclusive_u32(const uint32_t *in, uint64_t *out, uint64_t n, bool with_total, cudaStream_t s);
+int scan_exclusive_u64(const uint64_t *in, uint64_t *out, uint64_t n, bool with_total, cudaStream_t s);
+
+// Stream-ordered allocation helpers with error reporting.
+template <typename T>
+int dalloc(T **p, uint64_t count, cudaStream_t s) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), s);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? ASDM_ERR_OOM : ASDM_ERR_CUDA, "device allocation of %llu bytes: %s",
+                    (unsigned long long)(count * sizeof(T)), cudaGetErrorString(e));
+    return ASDM_OK;
+}
+template <typename T>
+void dfree(T *&p, cudaStream_t s) {
+    if (p) cudaFreeAsync((void *)p, s);
+    p = nullptr;
+}
+
+int device_setup(int *device, int *num_sms);
+
+}  // namespace asdm
+
+struct asdm_graph {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    asdm::DevGraph d;
+    uint32_t *buf = nullptr;               // one allocation backing every DevGraph array
+    std::vector<uint32_t> h_vbl_off;       // host copy of the label offsets
+    uint32_t max_deg = 0;
+};

@@ -1,0 +1,642 @@
+// K4-K8: exact enumeration over the candidate space.
+//
+// One warp runs an iterative depth-first search over the matching order
+// (the attribute-at-a-time leapfrog join the reference executes in
+// adaptiveShareJoin/adaptiveGlobalJoin, matching/adaptive.cpp:115-330,
+// 1179-2279, and attributeOpen, :901-1000).  The candidates of level k are the
+// intersection of the candidate-edge lists of its earlier query neighbours
+// (ComputeSetIntersection::LeapfrogJoin, utility/compute_set_intersection.cpp:193-233),
+// computed lazily 32 elements at a time: the shortest list drives, each lane
+// takes one driver element and gallops in every other list from a shared
+// cursor (the leapfrog seek, :177-191), and __ballot_sync/__popc compact the
+// survivors into the level's stack slot.  Injectivity (the reference's
+// visited[] array) only has to be checked against earlier levels that carry
+// the same label and are not adjacent to level k; adjacent levels can never
+// hold the same vertex.  The last level is counted, not descended: its count
+// is |intersection| minus the same-label earlier vertices that lie in it,
+// which is exactly what traverse()'s numTuples(visited) shortcut computes for
+// ALL_LEVEL builds (matching/join.cpp:852-877).  LOCAL mode walks the last
+// level element by element to add one to local[v][u_last] per match and adds
+// the completion count to every prefix vertex (produceResult's
+// ++gLocalCount[φ(u)][u], matching/join.cpp:1035-1041); EMBED mode also
+// writes each match as a row indexed by query vertex (COLLECT_RESULT,
+// :1032-1034).  Root tasks are the candidate edges of the first two levels,
+// claimed with one atomicAdd each, so power-law hubs are split across warps.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <numeric>
+
+#include "cs.cuh"
+
+namespace asdm {
+
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p);
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr uint32_t kFull = 0xffffffffu;
+
+enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4 };
+enum : int { kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5, kCtrN = 8 };
+
+struct DLevel {
+    const uint32_t *cand;  // C(u)
+    uint32_t ncand;
+    uint32_t u;            // query vertex of this level
+    uint32_t nback;        // earlier adjacent levels
+    uint32_t back_first;   // first slot in the DBack array
+    uint32_t nconf;        // earlier same-label non-adjacent levels
+    uint32_t conf_first;
+};
+static_assert(sizeof(DLevel) == 32, "DLevel layout");
+
+struct DBack {
+    const uint32_t *off;   // candidate-edge offsets of (u_j -> u_k), indexed by idx[j]
+    const uint32_t *list;  // candidate-edge entries (indices into C(u_k))
+    uint32_t level;        // j
+    uint32_t pad;
+};
+static_assert(sizeof(DBack) == 24, "DBack layout");
+
+struct EnumArgs {
+    const DLevel *lv;
+    const DBack *bk;
+    const uint32_t *conf;
+    uint32_t n, nb, nc, nq;
+    uint64_t ntasks;
+    const uint32_t *off01;   // candidate-edge offsets of the level-0 -> level-1 edge
+    const uint32_t *list01;
+    uint32_t n0;
+    unsigned long long *ctr;
+    unsigned long long *local;  // |Vg| x nq, MODE_LOCAL
+    uint32_t *rows;             // row_cap x nq, MODE_EMBED
+    uint64_t row_cap;
+    uint64_t limit_ns;          // 0 = none; else per-warp wall-clock budget
+};
+
+__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 38 * n + 3 * nb; }
+
+__host__ __device__ inline uint32_t plan_words(uint32_t n, uint32_t nb, uint32_t nc) {
+    return (uint32_t)((n * sizeof(DLevel) + nb * sizeof(DBack)) / 4) + ((nc + 3) & ~3u);
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Largest i in [0, n0) with off[i] <= t, given off[0] <= t < off[n0]:
+// 32-way search, every lane probes one point per round.
+__device__ __forceinline__ uint32_t warp_find_row(const uint32_t *__restrict__ off, uint32_t n0, uint64_t t, uint32_t lane) {
+    uint32_t lo = 0, hi = n0;
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t p = lo + lane * step;
+        const bool pred = p < hi && off[p] <= t;
+        const uint32_t m = __ballot_sync(kFull, pred);
+        const uint32_t nlo = lo + (31 - __clz(m)) * step;
+        hi = min(hi, nlo + step);
+        lo = nlo;
+    }
+    const uint32_t p = lo + lane;
+    const uint32_t m = __ballot_sync(kFull, p < hi && off[p] <= t);
+    return lo + (31 - __clz(m));
+}
+
+template <uint32_t MODE>
+struct Warp {
+    const EnumArgs &a;
+    const DLevel *L;
+    const DBack *B;
+    const uint32_t *CF;
+    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *drv, *sstart, *slen, *scur;
+    uint32_t lane;
+    unsigned long long count = 0, inter = 0, elems = 0;
+    bool overflow = false;
+
+    __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln)
+        : a(args), L(l), B(b), CF(cf), lane(ln) {
+        const uint32_t n = a.n;
+        idx = w;
+        vid = idx + n;
+        buf = vid + n;
+        cnt = buf + 32 * n;
+        pos = cnt + n;
+        dpos = pos + n;
+        drv = dpos + n;
+        sstart = drv + n;
+        slen = sstart + a.nb;
+        scur = slen + a.nb;
+    }
+
+    __device__ __forceinline__ void add_count(unsigned long long c) {
+        const unsigned long long nc = count + c;
+        overflow |= nc < count;
+        count = nc;
+    }
+
+    // Loads the candidate-edge lists of level d's earlier neighbours into the
+    // level's slots and picks the shortest as driver.  Returns its length.
+    __device__ uint32_t setup(uint32_t d) {
+        const DLevel lv = L[d];
+        uint32_t s_len = 0xFFFFFFFFu;
+        if (lane < lv.nback) {
+            const DBack bk = B[lv.back_first + lane];
+            const uint32_t ij = idx[bk.level];
+            const uint32_t s0 = bk.off[ij];
+            s_len = bk.off[ij + 1] - s0;
+            sstart[lv.back_first + lane] = s0;
+            slen[lv.back_first + lane] = s_len;
+            scur[lv.back_first + lane] = 0;
+        }
+        uint32_t key = s_len, who = lane;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const uint32_t k2 = __shfl_xor_sync(kFull, key, o), w2 = __shfl_xor_sync(kFull, who, o);
+            if (k2 < key || (k2 == key && w2 < who)) { key = k2; who = w2; }
+        }
+        uint32_t tot = lane < lv.nback ? s_len : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(kFull, tot, o);
+        elems += tot;
+        inter += lv.nback >= 2;
+        if (lane == 0) {
+            drv[d] = who;
+            dpos[d] = 0;
+            cnt[d] = 0;
+            pos[d] = 0;
+        }
+        __syncwarp();
+        return key;
+    }
+
+    // Membership of x (this lane's driver element) in every non-driver list
+    // of level d, galloping from the shared cursors; advances the cursors.
+    __device__ __forceinline__ bool probe(const DLevel &lv, uint32_t dslot, uint32_t x, bool valid, uint32_t lastlane) {
+        bool ok = valid;
+        for (uint32_t s = 0; s < lv.nback; ++s) {
+            const uint32_t sl = lv.back_first + s;
+            if (sl == dslot) continue;
+            if (!__any_sync(kFull, ok)) break;
+            const uint32_t *lst = B[sl].list + sstart[sl];
+            const uint32_t len = slen[sl];
+            const uint32_t cur = scur[sl];
+            const uint32_t q = valid ? gallop_lb(lst, cur, len, x) : len;
+            ok = ok && q < len && lst[q] == x;
+            const uint32_t nc = __shfl_sync(kFull, q, lastlane);
+            __syncwarp();
+            if (lane == 0) scur[sl] = nc;
+            __syncwarp();
+        }
+        return ok;
+    }
+
+    __device__ __forceinline__ bool no_conflict(const DLevel &lv, uint32_t vx) {
+        bool ok = true;
+        for (uint32_t c = 0; c < lv.nconf; ++c) ok &= vx != vid[CF[lv.conf_first + c]];
+        return ok;
+    }
+
+    // Next 32 driver elements of a non-last level into its stack slot.
+    __device__ void fill_chunk(uint32_t d) {
+        const DLevel lv = L[d];
+        const uint32_t dslot = lv.back_first + drv[d];
+        const uint32_t *dl = B[dslot].list + sstart[dslot];
+        const uint32_t dlen = slen[dslot];
+        const uint32_t p0 = dpos[d];
+        const uint32_t p = p0 + lane;
+        const bool valid = p < dlen;
+        const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
+        const uint32_t lastlane = min(31u, dlen - 1 - p0);
+        bool ok = probe(lv, dslot, x, valid, lastlane);
+        if (lv.nconf && __any_sync(kFull, ok)) {
+            const uint32_t vx = ok ? lv.cand[x] : 0;
+            ok = ok && no_conflict(lv, vx);
+        }
+        const uint32_t mask = __ballot_sync(kFull, ok);
+        if (ok) buf[32 * d + __popc(mask & ((1u << lane) - 1))] = x;
+        __syncwarp();
+        if (lane == 0) {
+            cnt[d] = __popc(mask);
+            pos[d] = 0;
+            dpos[d] = p0 + 32;
+        }
+        __syncwarp();
+    }
+
+    __device__ void emit_rows(uint32_t d, uint32_t vx, bool ok, uint32_t mask) {
+        unsigned long long base = 0;
+        if (lane == 0 && mask) base = atomicAdd(&a.ctr[kCtrRows], (unsigned long long)__popc(mask));
+        base = __shfl_sync(kFull, base, 0);
+        if (ok) {
+            const unsigned long long r = base + __popc(mask & ((1u << lane) - 1));
+            if (r < a.row_cap) {
+                uint32_t *row = a.rows + r * a.nq;
+                for (uint32_t j = 0; j < d; ++j) row[L[j].u] = vid[j];
+                row[L[d].u] = vx;
+            } else {
+                atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagCapacity);
+            }
+        }
+    }
+
+    // The last level: count (and in LOCAL/EMBED modes, emit) its matches.
+    __device__ void leaf(uint32_t d) {
+        const DLevel lv = L[d];
+        const uint32_t dslot = lv.back_first + drv[d];
+        const uint32_t *dl = B[dslot].list + sstart[dslot];
+        const uint32_t dlen = slen[dslot];
+        unsigned long long total = 0;
+        if (MODE == ASDM_MODE_COUNT) {
+            if (lv.nback == 1) {
+                total = dlen;
+            } else {
+                for (uint32_t p0 = 0; p0 < dlen; p0 += 32) {
+                    const uint32_t p = p0 + lane;
+                    const bool valid = p < dlen;
+                    const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
+                    const bool ok = probe(lv, dslot, x, valid, min(31u, dlen - 1 - p0));
+                    total += __popc(__ballot_sync(kFull, ok));
+                }
+            }
+            if (lv.nconf && total) {
+                // same-label earlier vertices inside the intersection are not matches
+                bool present = false;
+                if (lane < lv.nconf) {
+                    const uint32_t v = vid[CF[lv.conf_first + lane]];
+                    const uint32_t y = lower_bound_u32(lv.cand, lv.ncand, v);
+                    present = y < lv.ncand && lv.cand[y] == v;
+                    for (uint32_t s = 0; present && s < lv.nback; ++s) {
+                        const uint32_t sl = lv.back_first + s;
+                        const uint32_t *lst = B[sl].list + sstart[sl];
+                        const uint32_t len = slen[sl];
+                        const uint32_t q = lower_bound_u32(lst, len, y);
+                        present = q < len && lst[q] == y;
+                    }
+                }
+                total -= __popc(__ballot_sync(kFull, present));
+            }
+        } else {
+            for (uint32_t p0 = 0; p0 < dlen; p0 += 32) {
+                const uint32_t p = p0 + lane;
+                const bool valid = p < dlen;
+                const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
+                bool ok = probe(lv, dslot, x, valid, min(31u, dlen - 1 - p0));
+                const uint32_t vx = ok ? lv.cand[x] : 0;
+                ok = ok && no_conflict(lv, vx);
+                const uint32_t mask = __ballot_sync(kFull, ok);
+                total += __popc(mask);
+                if ((MODE & ASDM_MODE_LOCAL) && ok) atomicAdd(&a.local[(unsigned long long)vx * a.nq + lv.u], 1ull);
+                if (MODE & ASDM_MODE_EMBED) emit_rows(d, vx, ok, mask);
+            }
+            if ((MODE & ASDM_MODE_LOCAL) && total && lane < d)
+                atomicAdd(&a.local[(unsigned long long)vid[lane] * a.nq + L[lane].u], total);
+        }
+        add_count(total);
+    }
+
+    // A full match at the last level when the query has one or two vertices.
+    __device__ void single(uint32_t d) {
+        add_count(1);
+        if (MODE & ASDM_MODE_LOCAL) {
+            if (lane <= d) atomicAdd(&a.local[(unsigned long long)vid[lane] * a.nq + L[lane].u], 1ull);
+        }
+        if (MODE & ASDM_MODE_EMBED) {
+            const uint32_t vx = vid[d];
+            emit_rows(d, vx, lane == 0, 1u);
+        }
+    }
+};
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    DLevel *L = reinterpret_cast<DLevel *>(sm);
+    DBack *B = reinterpret_cast<DBack *>(L + a.n);
+    uint32_t *CF = reinterpret_cast<uint32_t *>(B + a.nb);
+    {
+        const uint32_t *src_l = reinterpret_cast<const uint32_t *>(a.lv);
+        uint32_t *dst_l = reinterpret_cast<uint32_t *>(L);
+        for (uint32_t i = threadIdx.x; i < a.n * (uint32_t)(sizeof(DLevel) / 4); i += blockDim.x) dst_l[i] = src_l[i];
+        const uint32_t *src_b = reinterpret_cast<const uint32_t *>(a.bk);
+        uint32_t *dst_b = reinterpret_cast<uint32_t *>(B);
+        for (uint32_t i = threadIdx.x; i < a.nb * (uint32_t)(sizeof(DBack) / 4); i += blockDim.x) dst_b[i] = src_b[i];
+        for (uint32_t i = threadIdx.x; i < a.nc; i += blockDim.x) CF[i] = a.conf[i];
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *wmem = sm + plan_words(a.n, a.nb, a.nc) + warp * warp_words(a.n, a.nb);
+    Warp<MODE> W(a, L, B, CF, wmem, lane);
+    const uint32_t n = a.n;
+    volatile unsigned int *flags = reinterpret_cast<volatile unsigned int *>(&a.ctr[kCtrFlags]);
+    uint32_t iter = 0;
+    bool stop = false;
+    uint64_t deadline = 0;
+    if (a.limit_ns && lane == 0) deadline = globaltimer() + a.limit_ns;
+    while (!stop) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(&a.ctr[kCtrTask], 1ull);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= a.ntasks) break;
+        uint32_t i0, i1 = 0;
+        if (n == 1) {
+            i0 = (uint32_t)t;
+        } else {
+            i0 = warp_find_row(a.off01, a.n0, t, lane);
+            i1 = a.list01[t];
+        }
+        if (lane == 0) {
+            W.idx[0] = i0;
+            W.vid[0] = L[0].cand[i0];
+            if (n > 1) {
+                W.idx[1] = i1;
+                W.vid[1] = L[1].cand[i1];
+            }
+        }
+        __syncwarp();
+        if (n <= 2) {
+            W.single(n - 1);
+            continue;
+        }
+        uint32_t d = 2;
+        // enter level 2
+        {
+            const uint32_t len = W.setup(d);
+            if (d == n - 1) {
+                if (len) W.leaf(d);
+                d = 1;
+            } else if (len == 0) {
+                d = 1;
+            }
+        }
+        while (d >= 2) {
+            if ((++iter & 63u) == 0) {
+                uint32_t s = 0;
+                if (lane == 0) {
+                    s = *flags & (kFlagOverflow | kFlagTimeout);
+                    if (!s && deadline && globaltimer() > deadline) {
+                        atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagTimeout);
+                        s = kFlagTimeout;
+                    }
+                }
+                if (__shfl_sync(kFull, s, 0)) { stop = true; break; }
+            }
+            if (W.pos[d] < W.cnt[d]) {
+                const uint32_t x = W.buf[32 * d + W.pos[d]];
+                __syncwarp();
+                if (lane == 0) {
+                    W.pos[d] += 1;
+                    W.idx[d] = x;
+                    W.vid[d] = L[d].cand[x];
+                }
+                __syncwarp();
+                ++d;
+                const uint32_t len = W.setup(d);
+                if (d == n - 1) {
+                    if (len) W.leaf(d);
+                    --d;
+                } else if (len == 0) {
+                    --d;
+                }
+                continue;
+            }
+            if (W.dpos[d] < W.slen[L[d].back_first + W.drv[d]]) {
+                W.fill_chunk(d);
+                continue;
+            }
+            --d;
+        }
+    }
+    // flush per-warp totals
+    unsigned long long c = W.count, in = W.inter, el = W.elems;
+    if (lane == 0) {
+        const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], c);
+        if (W.overflow || old + c < old) atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagOverflow);
+        atomicAdd(&a.ctr[kCtrInter], in);
+        atomicAdd(&a.ctr[kCtrElems], el);
+    }
+}
+
+template <uint32_t MODE>
+int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
+    auto k = enum_kernel<MODE>;
+    ASDM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    ASDM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem));
+    if (per_sm <= 0) return fail(ASDM_ERR_INVALID, "query too large for one block's shared memory (%u bytes)", smem);
+    const uint64_t want = (a.ntasks + kWarps - 1) / kWarps;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)per_sm * num_sms, want));
+    k<<<grid, kThreads, smem, s>>>(a);
+    ASDM_CUDA(cudaGetLastError());
+    return ASDM_OK;
+}
+
+}  // namespace
+
+int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_run_stats &st) {
+    asdm_graph *G = cs.g;
+    cudaStream_t s = G->stream;
+    const QueryGraph &q = cs.q;
+    const uint32_t n = q.n;
+    const uint32_t mode = opt.mode & (ASDM_MODE_LOCAL | ASDM_MODE_EMBED);
+    st = asdm_run_stats{};
+    if (opt.local_counts && (mode & ASDM_MODE_LOCAL))
+        std::fill(opt.local_counts, opt.local_counts + (uint64_t)G->d.n * n, 0ull);
+    if (!cs.nonempty) return ASDM_OK;
+    // device plan
+    std::vector<DLevel> lv(n);
+    std::vector<DBack> bk;
+    std::vector<uint32_t> cf;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t u = plan.order[k];
+        lv[k].cand = cs.d_cand + cs.cand_base[u];
+        lv[k].ncand = cs.ncand[u];
+        lv[k].u = u;
+        lv[k].nback = (uint32_t)plan.back[k].size();
+        lv[k].back_first = (uint32_t)bk.size();
+        for (auto &jb : plan.back[k]) {
+            const uint32_t e = jb.second;
+            bk.push_back(DBack{cs.d_eoff + cs.eoff_base[e], cs.d_elist + cs.elist_base[e], jb.first, 0});
+        }
+        lv[k].nconf = (uint32_t)plan.conf[k].size();
+        lv[k].conf_first = (uint32_t)cf.size();
+        cf.insert(cf.end(), plan.conf[k].begin(), plan.conf[k].end());
+    }
+    const uint32_t nb = (uint32_t)bk.size(), nc = (uint32_t)cf.size();
+    const uint64_t pbytes = n * sizeof(DLevel) + nb * sizeof(DBack) + nc * sizeof(uint32_t);
+    std::vector<uint8_t> hp(pbytes);
+    std::memcpy(hp.data(), lv.data(), n * sizeof(DLevel));
+    std::memcpy(hp.data() + n * sizeof(DLevel), bk.data(), nb * sizeof(DBack));
+    std::memcpy(hp.data() + n * sizeof(DLevel) + nb * sizeof(DBack), cf.data(), nc * sizeof(uint32_t));
+    uint8_t *d_plan = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_local = nullptr;
+    uint32_t *d_rows = nullptr;
+    int rc = ASDM_OK;
+    auto cleanup = [&]() {
+        dfree(d_plan, s);
+        dfree(d_ctr, s);
+        dfree(d_local, s);
+        dfree(d_rows, s);
+    };
+    EnumArgs a{};
+    uint64_t row_cap = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    do {
+        if ((rc = dalloc(&d_plan, pbytes, s))) break;
+        if ((rc = dalloc(&d_ctr, kCtrN, s))) break;
+        if (cudaMemcpyAsync(d_plan, hp.data(), pbytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemsetAsync(d_ctr, 0, kCtrN * sizeof(unsigned long long), s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "plan upload failed");
+            break;
+        }
+        const uint64_t local_n = (uint64_t)G->d.n * n;
+        if (mode & ASDM_MODE_LOCAL) {
+            if ((rc = dalloc(&d_local, local_n, s))) break;
+            if (cudaMemsetAsync(d_local, 0, local_n * sizeof(unsigned long long), s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "memset failed");
+                break;
+            }
+        }
+        if (mode & ASDM_MODE_EMBED) {
+            row_cap = opt.embeddings ? opt.emb_capacity : 0;
+            if ((rc = dalloc(&d_rows, std::max<uint64_t>(row_cap, 1) * n, s))) break;
+        }
+        a.lv = reinterpret_cast<const DLevel *>(d_plan);
+        a.bk = reinterpret_cast<const DBack *>(d_plan + n * sizeof(DLevel));
+        a.conf = reinterpret_cast<const uint32_t *>(d_plan + n * sizeof(DLevel) + nb * sizeof(DBack));
+        a.n = n;
+        a.nb = nb;
+        a.nc = nc;
+        a.nq = n;
+        if (n == 1) {
+            a.ntasks = cs.ncand[plan.order[0]];
+        } else {
+            const uint32_t e01 = plan.back[1][0].second;
+            a.off01 = cs.d_eoff + cs.eoff_base[e01];
+            a.list01 = cs.d_elist + cs.elist_base[e01];
+            a.n0 = cs.ncand[plan.order[0]];
+            a.ntasks = cs.etotal[e01];
+        }
+        a.ctr = d_ctr;
+        a.local = d_local;
+        a.rows = d_rows;
+        a.row_cap = row_cap;
+        a.limit_ns = opt.time_limit_s > 0 ? (uint64_t)(opt.time_limit_s * 1e9) : 0;
+        const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+        if (a.ntasks) {
+            switch (mode) {
+                case ASDM_MODE_COUNT: rc = launch<ASDM_MODE_COUNT>(a, smem, G->num_sms, s); break;
+                case ASDM_MODE_LOCAL: rc = launch<ASDM_MODE_LOCAL>(a, smem, G->num_sms, s); break;
+                case ASDM_MODE_EMBED: rc = launch<ASDM_MODE_EMBED>(a, smem, G->num_sms, s); break;
+                default: rc = launch<ASDM_MODE_LOCAL | ASDM_MODE_EMBED>(a, smem, G->num_sms, s); break;
+            }
+            if (rc) break;
+        }
+        cudaEventRecord(e1, s);
+        unsigned long long ctr[kCtrN];
+        if (cudaMemcpyAsync(ctr, d_ctr, sizeof ctr, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "counter readback failed");
+            break;
+        }
+        cudaError_t se = cudaStreamSynchronize(s);
+        if (se != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "enumeration kernel failed: %s", cudaGetErrorString(se));
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        st.kernel_ms = ms;
+        st.count = ctr[kCtrCount];
+        st.intersections = ctr[kCtrInter];
+        st.list_bytes = 4ull * ctr[kCtrElems];
+        st.tasks = a.ntasks;
+        const uint32_t flags = (uint32_t)ctr[kCtrFlags];
+        if (flags & kFlagOverflow) { rc = fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1"); break; }
+        if (flags & kFlagTimeout) { rc = fail(ASDM_ERR_TIMEOUT, "time limit reached"); break; }
+        if ((mode & ASDM_MODE_LOCAL) && opt.local_counts) {
+            if (cudaMemcpyAsync(opt.local_counts, d_local, local_n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+                break;
+            }
+        }
+        if (mode & ASDM_MODE_EMBED) {
+            const uint64_t rows = ctr[kCtrRows];
+            st.emb_rows = std::min<uint64_t>(rows, row_cap);
+            if (rows > row_cap) {
+                rc = fail(ASDM_ERR_CAPACITY, "%llu embeddings, buffer holds %llu", (unsigned long long)rows,
+                          (unsigned long long)row_cap);
+                break;
+            }
+            if (rows) {
+                std::vector<uint32_t> tmp(rows * n);
+                if (cudaMemcpyAsync(tmp.data(), d_rows, rows * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
+                        cudaSuccess ||
+                    cudaStreamSynchronize(s) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "embedding readback failed");
+                    break;
+                }
+                std::vector<uint64_t> perm(rows);
+                std::iota(perm.begin(), perm.end(), 0ull);
+                std::sort(perm.begin(), perm.end(), [&](uint64_t x, uint64_t y) {
+                    return std::lexicographical_compare(tmp.begin() + x * n, tmp.begin() + x * n + n,
+                                                        tmp.begin() + y * n, tmp.begin() + y * n + n);
+                });
+                for (uint64_t r = 0; r < rows; ++r)
+                    std::memcpy(opt.embeddings + r * n, tmp.data() + perm[r] * n, n * sizeof(uint32_t));
+            }
+        }
+    } while (false);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cleanup();
+    cudaStreamSynchronize(s);
+    return rc;
+}
+
+}  // namespace asdm
+
+using namespace asdm;
+
+extern "C" int asdm_run_plan(asdm_cs *cs, const asdm_plan *plan, const asdm_run_opts *opts, asdm_run_stats *stats) {
+    clear_error();
+    if (!cs || !opts) return fail(ASDM_ERR_INVALID, "null argument");
+    asdm_run_stats local_stats{};
+    asdm_run_stats &st = stats ? *stats : local_stats;
+    if ((opts->mode & ASDM_MODE_EMBED) && !opts->embeddings && opts->emb_capacity)
+        return fail(ASDM_ERR_INVALID, "embedding buffer is null");
+    if (!cs->nonempty) {
+        st = asdm_run_stats{};
+        if (opts->local_counts && (opts->mode & ASDM_MODE_LOCAL))
+            std::fill(opts->local_counts, opts->local_counts + (uint64_t)cs->g->d.n * cs->q.n, 0ull);
+        return ASDM_OK;
+    }
+    if (!plan) return fail(ASDM_ERR_INVALID, "null plan");
+    if (plan->order.size() != cs->q.n) return fail(ASDM_ERR_INVALID, "plan does not match the query");
+    return run_plan(*cs, *plan, *opts, st);
+}
+
+extern "C" int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                                const uint32_t *q_labels, uint32_t q_n, const asdm_run_opts *opts,
+                                asdm_run_stats *stats) {
+    clear_error();
+    if (!g || !opts) return fail(ASDM_ERR_INVALID, "null argument");
+    asdm_cs *cs = nullptr;
+    int nonempty = 0;
+    ASDM_TRY(asdm_candidate_space(g, q_offsets, q_nbrs, q_labels, q_n, &cs, &nonempty));
+    asdm_plan *plan = nullptr;
+    int rc = ASDM_OK;
+    if (nonempty) rc = asdm_plan_create(cs, nullptr, &plan);
+    if (rc == ASDM_OK) rc = asdm_run_plan(cs, plan, opts, stats);
+    asdm_plan_free(plan);
+    asdm_cs_free(cs);
+    return rc;
+}

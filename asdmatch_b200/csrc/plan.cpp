@@ -1,0 +1,145 @@
+// Host planner: chooses the matching order the enumeration kernels follow.
+//
+// The reference plans with a fractional hypertree decomposition, a sampling
+// cardinality estimator and a cost-based DP over bag permutations
+// (plan/optimizer.cpp:380-548, plan/estimator.cpp:173-291).  Plans change the
+// amount of work, never the count.  This planner uses the candidate space the
+// device already built: for a directed query edge e = (u -> u2) the average
+// list length a(e) = |candidate edges of e| / |C(u)| estimates how many u2
+// candidates extend one u candidate, and a(e)/|C(u2)| is the chance that a
+// given u2 candidate survives the extra intersection with e's list.  For every
+// start vertex it grows a connected order greedily by the smallest estimated
+// number of partial matches, and keeps the order with the smallest total
+// estimated work (partial matches expanded + 32-wide list chunks scanned).
+#include <algorithm>
+#include <cmath>
+#include <memory>
+
+#include "cs.cuh"
+
+namespace asdm {
+
+namespace {
+
+double avg_len(const asdm_cs &cs, uint32_t from, uint32_t to) {
+    const int k = cs.q.slot(from, to);
+    const uint32_t e = cs.q.off[from] + (uint32_t)k;
+    return cs.ncand[from] ? (double)cs.etotal[e] / (double)cs.ncand[from] : 0.0;
+}
+
+void greedy_from(const asdm_cs &cs, uint32_t start, std::vector<uint32_t> &order, double &cost) {
+    const QueryGraph &q = cs.q;
+    const uint32_t n = q.n;
+    std::vector<char> in(n, 0);
+    order.assign(1, start);
+    in[start] = 1;
+    double N = (double)cs.ncand[start];
+    cost = 0.0;
+    for (uint32_t k = 1; k < n; ++k) {
+        int best = -1;
+        double bestN = 0, bestWork = 0;
+        uint32_t bestB = 0;
+        for (uint32_t u = 0; u < n; ++u) {
+            if (in[u]) continue;
+            double drv = INFINITY;
+            std::vector<double> lens;
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                const uint32_t j = q.nbr[e];
+                if (!in[j]) continue;
+                const double a = avg_len(cs, j, u);
+                lens.push_back(a);
+                drv = std::min(drv, a);
+            }
+            if (lens.empty()) continue;
+            double factor = drv;
+            bool skipped = false;
+            for (double a : lens) {
+                if (!skipped && a == drv) { skipped = true; continue; }
+                factor *= std::min(1.0, a / std::max(1.0, (double)cs.ncand[u]));
+            }
+            const double Nu = N * factor;
+            const double work = N * (1.0 + lens.size() * std::ceil(std::max(drv, 1.0) / 32.0));
+            const uint32_t B = (uint32_t)lens.size();
+            if (best < 0 || Nu < bestN || (Nu == bestN && B > bestB)) {
+                best = (int)u;
+                bestN = Nu;
+                bestWork = work;
+                bestB = B;
+            }
+        }
+        if (best < 0) { cost = INFINITY; return; }  // disconnected
+        order.push_back((uint32_t)best);
+        in[best] = 1;
+        cost += bestWork + (k + 1 < n ? bestN : 0.0);
+        N = std::max(bestN, 1e-9);
+    }
+}
+
+}  // namespace
+
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p) {
+    const QueryGraph &q = cs.q;
+    const uint32_t n = q.n;
+    if (!cs.nonempty) return fail(ASDM_ERR_INVALID, "cannot plan over an empty candidate space");
+    if (user_order) {
+        p.order.assign(user_order, user_order + n);
+        std::vector<char> seen(n, 0);
+        for (uint32_t k = 0; k < n; ++k) {
+            if (p.order[k] >= n || seen[p.order[k]]) return fail(ASDM_ERR_INVALID, "order is not a permutation");
+            seen[p.order[k]] = 1;
+        }
+        p.cost = 0;
+    } else {
+        double best = INFINITY;
+        for (uint32_t s = 0; s < n; ++s) {
+            std::vector<uint32_t> o;
+            double c;
+            greedy_from(cs, s, o, c);
+            if (o.size() == n && c < best) {
+                best = c;
+                p.order = o;
+            }
+        }
+        if (p.order.size() != n) return fail(ASDM_ERR_INVALID, "query is not connected");
+        p.cost = best;
+    }
+    std::vector<uint32_t> level(n, 0);
+    for (uint32_t k = 0; k < n; ++k) level[p.order[k]] = k;
+    p.back.assign(n, {});
+    p.conf.assign(n, {});
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t u = p.order[k];
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t w = p.order[j];
+            const int slot = q.slot(w, u);
+            if (slot >= 0) p.back[k].push_back({j, q.off[w] + (uint32_t)slot});
+            else if (q.lab[w] == q.lab[u]) p.conf[k].push_back(j);
+        }
+        if (k > 0 && p.back[k].empty()) return fail(ASDM_ERR_INVALID, "order is not connected at level %u", k);
+    }
+    return ASDM_OK;
+}
+
+}  // namespace asdm
+
+using namespace asdm;
+
+extern "C" int asdm_plan_create(const asdm_cs *cs, const uint32_t *order, asdm_plan **out) {
+    clear_error();
+    if (!cs || !out) return fail(ASDM_ERR_INVALID, "null argument");
+    auto p = std::make_unique<asdm_plan>();
+    ASDM_TRY(build_plan(*cs, order, *p));
+    *out = p.release();
+    return ASDM_OK;
+}
+
+extern "C" int asdm_plan_order(const asdm_plan *p, uint32_t *order) {
+    if (!p || !order) return fail(ASDM_ERR_INVALID, "null argument");
+    std::copy(p->order.begin(), p->order.end(), order);
+    return ASDM_OK;
+}
+
+extern "C" int asdm_plan_free(asdm_plan *p) {
+    delete p;
+    return ASDM_OK;
+}

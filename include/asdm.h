@@ -1,0 +1,178 @@
+/*
+ * asdm.h — C ABI of the B200 matching and counting engine (libasdm_b200.so).
+ *
+ * Drop-in boundary for ASDMatch's matching and counting path.  Every entry
+ * point is extern "C", takes plain pointers and sizes, returns an int status
+ * (ASDM_OK = 0) and never traps; asdm_last_error() gives a one-line reason for
+ * the calling thread's last failure.  Handles are opaque.  Host buffers are
+ * owned by the caller; device memory is owned by the library.
+ *
+ * Each declaration names the reference interface it replaces
+ * (path:line inside the reference project magic62442/ASDMatch).
+ */
+#ifndef ASDM_H
+#define ASDM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ASDM_OK 0
+#define ASDM_ERR_INVALID 1   /* bad argument or malformed graph               */
+#define ASDM_ERR_IO 2        /* file cannot be opened ("Can not open file")   */
+#define ASDM_ERR_CUDA 3      /* CUDA runtime error (no device, launch error)  */
+#define ASDM_ERR_OOM 4       /* device allocation failed or budget exceeded   */
+#define ASDM_ERR_OVERFLOW 5  /* a uint64 count or local count overflowed      */
+#define ASDM_ERR_TIMEOUT 6   /* the run's time limit was reached              */
+#define ASDM_ERR_CAPACITY 7  /* embedding buffer smaller than the match count */
+#define ASDM_ERR_INTERNAL 8  /* device-side consistency check failed          */
+
+/* ---- run modes (bit mask); the reference selects these at compile time
+ *      with ALL_LEVEL / LOCAL_COUNT / COLLECT_RESULT (config/config.h:38-40) */
+#define ASDM_MODE_COUNT 0u   /* exact uint64 count (ALL_LEVEL)                 */
+#define ASDM_MODE_LOCAL 1u   /* + |Vg| x |Vq| local counts (LOCAL_COUNT)       */
+#define ASDM_MODE_EMBED 2u   /* + the embeddings themselves (COLLECT_RESULT)   */
+
+typedef struct asdm_host_graph asdm_host_graph; /* host CSR, reference layout  */
+typedef struct asdm_graph asdm_graph;           /* device-resident data graph  */
+typedef struct asdm_cs asdm_cs;                 /* device candidate space      */
+typedef struct asdm_plan asdm_plan;             /* matching order + level info */
+
+/* Returns a static, thread-local description of the last failure. */
+const char *asdm_last_error(void);
+/* Library version string. */
+const char *asdm_version(void);
+
+/* ---- host graphs ------------------------------------------------------- */
+
+/* Replaces Graph::loadGraphFromTextFile (relation/graph.cpp:68-148): 't N M'
+ * header, 'v id label degree' (degree fixes the CSR offsets), 'e a b' edges,
+ * other tokens skipped; neighbours sorted by (label, id). ASDM_ERR_IO if the
+ * file cannot be opened. */
+int asdm_host_graph_load(const char *path, asdm_host_graph **out);
+/* Builds a host graph from an undirected edge list (edges[2*i], edges[2*i+1]);
+ * same layout as the loader. Replaces nothing (synthetic inputs). */
+int asdm_host_graph_from_edges(uint32_t n, const uint32_t *labels, uint64_t m,
+                               const uint32_t *edges, asdm_host_graph **out);
+/* Size queries and zero-copy views of the CSR (offsets[n+1], nbrs[m2],
+ * labels[n]); the views live as long as the graph (relation/graph.h:58-104). */
+int asdm_host_graph_info(const asdm_host_graph *g, uint32_t *n, uint64_t *m2, uint32_t *nlabels);
+int asdm_host_graph_csr(const asdm_host_graph *g, const uint32_t **offsets, const uint32_t **nbrs,
+                        const uint32_t **labels);
+/* Writes the graph in 't/v/e' text (Graph::writeToTextFile, relation/graph.h:157). */
+int asdm_host_graph_write(const asdm_host_graph *g, const char *path);
+void asdm_host_graph_free(asdm_host_graph *g);
+
+/* Seeded Chung-Lu power-law graph: weights (i+i0)^(-1/(gamma-1)) with i0 set so
+ * that the largest weight is sqrt(2m), endpoint pairs drawn by weight until m
+ * distinct non-loop edges exist, labels i.i.d. Zipf(zipf_s) over nlabels,
+ * vertex ids randomly permuted.  No reference counterpart (synthetic input). */
+int asdm_gen_chung_lu(uint32_t n, uint64_t m, double gamma, uint32_t nlabels, double zipf_s,
+                      uint64_t seed, asdm_host_graph **out);
+/* Connected query by random walk with restart from a seeded data vertex: the
+ * induced subgraph on the first `size` distinct vertices, labels copied.
+ * density: 0 any, 1 dense (average degree >= 3), 2 sparse (< 3).  No
+ * reference counterpart (the reference ships its query sets as files). */
+int asdm_gen_query(const asdm_host_graph *g, uint32_t size, int density, uint64_t seed,
+                   asdm_host_graph **out);
+
+/* ---- device data graph ------------------------------------------------- */
+
+/* Uploads a CSR data graph whose neighbour lists are sorted by (label, id)
+ * (the loader's layout) and builds the label index on the device.  Replaces
+ * the data-side Graph of CandidateSpace(q, g) (relation/candidate_space.cpp:87,
+ * relation/graph.h:34-56). ASDM_ERR_INVALID if a list is not (label,id)-sorted. */
+int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, const uint32_t *labels,
+                      uint32_t n, uint64_t m2, uint32_t nlabels, asdm_graph **out);
+int asdm_graph_free(asdm_graph *g);
+
+/* ---- candidate space (K1-K3) ------------------------------------------- */
+
+/* CFL candidate space of a query (CSR in the loader's layout) on the device:
+ * CandidateSpace::CandidateSpace + buildCandCFL (relation/candidate_space.cpp:87-107,
+ * 550-721) including buildCandidateEdge(false) (:458-487).  *nonempty = 0 when
+ * some candidate set is empty (buildCandCFL returns false; the count is 0). */
+int asdm_candidate_space(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                         const uint32_t *q_labels, uint32_t q_n, asdm_cs **out, int *nonempty);
+/* |C(u)| for every query vertex (candidateSet[u].size()). */
+int asdm_cs_sizes(const asdm_cs *cs, uint32_t *sizes);
+/* C(u), sorted vertex ids (candidateSet[u], relation/candidate_space.h:47). */
+int asdm_cs_read(const asdm_cs *cs, uint32_t u, uint32_t *out, uint32_t capacity);
+/* Candidate edges of query edge (u, u2) (candidateEdge[u][v][u2], :49): offsets[|C(u)|+1]
+ * and the neighbour vertex ids, in the order writeToStream prints them (:489-505).
+ * *total receives the number of entries; ASDM_ERR_CAPACITY if it exceeds capacity. */
+int asdm_cs_read_edges(const asdm_cs *cs, uint32_t u, uint32_t u2, uint32_t *offsets,
+                       uint32_t *vertices, uint64_t capacity, uint64_t *total);
+int asdm_cs_free(asdm_cs *cs);
+
+/* ---- sorted-set intersection (K4) --------------------------------------- */
+
+/* Batched k-way intersection of sorted uint32 lists on the device: for each of
+ * `nsets` problems, list_ptr[list_first[s] .. list_first[s+1]) index into
+ * (values, list_off); result s is written to out[out_off[s] ..) with its size
+ * in out_count[s].  All arrays are host arrays.  Replaces
+ * ComputeSetIntersection::LeapfrogJoin (utility/compute_set_intersection.cpp:193-233). */
+int asdm_intersect_batch(const uint32_t *values, const uint64_t *list_off, uint64_t nlists,
+                         const uint32_t *list_first, uint32_t nsets, const uint64_t *out_off,
+                         uint32_t *out, uint32_t *out_count);
+
+/* ---- plan ---------------------------------------------------------------- */
+
+/* Matching order for the enumeration kernels.  order == NULL lets the planner
+ * choose (cost model over candidate-edge sizes, the role of optCostPlan /
+ * simplePlan, plan/optimizer.cpp:7-200,380-548); otherwise `order` is a
+ * connected permutation of the query vertices. */
+int asdm_plan_create(const asdm_cs *cs, const uint32_t *order, asdm_plan **out);
+int asdm_plan_order(const asdm_plan *p, uint32_t *order);
+int asdm_plan_free(asdm_plan *p);
+
+/* ---- enumeration and counting (K5-K8) ----------------------------------- */
+
+typedef struct asdm_run_opts {
+    uint32_t mode;          /* ASDM_MODE_* bit mask                            */
+    uint64_t budget_bytes;  /* -m budget for materialised prefixes (0 = 1.6e6 KB) */
+    double time_limit_s;    /* 0 = unlimited; else ASDM_ERR_TIMEOUT past it    */
+    uint64_t *local_counts; /* host |Vg| x |Vq| row-major (MODE_LOCAL) or NULL */
+    uint32_t *embeddings;   /* host rows x |Vq|, sorted on return (MODE_EMBED) */
+    uint64_t emb_capacity;  /* rows available in `embeddings`                  */
+} asdm_run_opts;
+
+typedef struct asdm_run_stats {
+    uint64_t count;          /* number of matches                               */
+    uint64_t emb_rows;       /* rows written to `embeddings`                    */
+    uint64_t intersections;  /* k-way intersections with k >= 2                 */
+    uint64_t list_bytes;     /* algorithmic bytes of lists read by the kernels  */
+    uint64_t tasks;          /* root tasks processed                            */
+    double kernel_ms;        /* device time of the enumeration kernels          */
+} asdm_run_stats;
+
+/* Exact enumeration of one query over its candidate space.  Replaces
+ * adaptiveShareJoin (matching/adaptive.cpp:1179-2279) with the ALL_LEVEL
+ * traverse/produceResult path (matching/join.cpp:819-907,1017-1097) and the
+ * gLocalCount accumulation (matching/join.cpp:1035-1041). */
+int asdm_run_plan(asdm_cs *cs, const asdm_plan *plan, const asdm_run_opts *opts,
+                  asdm_run_stats *stats);
+
+/* One call for a query end to end on a resident graph: candidate space, plan
+ * and count (the whole of ASDMatch.out's main(), main.cpp:11-147, without I/O). */
+int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q_nbrs,
+                     const uint32_t *q_labels, uint32_t q_n, const asdm_run_opts *opts,
+                     asdm_run_stats *stats);
+
+/* Many queries against one resident data graph (no reference counterpart; the
+ * reference runs one query per process).  Query i is the CSR slice
+ * q_offsets[q_off_base[i] ..], q_nbrs[q_nbr_base[i] ..], q_labels[q_lab_base[i] ..]
+ * with q_sizes[i] vertices.  counts[i] and status[i] receive each query's
+ * result; the call returns ASDM_OK when every status is ASDM_OK. */
+int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                   const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                   const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
+                   uint64_t *counts, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASDM_H */

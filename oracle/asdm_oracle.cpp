@@ -1,0 +1,524 @@
+// ORACLE — test infrastructure only.
+//
+// A plain CPU restatement of the reference's matching and counting path, used
+// by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the
+// checker.  The product (asdmatch_b200/, the CLI, the C-ABI library) never
+// links, loads or calls it.
+//
+// Parity is pinned against the reference itself: oracle/ref.mk compiles the
+// reference sources into oracle/_ref/{ref_count,ref_local,ref_embed}, and
+// tests/golden/ holds counts, local-count CSV digests, embedding digests and
+// candidate-space digests produced by those binaries (tests/golden/make_golden.py).
+//
+// What is restated (reference file:line):
+//  * Graph::loadGraphFromTextFile (relation/graph.cpp:68-148): 't N M' header,
+//    'v id label degree' lines whose degree sets the CSR offsets, 'e a b'
+//    lines appended to both endpoints, other tokens skipped; neighbours sorted
+//    by (label, id); vertices grouped by label in id order; numLabels =
+//    max label + 1.
+//  * nlcValid (utility/utils.cpp:30-40): for every label, the query vertex's
+//    neighbour-label count is <= the data vertex's.
+//  * CandidateSpace::selectCFLRoot (relation/candidate_space.cpp:723-763),
+//    buildCFLBFSTree (:765-816) and buildCandCFL (:550-721).  buildCandCFL is
+//    restated as the set formula it computes:
+//       F(u)    = { v in V_l(u) : deg v >= deg u, nlc(u) <= nlc(v) }
+//       Ctd(r)  = F(r) for the root r
+//       Ctd(u)  = F(u) ∩ ⋂_{p in before(u)} N_l(u)(S(p))    (BFS order)
+//       C(u)    = Ctd(u) ∩ ⋂_{p in N_q(u) \ before(u)} N_l(u)(S(p))
+//    where S(p) is the *storage* the reference scans for p's candidates: the
+//    top-down candidates Ctd(p) plus data vertex 0 whenever Ctd(p) is smaller
+//    than |V_l(p)| (candidateSet[p] is resized to |V_l(p)| up front and its
+//    unused zero-initialised tail is iterated by the range-for loops at
+//    :588,:623,:661; pruned entries stay in that storage until the final
+//    compaction at :692-703).
+//  * CandidateSpace::buildCandidateEdge(false) (:458-487): for query edge
+//    (u,u2) and v in C(u), the label-l(u2) neighbours of v that are in C(u2),
+//    in adjacency order; CandidateSpace::writeToStream (:489-505) format.
+//  * The ALL_LEVEL / LOCAL_COUNT / COLLECT_RESULT results of
+//    adaptiveShareJoin (matching/adaptive.cpp:1179-2279 with
+//    matching/join.cpp:819-907,1017-1097): the number of injective,
+//    label-preserving, edge-preserving maps V_q -> V_g; the |V_g|x|V_q|
+//    matrix of how many of them send u to v; the sorted list of the maps in
+//    storeMatches format (matching/join.cpp:1099-1107).  Counted here by plain
+//    backtracking over the candidate space, which is exact because the CFL
+//    filter only removes vertices that cannot be in any embedding.
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <queue>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct OGraph {
+    uint32_t n = 0;
+    uint64_t m2 = 0;
+    uint32_t nlabels = 0;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> nbr;
+    std::vector<uint32_t> lab;
+    std::vector<uint32_t> vbl_off;  // vertices by label: [vbl_off[l], vbl_off[l+1])
+    std::vector<uint32_t> vbl;
+
+    uint32_t deg(uint32_t v) const { return (uint32_t)(off[v + 1] - off[v]); }
+    // label-l neighbour run of v (neighbours are sorted by (label, id))
+    void run(uint32_t v, uint32_t l, uint64_t &b, uint64_t &e) const {
+        const uint32_t *base = nbr.data();
+        uint64_t lo = off[v], hi = off[v + 1];
+        auto cmp_lo = [&](uint32_t x, uint32_t lbl) { return lab[x] < lbl; };
+        b = std::lower_bound(base + lo, base + hi, l, cmp_lo) - base;
+        uint64_t p = b;
+        while (p < hi && lab[base[p]] == l) ++p;
+        e = p;
+    }
+    bool adjacent(uint32_t a, uint32_t b) const {
+        uint64_t s, e;
+        run(a, lab[b], s, e);
+        return std::binary_search(nbr.begin() + s, nbr.begin() + e, b);
+    }
+    // neighbour-label counts, sorted by label
+    std::vector<std::pair<uint32_t, uint32_t>> nlc(uint32_t v) const {
+        std::vector<std::pair<uint32_t, uint32_t>> r;
+        for (uint64_t i = off[v]; i < off[v + 1]; ++i) {
+            uint32_t l = lab[nbr[i]];
+            if (!r.empty() && r.back().first == l) ++r.back().second;
+            else r.emplace_back(l, 1);
+        }
+        return r;
+    }
+};
+
+bool load_graph(const std::string &path, OGraph &g) {
+    std::ifstream in(path);
+    if (!in.is_open()) return false;
+    std::string tok;
+    uint64_t m = 0;
+    in >> tok >> g.n >> m;
+    g.m2 = 2 * m;
+    g.off.assign(g.n + 1, 0);
+    g.lab.assign(g.n, 0);
+    g.nbr.assign(g.m2, 0);
+    std::vector<uint64_t> fill(g.n, 0);
+    uint32_t maxl = 0;
+    while (in >> tok) {
+        if (tok == "v") {
+            uint64_t id, l, d;
+            in >> id >> l >> d;
+            g.lab[id] = (uint32_t)l;
+            g.off[id + 1] = g.off[id] + d;
+            maxl = std::max<uint32_t>(maxl, (uint32_t)l);
+        } else if (tok == "e") {
+            uint64_t a, b;
+            in >> a >> b;
+            g.nbr[g.off[a] + fill[a]++] = (uint32_t)b;
+            g.nbr[g.off[b] + fill[b]++] = (uint32_t)a;
+        }
+    }
+    g.nlabels = maxl + 1;
+    for (uint32_t v = 0; v < g.n; ++v)
+        std::sort(g.nbr.begin() + g.off[v], g.nbr.begin() + g.off[v + 1], [&](uint32_t a, uint32_t b) {
+            return g.lab[a] != g.lab[b] ? g.lab[a] < g.lab[b] : a < b;
+        });
+    g.vbl_off.assign(g.nlabels + 1, 0);
+    for (uint32_t v = 0; v < g.n; ++v) g.vbl_off[g.lab[v] + 1]++;
+    for (uint32_t l = 0; l < g.nlabels; ++l) g.vbl_off[l + 1] += g.vbl_off[l];
+    g.vbl.resize(g.n);
+    std::vector<uint32_t> pos(g.vbl_off.begin(), g.vbl_off.end() - 1);
+    for (uint32_t v = 0; v < g.n; ++v) g.vbl[pos[g.lab[v]]++] = v;
+    return true;
+}
+
+bool nlc_contained(const std::vector<std::pair<uint32_t, uint32_t>> &qn,
+                   const std::vector<std::pair<uint32_t, uint32_t>> &dn) {
+    size_t j = 0;
+    for (auto &e : qn) {
+        while (j < dn.size() && dn[j].first < e.first) ++j;
+        if (j == dn.size() || dn[j].first != e.first || dn[j].second < e.second) return false;
+    }
+    return true;
+}
+
+struct CandSpace {
+    bool ok = false;
+    std::vector<std::vector<uint32_t>> C;  // sorted candidate vertex ids per query vertex
+    // edges[u][k] = candidate edge lists for the k-th query neighbour of u:
+    // lists[i] = neighbours of C[u][i] (vertex ids) in C[u2]
+    std::vector<std::vector<std::vector<std::vector<uint32_t>>>> edges;
+    uint32_t root = 0;
+    std::vector<uint32_t> bfs_order;
+};
+
+void label_vertices(const OGraph &g, uint32_t l, const uint32_t *&p, uint32_t &cnt) {
+    if (l >= g.nlabels) { p = nullptr; cnt = 0; return; }
+    p = g.vbl.data() + g.vbl_off[l];
+    cnt = g.vbl_off[l + 1] - g.vbl_off[l];
+}
+
+CandSpace build_cfl(const OGraph &q, const OGraph &g) {
+    CandSpace cs;
+    const uint32_t nq = q.n;
+    std::vector<std::vector<char>> F(nq);
+    std::vector<uint32_t> fsize(nq, 0);
+    for (uint32_t u = 0; u < nq; ++u) {
+        F[u].assign(g.n, 0);
+        const uint32_t *vs; uint32_t cnt;
+        label_vertices(g, q.lab[u], vs, cnt);
+        auto qn = q.nlc(u);
+        for (uint32_t i = 0; i < cnt; ++i) {
+            uint32_t v = vs[i];
+            if (g.deg(v) < q.deg(u)) continue;
+            if (!nlc_contained(qn, g.nlc(v))) continue;
+            F[u][v] = 1;
+            ++fsize[u];
+        }
+    }
+    // Root: keep the three smallest |V_l(u)|/deg(u) in a max-heap (same
+    // container and comparator semantics as candidate_space.cpp:724-733), then
+    // pop them largest-first and keep the first strict minimum of
+    // |F(u)|/deg(u).
+    auto cmp = [](const std::pair<uint32_t, double> &a, const std::pair<uint32_t, double> &b) {
+        return a.second < b.second;
+    };
+    std::priority_queue<std::pair<uint32_t, double>, std::vector<std::pair<uint32_t, double>>, decltype(cmp)> pq(cmp);
+    for (uint32_t u = 0; u < nq; ++u) {
+        const uint32_t *vs; uint32_t cnt;
+        label_vertices(g, q.lab[u], vs, cnt);
+        pq.emplace(u, cnt / (double)q.deg(u));
+    }
+    while (pq.size() > 3) pq.pop();
+    uint32_t root = 0;
+    double best = g.n;
+    while (!pq.empty()) {
+        uint32_t u = pq.top().first;
+        pq.pop();
+        double score = fsize[u] / (double)q.deg(u);
+        if (score < best) { best = score; root = u; }
+    }
+    cs.root = root;
+    // BFS levels; within a level, discovery order over each vertex's
+    // (label, id)-sorted query neighbours.
+    std::vector<uint32_t> order;
+    std::vector<char> seen(nq, 0);
+    std::vector<uint32_t> frontier{root};
+    seen[root] = 1;
+    while (!frontier.empty()) {
+        std::vector<uint32_t> next;
+        for (uint32_t u : frontier) {
+            order.push_back(u);
+            for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                uint32_t w = q.nbr[e];
+                if (!seen[w]) { seen[w] = 1; next.push_back(w); }
+            }
+        }
+        frontier.swap(next);
+    }
+    cs.bfs_order = order;
+    std::vector<uint32_t> rank(nq, 0);
+    for (uint32_t i = 0; i < order.size(); ++i) rank[order[i]] = i;
+    // Unreached query vertices (disconnected query) never get candidates in
+    // the reference's pass loop; they keep an empty set.
+    std::vector<char> reached(nq, 0);
+    for (uint32_t u : order) reached[u] = 1;
+
+    auto mark_neighbours = [&](const std::vector<uint32_t> &support, uint32_t l, std::vector<char> &mark) {
+        mark.assign(g.n, 0);
+        for (uint32_t w : support) {
+            uint64_t b, e;
+            g.run(w, l, b, e);
+            for (uint64_t i = b; i < e; ++i) mark[g.nbr[i]] = 1;
+        }
+    };
+    std::vector<std::vector<uint32_t>> Ctd(nq), S(nq);
+    std::vector<char> mark;
+    for (uint32_t u : order) {
+        std::vector<char> cur = F[u];
+        if (u != root) {
+            for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                uint32_t p = q.nbr[e];
+                if (rank[p] >= rank[u]) continue;
+                mark_neighbours(S[p], q.lab[u], mark);
+                for (uint32_t v = 0; v < g.n; ++v) cur[v] &= mark[v];
+            }
+        }
+        for (uint32_t v = 0; v < g.n; ++v) if (cur[v]) Ctd[u].push_back(v);
+        const uint32_t *vs; uint32_t cnt;
+        label_vertices(g, q.lab[u], vs, cnt);
+        S[u] = Ctd[u];
+        if (Ctd[u].size() < cnt) S[u].push_back(0);
+    }
+    cs.C.assign(nq, {});
+    for (uint32_t u = 0; u < nq; ++u) {
+        if (!reached[u]) continue;
+        std::vector<char> cur(g.n, 0);
+        for (uint32_t v : Ctd[u]) cur[v] = 1;
+        for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            uint32_t p = q.nbr[e];
+            if (rank[p] < rank[u]) continue;
+            mark_neighbours(S[p], q.lab[u], mark);
+            for (uint32_t v = 0; v < g.n; ++v) cur[v] &= mark[v];
+        }
+        for (uint32_t v = 0; v < g.n; ++v) if (cur[v]) cs.C[u].push_back(v);
+    }
+    for (uint32_t u = 0; u < nq; ++u)
+        if (cs.C[u].empty()) { cs.ok = false; return cs; }
+    cs.ok = true;
+    cs.edges.assign(nq, {});
+    std::vector<std::vector<char>> inC(nq, std::vector<char>(g.n, 0));
+    for (uint32_t u = 0; u < nq; ++u) for (uint32_t v : cs.C[u]) inC[u][v] = 1;
+    for (uint32_t u = 0; u < nq; ++u) {
+        for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            uint32_t u2 = q.nbr[e];
+            std::vector<std::vector<uint32_t>> lists(cs.C[u].size());
+            for (size_t i = 0; i < cs.C[u].size(); ++i) {
+                uint64_t b, en;
+                g.run(cs.C[u][i], q.lab[u2], b, en);
+                for (uint64_t k = b; k < en; ++k)
+                    if (inC[u2][g.nbr[k]]) lists[i].push_back(g.nbr[k]);
+            }
+            cs.edges[u].push_back(std::move(lists));
+        }
+    }
+    return cs;
+}
+
+void write_cs(const OGraph &q, const CandSpace &cs, std::ostream &os) {
+    for (uint32_t u = 0; u < q.n; ++u) {
+        os << "C " << u << " " << cs.C[u].size();
+        for (uint32_t v : cs.C[u]) os << " " << v;
+        os << "\n";
+    }
+    for (uint32_t u = 0; u < q.n; ++u) {
+        for (uint64_t e = q.off[u], k = 0; e < q.off[u + 1]; ++e, ++k) {
+            os << "# " << u << " " << q.nbr[e] << "\n";
+            for (size_t i = 0; i < cs.C[u].size(); ++i)
+                for (uint32_t v2 : cs.edges[u][k][i]) os << cs.C[u][i] << " " << v2 << "\n";
+        }
+    }
+}
+
+enum { MODE_COUNT = 0, MODE_LOCAL = 1, MODE_EMBED = 2 };
+
+struct Enumerator {
+    const OGraph &q, &g;
+    const CandSpace &cs;
+    int mode;
+    std::vector<uint32_t> order;                 // level -> query vertex
+    std::vector<uint32_t> first_parent_level;    // level -> level of the parent whose list drives it
+    std::vector<uint32_t> first_parent_slot;     // index of u_k in that parent's neighbour list
+    std::vector<std::vector<uint32_t>> checks;   // level -> other backward levels (adjacency checks)
+    std::vector<uint32_t> phi, phi_idx;          // per level: vertex id, index in C(u)
+    std::vector<char> used;
+    uint64_t count = 0;
+    bool overflow = false;
+    std::vector<uint64_t> *local = nullptr;      // |Vg| x |Vq|, row-major
+    std::vector<std::vector<uint32_t>> *emb = nullptr;
+
+    Enumerator(const OGraph &q_, const OGraph &g_, const CandSpace &cs_, int mode_)
+        : q(q_), g(g_), cs(cs_), mode(mode_) {
+        // Connected order: start at the smallest candidate set, then always
+        // take the frontier vertex with the most already-ordered neighbours
+        // (ties: smaller candidate set, then smaller id).
+        const uint32_t nq = q.n;
+        std::vector<char> in(nq, 0);
+        uint32_t start = 0;
+        for (uint32_t u = 1; u < nq; ++u)
+            if (cs.C[u].size() < cs.C[start].size()) start = u;
+        order.push_back(start);
+        in[start] = 1;
+        while (order.size() < nq) {
+            int best = -1; uint32_t bestConn = 0;
+            for (uint32_t u = 0; u < nq; ++u) {
+                if (in[u]) continue;
+                uint32_t conn = 0;
+                for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) conn += in[q.nbr[e]];
+                if (conn == 0) continue;
+                if (best < 0 || conn > bestConn ||
+                    (conn == bestConn && cs.C[u].size() < cs.C[best].size())) {
+                    best = (int)u; bestConn = conn;
+                }
+            }
+            if (best < 0) break;  // disconnected query: handled by the caller
+            order.push_back((uint32_t)best);
+            in[best] = 1;
+        }
+        std::vector<uint32_t> lvl(nq, 0);
+        for (uint32_t i = 0; i < order.size(); ++i) lvl[order[i]] = i;
+        first_parent_level.assign(nq, 0);
+        first_parent_slot.assign(nq, 0);
+        checks.assign(nq, {});
+        for (uint32_t k = 1; k < order.size(); ++k) {
+            uint32_t u = order[k];
+            bool have = false;
+            for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                uint32_t p = q.nbr[e];
+                if (lvl[p] >= k) continue;
+                if (!have) {
+                    have = true;
+                    first_parent_level[k] = lvl[p];
+                    uint32_t slot = 0;
+                    for (uint64_t e2 = q.off[p]; e2 < q.off[p + 1]; ++e2, ++slot)
+                        if (q.nbr[e2] == u) break;
+                    first_parent_slot[k] = slot;
+                } else {
+                    checks[k].push_back(lvl[p]);
+                }
+            }
+        }
+        phi.assign(nq, 0);
+        phi_idx.assign(nq, 0);
+        used.assign(g.n, 0);
+    }
+
+    void add(uint64_t c) {
+        if (__builtin_add_overflow(count, c, &count)) overflow = true;
+    }
+
+    void record_full() {
+        if (mode == MODE_LOCAL || mode == MODE_EMBED)
+            for (uint32_t k = 0; k < q.n; ++k) (*local)[(uint64_t)phi[k] * q.n + order[k]] += 1;
+        if (mode == MODE_EMBED) {
+            std::vector<uint32_t> row(q.n);
+            for (uint32_t k = 0; k < q.n; ++k) row[order[k]] = phi[k];
+            emb->push_back(std::move(row));
+        }
+    }
+
+    void extend(uint32_t k) {
+        const uint32_t u = order[k];
+        const uint32_t pl = first_parent_level[k];
+        const uint32_t pu = order[pl];
+        const std::vector<uint32_t> &list = cs.edges[pu][first_parent_slot[k]][phi_idx[pl]];
+        for (uint32_t v : list) {
+            if (used[v]) continue;
+            bool ok = true;
+            for (uint32_t j : checks[k])
+                if (!g.adjacent(phi[j], v)) { ok = false; break; }
+            if (!ok) continue;
+            phi[k] = v;
+            phi_idx[k] = (uint32_t)(std::lower_bound(cs.C[u].begin(), cs.C[u].end(), v) - cs.C[u].begin());
+            if (k + 1 == q.n) {
+                add(1);
+                record_full();
+            } else {
+                used[v] = 1;
+                extend(k + 1);
+                used[v] = 0;
+            }
+        }
+    }
+
+    void run() {
+        const uint32_t u0 = order[0];
+        for (uint32_t i = 0; i < cs.C[u0].size(); ++i) {
+            uint32_t v = cs.C[u0][i];
+            phi[0] = v;
+            phi_idx[0] = i;
+            if (q.n == 1) { add(1); record_full(); continue; }
+            used[v] = 1;
+            extend(1);
+            used[v] = 0;
+        }
+    }
+};
+
+struct RunResult {
+    uint64_t count = 0;
+    bool overflow = false;
+    bool empty_cs = false;
+};
+
+int run_files(const char *qpath, const char *dpath, int mode, RunResult &res, const char *csv,
+              const char *embp, const char *csp) {
+    OGraph q, g;
+    if (!load_graph(qpath, q) || !load_graph(dpath, g)) return 2;
+    CandSpace cs = build_cfl(q, g);
+    std::vector<uint64_t> local;
+    std::vector<std::vector<uint32_t>> emb;
+    if (!cs.ok) {
+        res.empty_cs = true;
+        res.count = 0;
+        local.assign((uint64_t)g.n * q.n, 0);
+    } else {
+        if (csp && *csp) {
+            std::ofstream os(csp);
+            write_cs(q, cs, os);
+        }
+        Enumerator en(q, g, cs, mode);
+        if (en.order.size() != q.n) return 3;  // disconnected query
+        if (mode != MODE_COUNT) local.assign((uint64_t)g.n * q.n, 0);
+        en.local = &local;
+        en.emb = &emb;
+        en.run();
+        res.count = en.count;
+        res.overflow = en.overflow;
+    }
+    if (csv && *csv && mode != MODE_COUNT) {
+        std::ofstream os(csv);
+        for (uint32_t v = 0; v < g.n; ++v) {
+            for (uint32_t u = 0; u < q.n; ++u) {
+                os << local[(uint64_t)v * q.n + u];
+                if (u + 1 != q.n) os << ",";
+            }
+            os << "\n";
+        }
+    }
+    if (embp && *embp && mode == MODE_EMBED) {
+        std::sort(emb.begin(), emb.end());
+        std::ofstream os(embp);
+        os << emb.size() << "\n";
+        for (auto &r : emb) {
+            for (uint32_t v : r) os << v << " ";
+            os << "\n";
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// mode: 0 count, 1 local counts (csv), 2 local counts + embeddings.
+// Returns 0 on success, 2 unreadable file, 3 disconnected query.
+// *flags: bit0 = uint64 overflow of the count, bit1 = empty candidate set.
+int orc_run(const char *qpath, const char *dpath, int mode, uint64_t *count, uint32_t *flags,
+            const char *csv_path, const char *emb_path, const char *cs_path) {
+    RunResult r;
+    int rc = run_files(qpath, dpath, mode, r, csv_path, emb_path, cs_path);
+    if (count) *count = r.count;
+    if (flags) *flags = (r.overflow ? 1u : 0u) | (r.empty_cs ? 2u : 0u);
+    return rc;
+}
+
+}  // extern "C"
+
+#ifdef ORACLE_MAIN
+// CLI: asdm_oracle -q Q -d D [-c csv] [-e emb] [-w csdump]; prints the
+// reference's "Number of matches:" line.
+int main(int argc, char **argv) {
+    std::string qp, dp, csv, emb, csd;
+    for (int i = 1; i + 1 < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "-q") qp = argv[i + 1];
+        else if (a == "-d") dp = argv[i + 1];
+        else if (a == "-c") csv = argv[i + 1];
+        else if (a == "-e") emb = argv[i + 1];
+        else if (a == "-w") csd = argv[i + 1];
+    }
+    int mode = !emb.empty() ? MODE_EMBED : (!csv.empty() ? MODE_LOCAL : MODE_COUNT);
+    uint64_t c = 0;
+    uint32_t fl = 0;
+    int rc = orc_run(qp.c_str(), dp.c_str(), mode, &c, &fl, csv.c_str(), emb.c_str(), csd.c_str());
+    if (rc == 2) { std::cout << "Can not open file ." << std::endl; return 1; }
+    if (rc != 0) { std::cout << "error " << rc << std::endl; return 1; }
+    std::cout << "Number of matches: " << c << std::endl;
+    if (fl & 1) std::cout << "overflow" << std::endl;
+    return 0;
+}
+#endif

@@ -1,0 +1,185 @@
+// Test infrastructure only: a driver around the reference implementation's own
+// matching path, compiled from the reference sources by oracle/ref.mk into
+// oracle/_ref/.  Nothing in the product links or calls this file.
+//
+// It runs the same sequence of reference calls as the reference's ASDMatch.out
+// entry point (main.cpp:11-147 of the reference):
+//   Graph::loadGraphFromTextFile -> CandidateSpace::buildCandCFL ->
+//   setQueryGraphWeights -> buildFHD/HyperTree::buildFromTD -> reorderBags ->
+//   smallCard + SubsetStructure::optimalPlanDP/reverseDP (or a .card via -s) ->
+//   optCostPlan/simplePlan -> adaptiveShareJoin
+// with two harness differences:
+//   1. the per-bag trie root vector is sized *after* reorderBags(), because
+//      reorderBags may append a virtual global bag and the reference's own
+//      entry point sizes it before (main.cpp:51 vs main.cpp:69), which makes
+//      adaptiveGlobalJoin index one past the end (matching/adaptive.cpp:304);
+//   2. extra outputs for parity checks:
+//        -w <file>  candidate space dump: "C <u> <n> v..." lines, then the
+//                   reference's CandidateSpace::writeToStream listing
+//                   (relation/candidate_space.cpp:489-505);
+//        -e <file>  (COLLECT_RESULT builds) the embedding set, sorted, in the
+//                   reference's storeMatches format (matching/join.cpp:1099-1107).
+// Build variants select the reference's compile-time modes (config/config.h:38-40):
+//   ref_count : ALL_LEVEL                          (exact counts)
+//   ref_local : ALL_LEVEL + LOCAL_COUNT            (+ |Vg|x|Vq| CSV via -c)
+//   ref_embed : ALL_LEVEL + LOCAL_COUNT + COLLECT_RESULT (+ -e dump)
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "adaptive.h"
+#include "candidate_space.h"
+#include "command.h"
+#include "estimator.h"
+#include "join.h"
+#include "optimizer.h"
+
+static std::string option_after(int argc, char **argv, const char *flag) {
+    for (int i = 1; i + 1 < argc; ++i)
+        if (std::strcmp(argv[i], flag) == 0) return argv[i + 1];
+    return "";
+}
+
+static double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int main(int argc, char **argv) {
+    Command cmd(argc, argv);
+    const std::string qpath = cmd.getQueryGraphPath();
+    const std::string dpath = cmd.getDataGraphPath();
+    const std::string cardPath = cmd.getDPStructPath();
+    const std::string csDump = option_after(argc, argv, "-w");
+    const std::string embDump = option_after(argc, argv, "-e");
+    int memKB = cmd.getMemoryBudget();
+    if (memKB == 0) memKB = 16e5;
+    const size_t budget = (size_t)1024 * memKB;
+
+    Graph q, g;
+    q.loadGraphFromTextFile(qpath);
+    g.loadGraphFromTextFile(dpath);
+    CandidateSpace cs(q, g);
+
+    auto t0 = std::chrono::steady_clock::now();
+    if (!cs.buildCandCFL()) {
+        // The reference returns silently here (main.cpp:35-37); the harness
+        // reports the empty candidate space explicitly so tests can see it.
+        std::cout << "Empty candidate set" << std::endl;
+        std::cout << "Number of matches: 0" << std::endl;
+        return 0;
+    }
+    std::cout << "Filtering time (s): " << seconds_since(t0) << std::endl;
+
+    if (!csDump.empty()) {
+        std::ofstream os(csDump);
+        for (VertexID u = 0; u < q.getNumVertices(); ++u) {
+            os << "C " << u << " " << cs.candidateSet[u].size();
+            for (VertexID v : cs.candidateSet[u]) os << " " << v;
+            os << "\n";
+        }
+        cs.writeToStream(os);
+    }
+
+    cs.setQueryGraphWeights(q);
+    t0 = std::chrono::steady_clock::now();
+    FHD fhd;
+    q.buildFHD(fhd);
+    HyperTree t;
+    t.buildFromTD(fhd);
+    double fhdTime = seconds_since(t0);
+    std::cout << "FHD time (s): " << fhdTime << std::endl;
+
+    std::vector<std::vector<VertexID>> result;
+    bool *visited = new bool[g.getNumVertices()];
+    std::memset(visited, 0, sizeof(bool) * g.getNumVertices());
+    VertexID *partMatch = new VertexID[q.getNumVertices()];
+    VertexID **candidates = new VertexID *[q.getNumVertices()];
+    const ui maxSize = cs.getMaxSize();
+    for (ui i = 0; i < q.getNumVertices(); ++i) candidates[i] = new VertexID[maxSize];
+    ui *candCount = new ui[q.getNumVertices()];
+    std::memset(candCount, 0, sizeof(ui) * q.getNumVertices());
+
+    reorderBags(q, t);
+    // Harness difference 1: size the trie roots after the global bag exists.
+    std::vector<TrieNode *> nodes(t.numNodes);
+    for (ui i = 0; i < t.numNodes; ++i) nodes[i] = new TrieNode();
+
+    std::vector<SubsetStructure> dp;
+    ui numNodes = t.numNodes;
+    if (t.newGlobalNode) --numNodes;
+    double cardTime = 0.0;
+    if (cardPath.empty()) {
+        smallCard(q, cs);
+        dp.resize(numNodes);
+        t0 = std::chrono::steady_clock::now();
+        for (VertexID nID = 0; nID < numNodes; ++nID) {
+            std::vector<VertexID> local(t.nodes[nID].attributes,
+                                        t.nodes[nID].attributes + t.nodes[nID].numAttributes);
+            SubsetStructure s(local, q, false);
+            s.optimalPlanDP(q, cs, visited, partMatch, candidates, candCount);
+            s.reverseDP(q, cs);
+            dp[nID] = s;
+        }
+        cardTime = seconds_since(t0);
+    } else {
+        std::ifstream ifs(cardPath, std::ios::binary);
+        dp.resize(numNodes);
+        for (VertexID nID = 0; nID < numNodes; ++nID) dp[nID].readFromStream(ifs);
+        if (!loadSubsetToCard(ifs)) return 1;
+        int scaled = 0;
+        ifs.read(reinterpret_cast<char *>(&scaled), sizeof(int));
+        cardTime = scaled / 10000.0;
+    }
+    cardTime += fhdTime;
+
+    bool traverseAll = false;
+#if defined(ALL_LEVEL) || defined(COLLECT_RESULT)
+    traverseAll = true;
+#endif
+#ifdef LOCAL_COUNT
+    gLocalCount = std::vector<std::vector<size_t>>(g.getNumVertices(),
+                                                   std::vector<size_t>(q.getNumVertices(), 0));
+#endif
+    PrefixNode *pt = nullptr;
+    double minCost = 0.0;
+    t0 = std::chrono::steady_clock::now();
+    if (numNodes != 1)
+        optCostPlan(q, t, cs, pt, dp, minCost, 1, true, false);
+    else
+        simplePlan(q, t, cs, pt, dp, visited, partMatch, candidates, candCount, minCost, nullptr, false);
+    std::cout << "Planning Time: " << seconds_since(t0) + cardTime << std::endl;
+    std::cout << "cost: " << minCost << std::endl;
+
+    size_t count = 0;
+    t0 = std::chrono::steady_clock::now();
+    adaptiveShareJoin(q, t, pt, cs, nodes, visited, result, count, traverseAll, budget, false);
+    std::cout << "Execution Time: " << seconds_since(t0) << std::endl;
+    std::cout << "Number of matches: " << count << std::endl;
+    std::cout << "Number of intersections: " << gNumInterSection << std::endl;
+
+#ifdef LOCAL_COUNT
+    const std::string csvPath = cmd.getCountPath();
+    if (!csvPath.empty()) {
+        std::ofstream os(csvPath);
+        for (VertexID v = 0; v < g.getNumVertices(); ++v) {
+            for (VertexID u = 0; u < q.getNumVertices(); ++u) {
+                os << gLocalCount[v][u];
+                if (u + 1 != q.getNumVertices()) os << ",";
+            }
+            os << "\n";
+        }
+    }
+#endif
+#ifdef COLLECT_RESULT
+    if (!embDump.empty()) {
+        std::sort(result.begin(), result.end());
+        std::ofstream os(embDump);
+        storeMatches(result, os);
+    }
+#endif
+    return 0;
+}

@@ -1,0 +1,60 @@
+"""The CPU oracle against the reference's golden vectors (and, where the
+reference build exists in this container, against the reference live)."""
+import os
+
+import pytest
+
+import oracle_util as O
+
+YEAST = "/root/reference/dataset/yeast.tar.gz"
+
+
+def _check(rec, qpath, dpath, tmp_path, full):
+    cs = str(tmp_path / "cs.txt")
+    csv = str(tmp_path / "l.csv") if full else None
+    emb = str(tmp_path / "e.txt") if full else None
+    mode = O.MODE_EMBED if full else O.MODE_COUNT
+    count, flags = O.oracle_run(qpath, dpath, mode, csv=csv, emb=emb, cs=cs)
+    assert count == rec["count"], qpath
+    if rec.get("cs_sha") is not None and rec["count"] > 0:
+        assert O.sha256_file(cs) == rec["cs_sha"], qpath
+    if full:
+        assert O.sha256_file(csv) == rec["csv_sha"], qpath
+        assert O.sha256_file(emb) == rec["emb_sha"], qpath
+
+
+def test_oracle_c0_counts_and_candidate_spaces(golden, c0_files, tmp_path):
+    _, dpath, _, qpaths = c0_files
+    for rec in golden["sets"]["c0"]:
+        _check(rec, qpaths[rec["index"]], dpath, tmp_path, "csv_sha" in rec)
+
+
+def test_oracle_c0d(golden, c0d_files, tmp_path):
+    _, dpath, by_size = c0d_files
+    for rec in golden["sets"]["c0d"]:
+        if rec["count"] > 3_000_000 and "csv_sha" not in rec:
+            continue  # keep the CPU suite short; the GPU suite covers these
+        _check(rec, by_size[rec["size"]][1][rec["index"]], dpath, tmp_path, "csv_sha" in rec)
+
+
+def test_oracle_edge_cases(golden, c0_files, edge_files, tmp_path):
+    _, dpath, _, _ = c0_files
+    for rec in golden["sets"]["edge"]:
+        _check(rec, edge_files[rec["name"]][1], dpath, tmp_path, "csv_sha" in rec)
+
+
+@pytest.mark.skipif(not (os.path.exists(YEAST) and O.ref_available()), reason="needs the reference tree and oracle/_ref")
+def test_oracle_matches_reference_on_yeast(tmp_path):
+    import tarfile
+    with tarfile.open(YEAST) as t:
+        t.extractall(tmp_path)
+    base = tmp_path / "yeast"
+    dpath = str(base / "data_graph" / "yeast.graph")
+    for size, idx in ((8, range(1, 21)), (12, range(1, 6)), (16, range(1, 4))):
+        for i in idx:
+            q = str(base / "query_graph" / ("query_%d_%d.graph" % (size, i)))
+            rcs, ocs = str(tmp_path / "r.txt"), str(tmp_path / "o.txt")
+            r = O.ref_run("ref_count", q, dpath, cs=rcs)
+            c, _ = O.oracle_run(q, dpath, O.MODE_COUNT, cs=ocs)
+            assert c == r, q
+            assert O.sha256_file(rcs) == O.sha256_file(ocs), q

@@ -1,0 +1,191 @@
+"""GPU parity: the device candidate space, counts, local-count CSVs and
+embedding sets against the reference's golden vectors, plus the
+size-independent properties (plan invariance, consistency between modes)."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import asdmatch_b200 as A
+
+pytestmark = pytest.mark.gpu
+
+
+def csv_sha(local):
+    text = "".join(",".join(str(int(x)) for x in row) + "\n" for row in local)
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def emb_sha(emb):
+    text = "%d\n" % len(emb) + "".join("".join("%d " % int(x) for x in row) + "\n" for row in emb)
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def dg_c0(c0_files):
+    dg = A.DeviceGraph(c0_files[0])
+    yield dg
+    dg.close()
+
+
+@pytest.fixture(scope="module")
+def dg_c0d(c0d_files):
+    dg = A.DeviceGraph(c0d_files[0])
+    yield dg
+    dg.close()
+
+
+def test_candidate_space_matches_reference_dump(golden, c0_files, dg_c0):
+    _, _, qs, _ = c0_files
+    for rec in golden["sets"]["c0"][:80]:
+        cs = A.CandidateSpace(dg_c0, qs[rec["index"]])
+        if rec["cs_sha"] is None:
+            assert not cs.build_cand_cfl()
+            continue
+        assert cs.build_cand_cfl()
+        assert hashlib.sha256(cs.write_to_stream().encode()).hexdigest() == rec["cs_sha"], rec["index"]
+        cs.close()
+
+
+def test_candidate_space_c0d(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    for rec in golden["sets"]["c0d"][::4]:
+        cs = A.CandidateSpace(dg_c0d, by_size[rec["size"]][0][rec["index"]])
+        assert hashlib.sha256(cs.write_to_stream().encode()).hexdigest() == rec["cs_sha"], rec
+        cs.close()
+
+
+def test_counts_c0(golden, c0_files, dg_c0):
+    _, _, qs, _ = c0_files
+    for rec in golden["sets"]["c0"]:
+        assert A.match(dg_c0, qs[rec["index"]]).count == rec["count"], rec["index"]
+
+
+def test_counts_c0d(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    for rec in golden["sets"]["c0d"]:
+        assert A.match(dg_c0d, by_size[rec["size"]][0][rec["index"]]).count == rec["count"], rec
+
+
+def test_local_counts_and_embeddings_c0(golden, c0_files, dg_c0):
+    _, _, qs, _ = c0_files
+    checked = 0
+    for rec in golden["sets"]["c0"]:
+        if "csv_sha" not in rec:
+            continue
+        r = A.match(dg_c0, qs[rec["index"]], mode=A.MODE_LOCAL | A.MODE_EMBED)
+        assert r.count == rec["count"]
+        assert csv_sha(r.local_counts) == rec["csv_sha"], rec["index"]
+        assert emb_sha(r.embeddings) == rec["emb_sha"], rec["index"]
+        checked += 1
+    assert checked >= 30
+
+
+def test_local_counts_and_embeddings_c0d(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    for rec in golden["sets"]["c0d"]:
+        if "csv_sha" not in rec:
+            continue
+        r = A.match(dg_c0d, by_size[rec["size"]][0][rec["index"]], mode=A.MODE_LOCAL | A.MODE_EMBED)
+        assert csv_sha(r.local_counts) == rec["csv_sha"], rec
+        assert emb_sha(r.embeddings) == rec["emb_sha"], rec
+
+
+def test_edge_cases(golden, dg_c0, edge_files):
+    for rec in golden["sets"]["edge"]:
+        q = edge_files[rec["name"]][0]
+        r = A.match(dg_c0, q, mode=A.MODE_LOCAL | A.MODE_EMBED)
+        assert r.count == rec["count"], rec["name"]
+        if "csv_sha" in rec:
+            assert csv_sha(r.local_counts) == rec["csv_sha"], rec["name"]
+            assert emb_sha(r.embeddings) == rec["emb_sha"], rec["name"]
+
+
+def _random_connected_order(q, rng):
+    n = q.n
+    start = int(rng.integers(n))
+    order, seen = [start], {start}
+    while len(order) < n:
+        frontier = sorted({int(w) for u in order for w in q.nbrs[q.offsets[u]:q.offsets[u + 1]]} - seen)
+        nxt = frontier[int(rng.integers(len(frontier)))]
+        order.append(nxt)
+        seen.add(nxt)
+    return order
+
+
+def test_count_is_plan_invariant(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    rng = np.random.default_rng(5)
+    for rec in golden["sets"]["c0d"][40:56]:
+        q = by_size[rec["size"]][0][rec["index"]]
+        for _ in range(3):
+            order = _random_connected_order(q, rng)
+            assert A.match(dg_c0d, q, order=order).count == rec["count"], (rec, order)
+
+
+def test_local_count_columns_sum_to_count(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    for rec in golden["sets"]["c0d"][40:50]:
+        r = A.match(dg_c0d, by_size[rec["size"]][0][rec["index"]], mode=A.MODE_LOCAL)
+        assert r.count == rec["count"]
+        assert all(int(s) == rec["count"] for s in r.local_counts.sum(axis=0, dtype=np.uint64))
+
+
+def test_count_query_and_batch_entry_points(golden, c0_files, dg_c0):
+    _, _, qs, _ = c0_files
+    recs = golden["sets"]["c0"][:50]
+    for rec in recs[:10]:
+        assert A.count_query(dg_c0, qs[rec["index"]]).count == rec["count"]
+    counts, status = A.run_batch(dg_c0, [qs[r["index"]] for r in recs])
+    assert status.tolist() == [0] * len(recs)
+    assert counts.tolist() == [r["count"] for r in recs]
+
+
+def test_leapfrog_join_matches_numpy():
+    rng = np.random.default_rng(0)
+    sets = []
+    for k in (1, 2, 3, 5, 8, 31):
+        for ratio in (1, 10, 1000):
+            lists = []
+            for j in range(k):
+                n = int(rng.integers(0, 50)) * (ratio if j == 0 else 1) + (1 if j else 0)
+                lists.append(np.unique(rng.integers(0, 4000, size=n)).astype(np.uint32))
+            sets.append(lists)
+    sets.append([np.zeros(0, np.uint32), np.arange(10, dtype=np.uint32)])
+    sets.append([])
+    out = A.leapfrog_join(sets)
+    for lists, got in zip(sets, out):
+        if not lists:
+            assert len(got) == 0
+            continue
+        want = lists[0]
+        for l in lists[1:]:
+            want = np.intersect1d(want, l)
+        assert np.array_equal(got, want)
+
+
+def test_time_limit_returns_status_and_device_stays_usable(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    rec = max(golden["sets"]["c0d"], key=lambda r: r["count"])
+    q = by_size[rec["size"]][0][rec["index"]]
+    with pytest.raises(A.AsdmError) as e:
+        A.match(dg_c0d, q, time_limit_s=1e-7)
+    assert e.value.code == A.ERR_TIMEOUT
+    assert A.match(dg_c0d, q).count == rec["count"]
+
+
+def test_bad_queries_are_rejected(dg_c0):
+    # asymmetric adjacency / unsorted neighbour list / oversized query
+    q = A.HostGraph.from_edges(3, [0, 0, 0], [(0, 1), (1, 2)])
+    bad = q.nbrs.copy()
+    bad[0], bad[1] = bad[1], bad[0]
+    with pytest.raises(A.AsdmError) as e:
+        A._check(A._cs_build(dg_c0._h, A._ptr(q.offsets), A._ptr(np.ascontiguousarray(q.nbrs[::-1])),
+                             A._ptr(q.labels), q.n, A.C.byref(A._vp()), A.C.byref(A.C.c_int())))
+    assert e.value.code == A.ERR_INVALID
+
+
+def test_disconnected_query_has_no_candidates(dg_c0):
+    q = A.HostGraph.from_edges(4, [0, 0, 0, 0], [(0, 1), (2, 3)])
+    r = A.match(dg_c0, q)
+    assert r.count == 0 and not r.nonempty
