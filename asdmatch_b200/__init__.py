@@ -26,11 +26,11 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libasdm_b200.so")
 BIN_DIR = os.path.join(_PKG, "bin")
 
-OK, ERR_INVALID, ERR_IO, ERR_CUDA, ERR_OOM, ERR_OVERFLOW, ERR_TIMEOUT, ERR_CAPACITY, ERR_INTERNAL = range(9)
+OK, ERR_INVALID, ERR_IO, ERR_CUDA, ERR_OOM, ERR_OVERFLOW, ERR_TIMEOUT, ERR_CAPACITY, ERR_INTERNAL, ERR_LIMIT = range(10)
 MODE_COUNT, MODE_LOCAL, MODE_EMBED = 0, 1, 2
 
 _ERR_NAMES = {ERR_INVALID: "invalid", ERR_IO: "io", ERR_CUDA: "cuda", ERR_OOM: "oom", ERR_OVERFLOW: "overflow",
-              ERR_TIMEOUT: "timeout", ERR_CAPACITY: "capacity", ERR_INTERNAL: "internal"}
+              ERR_TIMEOUT: "timeout", ERR_CAPACITY: "capacity", ERR_INTERNAL: "internal", ERR_LIMIT: "limit"}
 
 
 class AsdmError(RuntimeError):
@@ -50,7 +50,8 @@ _vp = C.c_void_p
 
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("budget_bytes", C.c_uint64), ("time_limit_s", C.c_double),
-                ("local_counts", _u64p), ("embeddings", _u32p), ("emb_capacity", C.c_uint64)]
+                ("local_counts", _u64p), ("embeddings", _u32p), ("emb_capacity", C.c_uint64),
+                ("count_limit", C.c_uint64)]
 
 
 class RunStats(C.Structure):
@@ -75,6 +76,8 @@ _hg_write = _sig("asdm_host_graph_write", C.c_int, [_vp, C.c_char_p])
 _hg_free = _sig("asdm_host_graph_free", None, [_vp])
 _gen_cl = _sig("asdm_gen_chung_lu", C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_uint32, C.c_double, C.c_uint64,
                                               C.POINTER(_vp)])
+_gen_clc = _sig("asdm_gen_chung_lu_capped", C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_uint32, C.c_double,
+                                                      C.c_double, C.c_uint64, C.POINTER(_vp)])
 _gen_q = _sig("asdm_gen_query", C.c_int, [_vp, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_vp)])
 _g_upload = _sig("asdm_graph_upload", C.c_int, [_u32p, _u32p, _u32p, C.c_uint32, C.c_uint64, C.c_uint32,
                                                 C.POINTER(_vp)])
@@ -92,6 +95,9 @@ _plan_free = _sig("asdm_plan_free", C.c_int, [_vp])
 _run_plan = _sig("asdm_run_plan", C.c_int, [_vp, _vp, C.POINTER(RunOpts), C.POINTER(RunStats)])
 _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(RunOpts),
                                                   C.POINTER(RunStats)])
+_launches = _sig("asdm_kernel_launches", C.c_uint64, [])
+_g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
+_cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
 _run_batch = _sig("asdm_run_batch", C.c_int, [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p,
                                               C.c_double, _u64p, C.POINTER(C.c_int)])
 
@@ -108,6 +114,11 @@ def _ptr(a: np.ndarray, ty=_u32p):
 
 def version() -> str:
     return _version().decode()
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched so far in this process."""
+    return int(_launches())
 
 
 class HostGraph:
@@ -140,9 +151,14 @@ class HostGraph:
         return cls(h.value)
 
     @classmethod
-    def chung_lu(cls, n: int, m: int, gamma: float, nlabels: int, zipf_s: float, seed: int) -> "HostGraph":
+    def chung_lu(cls, n: int, m: int, gamma: float, nlabels: int, zipf_s: float, seed: int,
+                 wmax: float = 0.0) -> "HostGraph":
+        """Seeded Chung-Lu graph; wmax is the largest expected degree (0: sqrt(2m))."""
         h = _vp()
-        _check(_gen_cl(n, m, gamma, nlabels, zipf_s, seed, C.byref(h)), "chung_lu")
+        if wmax > 0:
+            _check(_gen_clc(n, m, gamma, nlabels, zipf_s, wmax, seed, C.byref(h)), "chung_lu")
+        else:
+            _check(_gen_cl(n, m, gamma, nlabels, zipf_s, seed, C.byref(h)), "chung_lu")
         return cls(h.value)
 
     def random_walk_query(self, size: int, seed: int, density: int = 0) -> "HostGraph":
@@ -185,6 +201,12 @@ class DeviceGraph:
         self.n = g.n
         self.host = g
 
+    def stream(self) -> int:
+        """cudaStream_t (as an int) the library uses for this graph."""
+        s = _vp()
+        _check(_g_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def close(self):
         if self._h is not None and self._h.value:
             _g_free(self._h)
@@ -213,6 +235,12 @@ class CandidateSpace:
     def build_cand_cfl(self) -> bool:
         """The reference's return value: False when some candidate set is empty."""
         return self.nonempty
+
+    def build_stats(self):
+        """(algorithmic bytes, device ms) of the candidate-space build."""
+        b, ms = C.c_uint64(), C.c_double()
+        _check(_cs_stats(self._h, C.byref(b), C.byref(ms)))
+        return b.value, ms.value
 
     def sizes(self) -> np.ndarray:
         out = np.zeros(self.q.n, np.uint32)
@@ -304,13 +332,15 @@ class MatchResult:
 
 
 def adaptive_share_join(cs: CandidateSpace, plan: Optional[Plan] = None, mode: int = MODE_COUNT,
-                        emb_capacity: int = 0, budget_bytes: int = 0, time_limit_s: float = 0.0) -> MatchResult:
+                        emb_capacity: int = 0, budget_bytes: int = 0, time_limit_s: float = 0.0,
+                        count_limit: int = 0) -> MatchResult:
     """Exact enumeration of one query: count, local counts (MODE_LOCAL), embeddings (MODE_EMBED)."""
     n = cs.q.n
     opts = RunOpts()
     opts.mode = mode
     opts.budget_bytes = budget_bytes
     opts.time_limit_s = time_limit_s
+    opts.count_limit = count_limit
     local = emb = None
     if mode & MODE_LOCAL:
         local = np.zeros((cs.dg.n, n), np.uint64)
@@ -346,11 +376,12 @@ def match(dg: DeviceGraph, q: HostGraph, mode: int = MODE_COUNT, order: Optional
         cs.close()
 
 
-def count_query(dg: DeviceGraph, q: HostGraph, time_limit_s: float = 0.0) -> MatchResult:
+def count_query(dg: DeviceGraph, q: HostGraph, time_limit_s: float = 0.0, count_limit: int = 0) -> MatchResult:
     """One-call count (asdm_count_query)."""
     opts = RunOpts()
     opts.mode = MODE_COUNT
     opts.time_limit_s = time_limit_s
+    opts.count_limit = count_limit
     st = RunStats()
     _check(_count_query(dg._h, _ptr(q.offsets), _ptr(q.nbrs), _ptr(q.labels), q.n, C.byref(opts), C.byref(st)),
            "count")

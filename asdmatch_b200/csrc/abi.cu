@@ -1,6 +1,7 @@
 // Remaining C-ABI entry points: batched set intersection (K4 as a standalone
 // primitive), the multi-query front end and the version string.
 #include <algorithm>
+#include <atomic>
 #include <memory>
 
 #include "cs.cuh"
@@ -73,7 +74,27 @@ __global__ void __launch_bounds__(256) intersect_kernel(const uint32_t *__restri
 }  // namespace
 }  // namespace asdm
 
+namespace asdm {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace asdm
+
 using namespace asdm;
+
+extern "C" uint64_t asdm_kernel_launches(void) { return asdm::g_launches.load(); }
+
+extern "C" int asdm_graph_stream(asdm_graph *g, void **stream) {
+    if (!g || !stream) return fail(ASDM_ERR_INVALID, "null argument");
+    *stream = (void *)g->stream;
+    return ASDM_OK;
+}
+
+extern "C" int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms) {
+    if (!cs) return fail(ASDM_ERR_INVALID, "null argument");
+    if (build_bytes) *build_bytes = cs->build_bytes;
+    if (build_ms) *build_ms = cs->build_ms;
+    return ASDM_OK;
+}
 
 extern "C" const char *asdm_version(void) { return "asdmatch-b200 0.1 (sm_100a)"; }
 
@@ -119,6 +140,7 @@ extern "C" int asdm_intersect_batch(const uint32_t *values, const uint64_t *list
         }
         const unsigned grid = (unsigned)std::min<uint64_t>((nsets + 7) / 8, (uint64_t)sms * 16);
         intersect_kernel<<<grid, 256, 0, s>>>(d_vals, d_loff, d_first, nsets, d_ooff, d_out, d_cnt);
+        ::asdm::count_launch();
         if (cudaGetLastError() != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "intersection launch failed");
             break;

@@ -327,9 +327,11 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, std::vector<uint32
     ASDM_CUDA(cudaMemcpyAsync(d_tf, tile_first.data(), (nseg + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     ASDM_CUDA(cudaMemsetAsync(d_sc, 0, nseg * sizeof(uint32_t), s));
     k3_count<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_cnt);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     ASDM_TRY(scan_exclusive_u32(d_cnt, d_pos, ntiles, true, s));
     k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, d_sc);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     ASDM_CUDA(cudaMemcpyAsync(sizes.data(), d_sc, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     ASDM_CUDA(cudaStreamSynchronize(s));
@@ -352,6 +354,7 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     ASDM_CUDA(cudaMemcpyAsync(d_p, passes.data(), np * sizeof(PassDesc), cudaMemcpyHostToDevice, s));
     ASDM_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), (np + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, d_elems);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     dfree(d_p, s);
     dfree(d_prefix, s);
@@ -426,6 +429,7 @@ int build(asdm_cs &cs) {
     if (seg[nq]) {
         FilterArgs fa{g, st, d_seg, d_small, d_small + nq, d_small + 2 * nq, d_small + 2 * nq + qnlc.size(), nq, d_fcount};
         k1_filter<<<grid_for(seg[nq], G->num_sms), kBlock, 0, s>>>(fa);
+        ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
     }
     std::vector<uint32_t> fcount(nq, 0);
@@ -587,6 +591,7 @@ int build(asdm_cs &cs) {
             ASDM_CUDA(cudaMemcpyAsync(d_maps, &maps[u], sizeof(uint32_t *), cudaMemcpyHostToDevice, s));
             k3_scatter_map<<<grid_for(cs.ncand[u], G->num_sms), kBlock, 0, s>>>(cs.d_cand + cs.cand_base[u], d_one, 1,
                                                                                d_maps, g.pos_in_label);
+            ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         }
     }
@@ -614,6 +619,7 @@ int build(asdm_cs &cs) {
     ASDM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), s));
     const unsigned egrid = grid_for(nitems, G->num_sms);
     k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, cs.d_eoff, nullptr, nullptr, d_elems + 1);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     ASDM_TRY(scan_exclusive_u32(cs.d_eoff, d_wpos, nitems, true, s));
     uint64_t total = 0;
@@ -621,8 +627,10 @@ int build(asdm_cs &cs) {
     ASDM_CUDA(cudaStreamSynchronize(s));
     ASDM_TRY(dalloc(&cs.d_elist, total, s));
     k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, cs.d_elist, nullptr);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, cs.d_eoff, d_estart, d_bad);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     std::vector<uint64_t> estart(ne, 0);
     uint32_t bad = 0;

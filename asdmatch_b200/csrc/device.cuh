@@ -111,6 +111,9 @@ void dfree(T *&p, cudaStream_t s) {
 
 int device_setup(int *device, int *num_sms);
 
+// Number of kernels this library has launched (all threads, all devices).
+void count_launch();
+
 }  // namespace asdm
 
 struct asdm_graph {

@@ -39,8 +39,17 @@ constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr uint32_t kFull = 0xffffffffu;
 
-enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4 };
-enum : int { kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5, kCtrN = 8 };
+enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4, kFlagInternal = 8, kFlagLimit = 16 };
+constexpr uint32_t kStopFlags = kFlagOverflow | kFlagTimeout | kFlagInternal | kFlagLimit;
+enum : int {
+    kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5,
+    kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrN = 16
+};
+// Work-donation ring (a bounded multi-producer multi-consumer queue with a
+// sequence number per slot): a record is [level s, lo, hi, idx[0..s-1]].
+constexpr uint32_t kRecWords = 3 + 32;
+constexpr uint64_t kQueueCap = 1u << 16;      // power of two
+constexpr uint32_t kIdlePolls = 1u << 20;     // an idle warp gives up after this many polls
 
 struct DLevel {
     const uint32_t *cand;  // C(u)
@@ -75,9 +84,12 @@ struct EnumArgs {
     uint32_t *rows;             // row_cap x nq, MODE_EMBED
     uint64_t row_cap;
     uint64_t limit_ns;          // 0 = none; else per-warp wall-clock budget
+    unsigned long long count_limit;  // 0 = none
+    uint32_t *queue;            // kQueueCap records of kRecWords words
+    unsigned long long *qseq;   // kQueueCap slot sequence numbers
 };
 
-__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 38 * n + 3 * nb; }
+__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb; }
 
 __host__ __device__ inline uint32_t plan_words(uint32_t n, uint32_t nb, uint32_t nc) {
     return (uint32_t)((n * sizeof(DLevel) + nb * sizeof(DBack)) / 4) + ((nc + 3) & ~3u);
@@ -113,7 +125,7 @@ struct Warp {
     const DLevel *L;
     const DBack *B;
     const uint32_t *CF;
-    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *drv, *sstart, *slen, *scur;
+    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur;
     uint32_t lane;
     unsigned long long count = 0, inter = 0, elems = 0;
     bool overflow = false;
@@ -127,7 +139,8 @@ struct Warp {
         cnt = buf + 32 * n;
         pos = cnt + n;
         dpos = pos + n;
-        drv = dpos + n;
+        dend = dpos + n;
+        drv = dend + n;
         sstart = drv + n;
         slen = sstart + a.nb;
         scur = slen + a.nb;
@@ -137,6 +150,20 @@ struct Warp {
         const unsigned long long nc = count + c;
         overflow |= nc < count;
         count = nc;
+    }
+
+    // Moves this warp's count into the global total (lane 0), checking for
+    // uint64 wrap-around and the caller's count limit.
+    __device__ void flush_count() {
+        if (lane == 0 && (count || overflow)) {
+            const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], count);
+            uint32_t f = 0;
+            if (overflow || old + count < old) f |= kFlagOverflow;
+            if (a.count_limit && old + count > a.count_limit) f |= kFlagLimit;
+            if (f) atomicOr((unsigned int *)&a.ctr[kCtrFlags], f);
+        }
+        count = 0;
+        overflow = false;
     }
 
     // Loads the candidate-edge lists of level d's earlier neighbours into the
@@ -167,11 +194,90 @@ struct Warp {
         if (lane == 0) {
             drv[d] = who;
             dpos[d] = 0;
+            dend[d] = key;
             cnt[d] = 0;
             pos[d] = 0;
         }
         __syncwarp();
         return key;
+    }
+
+    // Gives the upper half of the undispatched driver range of the shallowest
+    // open level to the donation ring (called when more warps are idle than
+    // records are waiting).
+    __device__ void try_donate(uint32_t base, uint32_t d) {
+        uint32_t s = kNone;
+        for (uint32_t l = base; l <= d; ++l)
+            if (dend[l] > dpos[l]) { s = l; break; }
+        if (s == kNone) return;
+        unsigned long long pos = ~0ull;
+        if (lane == 0) {
+            volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
+            unsigned long long p = vc[kCtrTail];
+            for (int tries = 0; tries < 64; ++tries) {
+                const unsigned long long seq = *(volatile unsigned long long *)&a.qseq[p & (kQueueCap - 1)];
+                if (seq == p) {
+                    const unsigned long long prev = atomicCAS(&a.ctr[kCtrTail], p, p + 1);
+                    if (prev == p) { pos = p; break; }
+                    p = prev;
+                } else if (seq < p) {
+                    break;  // ring full
+                } else {
+                    p = vc[kCtrTail];
+                }
+            }
+        }
+        pos = __shfl_sync(kFull, pos, 0);
+        if (pos == ~0ull) return;
+        const uint32_t lo = dpos[s] + (dend[s] - dpos[s]) / 2, hi = dend[s];
+        uint32_t *rec = a.queue + (pos & (kQueueCap - 1)) * kRecWords;
+        if (lane < s) rec[3 + lane] = idx[lane];
+        if (lane == 0) {
+            rec[0] = s;
+            rec[1] = lo;
+            rec[2] = hi;
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+            atomicExch(&a.qseq[pos & (kQueueCap - 1)], pos + 1);
+            atomicAdd(&a.ctr[kCtrDonated], 1ull);
+            dend[s] = lo;
+        }
+        __syncwarp();
+    }
+
+    // Idle: polls the donation ring.  Returns the claimed position, or ~0
+    // when no warp is working any more (or the poll budget ran out).  The
+    // caller copies the record and then calls release().
+    __device__ unsigned long long take_queued() {
+        unsigned long long pos = ~0ull;
+        if (lane == 0) {
+            volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
+            atomicAdd(&a.ctr[kCtrIdle], 1ull);
+            for (uint32_t it = 0; it < kIdlePolls; ++it) {
+                const unsigned long long p = vc[kCtrHead];
+                const unsigned long long seq = *(volatile unsigned long long *)&a.qseq[p & (kQueueCap - 1)];
+                if (seq == p + 1) {
+                    if (atomicCAS(&a.ctr[kCtrHead], p, p + 1) == p) { pos = p; break; }
+                } else if (seq < p + 1) {
+                    if (vc[kCtrActive] == 0 || (vc[kCtrFlags] & kStopFlags)) break;
+                    __nanosleep(256);
+                }
+            }
+            if (pos != ~0ull) atomicAdd(&a.ctr[kCtrActive], 1ull);
+            atomicAdd(&a.ctr[kCtrIdle], ~0ull);
+            __threadfence();
+        }
+        return __shfl_sync(kFull, pos, 0);
+    }
+
+    __device__ void release(unsigned long long pos) {
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            atomicExch(&a.qseq[pos & (kQueueCap - 1)], pos + kQueueCap);
+        }
     }
 
     // Membership of x (this lane's driver element) in every non-driver list
@@ -206,7 +312,7 @@ struct Warp {
         const DLevel lv = L[d];
         const uint32_t dslot = lv.back_first + drv[d];
         const uint32_t *dl = B[dslot].list + sstart[dslot];
-        const uint32_t dlen = slen[dslot];
+        const uint32_t dlen = dend[d];
         const uint32_t p0 = dpos[d];
         const uint32_t p = p0 + lane;
         const bool valid = p < dlen;
@@ -334,37 +440,49 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
     const uint32_t n = a.n;
     volatile unsigned int *flags = reinterpret_cast<volatile unsigned int *>(&a.ctr[kCtrFlags]);
     uint32_t iter = 0;
-    bool stop = false;
+    bool stop = false, roots_left = true;
     uint64_t deadline = 0;
     if (a.limit_ns && lane == 0) deadline = globaltimer() + a.limit_ns;
     while (!stop) {
-        unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(&a.ctr[kCtrTask], 1ull);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= a.ntasks) break;
-        uint32_t i0, i1 = 0;
-        if (n == 1) {
-            i0 = (uint32_t)t;
-        } else {
-            i0 = warp_find_row(a.off01, a.n0, t, lane);
-            i1 = a.list01[t];
-        }
-        if (lane == 0) {
-            W.idx[0] = i0;
-            W.vid[0] = L[0].cand[i0];
-            if (n > 1) {
-                W.idx[1] = i1;
-                W.vid[1] = L[1].cand[i1];
+        uint32_t base = 2;
+        bool have = false;
+        if (roots_left) {
+            unsigned long long t = 0;
+            if (lane == 0) {
+                atomicAdd(&a.ctr[kCtrActive], 1ull);
+                t = atomicAdd(&a.ctr[kCtrTask], 1ull);
+                if (t >= a.ntasks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+            }
+            t = __shfl_sync(kFull, t, 0);
+            if (t < a.ntasks) {
+                have = true;
+                uint32_t i0, i1 = 0;
+                if (n == 1) {
+                    i0 = (uint32_t)t;
+                } else {
+                    i0 = warp_find_row(a.off01, a.n0, t, lane);
+                    i1 = a.list01[t];
+                }
+                if (lane == 0) {
+                    W.idx[0] = i0;
+                    W.vid[0] = L[0].cand[i0];
+                    if (n > 1) {
+                        W.idx[1] = i1;
+                        W.vid[1] = L[1].cand[i1];
+                    }
+                }
+                __syncwarp();
+            } else {
+                roots_left = false;
             }
         }
-        __syncwarp();
-        if (n <= 2) {
-            W.single(n - 1);
-            continue;
-        }
         uint32_t d = 2;
-        // enter level 2
-        {
+        if (have) {
+            if (n <= 2) {
+                W.single(n - 1);
+                if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+                continue;
+            }
             const uint32_t len = W.setup(d);
             if (d == n - 1) {
                 if (len) W.leaf(d);
@@ -372,18 +490,43 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
             } else if (len == 0) {
                 d = 1;
             }
+        } else {
+            const unsigned long long qpos = W.take_queued();
+            if (qpos == ~0ull) break;
+            const volatile uint32_t *rec = a.queue + (qpos & (kQueueCap - 1)) * kRecWords;
+            base = rec[0];
+            const uint32_t lo = rec[1], hi = rec[2];
+            if (lane < base) {
+                const uint32_t x = rec[3 + lane];
+                W.idx[lane] = x;
+                W.vid[lane] = L[lane].cand[x];
+            }
+            W.release(qpos);
+            __syncwarp();
+            d = base;
+            W.setup(d);
+            if (lane == 0) {
+                W.dpos[d] = lo;
+                W.dend[d] = hi;
+            }
+            __syncwarp();
         }
-        while (d >= 2) {
+        while (d >= base) {
             if ((++iter & 63u) == 0) {
-                uint32_t s = 0;
+                uint32_t st = 0, want = 0;
+                W.flush_count();
                 if (lane == 0) {
-                    s = *flags & (kFlagOverflow | kFlagTimeout);
-                    if (!s && deadline && globaltimer() > deadline) {
+                    st = *flags & kStopFlags;
+                    if (!st && deadline && globaltimer() > deadline) {
                         atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagTimeout);
-                        s = kFlagTimeout;
+                        st = kFlagTimeout;
                     }
+                    volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
+                    const unsigned long long idle = vc[kCtrIdle], pend = vc[kCtrTail] - vc[kCtrHead];
+                    want = idle > pend && (long long)pend >= 0;
                 }
-                if (__shfl_sync(kFull, s, 0)) { stop = true; break; }
+                if (__shfl_sync(kFull, st, 0)) { stop = true; break; }
+                if (__shfl_sync(kFull, want, 0)) W.try_donate(base, d);
             }
             if (W.pos[d] < W.cnt[d]) {
                 const uint32_t x = W.buf[32 * d + W.pos[d]];
@@ -404,21 +547,25 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
                 }
                 continue;
             }
-            if (W.dpos[d] < W.slen[L[d].back_first + W.drv[d]]) {
+            if (W.dpos[d] < W.dend[d]) {
                 W.fill_chunk(d);
                 continue;
             }
             --d;
         }
+        if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
     }
     // flush per-warp totals
-    unsigned long long c = W.count, in = W.inter, el = W.elems;
+    W.flush_count();
     if (lane == 0) {
-        const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], c);
-        if (W.overflow || old + c < old) atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagOverflow);
-        atomicAdd(&a.ctr[kCtrInter], in);
-        atomicAdd(&a.ctr[kCtrElems], el);
+        atomicAdd(&a.ctr[kCtrInter], W.inter);
+        atomicAdd(&a.ctr[kCtrElems], W.elems);
     }
+}
+
+__global__ void queue_init(unsigned long long *seq) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kQueueCap) seq[i] = i;
 }
 
 template <uint32_t MODE>
@@ -428,9 +575,10 @@ int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
     int per_sm = 0;
     ASDM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem));
     if (per_sm <= 0) return fail(ASDM_ERR_INVALID, "query too large for one block's shared memory (%u bytes)", smem);
-    const uint64_t want = (a.ntasks + kWarps - 1) / kWarps;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)per_sm * num_sms, want));
+    // persistent grid: warps without a root task steal donated work
+    const unsigned grid = (unsigned)std::max(1, per_sm * num_sms);
     k<<<grid, kThreads, smem, s>>>(a);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     return ASDM_OK;
 }
@@ -474,13 +622,14 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     std::memcpy(hp.data() + n * sizeof(DLevel) + nb * sizeof(DBack), cf.data(), nc * sizeof(uint32_t));
     uint8_t *d_plan = nullptr;
     unsigned long long *d_ctr = nullptr, *d_local = nullptr;
-    uint32_t *d_rows = nullptr;
+    uint32_t *d_rows = nullptr, *d_queue = nullptr;
     int rc = ASDM_OK;
     auto cleanup = [&]() {
         dfree(d_plan, s);
         dfree(d_ctr, s);
         dfree(d_local, s);
         dfree(d_rows, s);
+        dfree(d_queue, s);
     };
     EnumArgs a{};
     uint64_t row_cap = 0;
@@ -488,6 +637,14 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     do {
         if ((rc = dalloc(&d_plan, pbytes, s))) break;
         if ((rc = dalloc(&d_ctr, kCtrN, s))) break;
+        if ((rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s))) break;
+        queue_init<<<(unsigned)(kQueueCap / 256), 256, 0, s>>>(
+            reinterpret_cast<unsigned long long *>(d_queue + kQueueCap * kRecWords));
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "queue reset failed");
+            break;
+        }
         if (cudaMemcpyAsync(d_plan, hp.data(), pbytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemsetAsync(d_ctr, 0, kCtrN * sizeof(unsigned long long), s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "plan upload failed");
@@ -525,7 +682,10 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         a.local = d_local;
         a.rows = d_rows;
         a.row_cap = row_cap;
+        a.queue = d_queue;
+        a.qseq = reinterpret_cast<unsigned long long *>(d_queue + kQueueCap * kRecWords);
         a.limit_ns = opt.time_limit_s > 0 ? (uint64_t)(opt.time_limit_s * 1e9) : 0;
+        a.count_limit = opt.count_limit;
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -556,10 +716,12 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         st.count = ctr[kCtrCount];
         st.intersections = ctr[kCtrInter];
         st.list_bytes = 4ull * ctr[kCtrElems];
-        st.tasks = a.ntasks;
+        st.tasks = std::min<uint64_t>(ctr[kCtrTask], a.ntasks);  // claimed root tasks
         const uint32_t flags = (uint32_t)ctr[kCtrFlags];
+        if (flags & kFlagInternal) { rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready"); break; }
         if (flags & kFlagOverflow) { rc = fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1"); break; }
         if (flags & kFlagTimeout) { rc = fail(ASDM_ERR_TIMEOUT, "time limit reached"); break; }
+        if (flags & kFlagLimit) { rc = fail(ASDM_ERR_LIMIT, "count limit reached"); break; }
         if ((mode & ASDM_MODE_LOCAL) && opt.local_counts) {
             if (cudaMemcpyAsync(opt.local_counts, d_local, local_n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 s) != cudaSuccess ||

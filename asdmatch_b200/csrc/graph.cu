@@ -168,6 +168,7 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     ASDM_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), s));
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 7) / 8, (uint64_t)g->num_sms * 16);
     check_and_count_runs<<<blocks, 256, 0, s>>>(d, runs, bad);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     ASDM_TRY(scan_exclusive_u32(runs, run_pos, n, true, s));
     uint32_t h_bad = 0;
@@ -186,7 +187,9 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     ASDM_CUDA(cudaMalloc((void **)&run_buf, std::max<uint64_t>(2 * nruns, 1) * sizeof(uint32_t)));
     uint32_t *d_run_lab = run_buf, *d_run_start = run_buf + nruns;
     narrow_u64<<<(unsigned)std::min<uint64_t>((n + 256) / 256, 4096), 256, 0, s>>>(run_pos, d_run_off, (uint64_t)n + 1);
+    ::asdm::count_launch();
     write_runs<<<blocks, 256, 0, s>>>(d, run_pos, d_run_lab, d_run_start);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     d.run_lab = d_run_lab;
     d.run_start = d_run_start;

@@ -302,12 +302,18 @@ void asdm_host_graph_free(asdm_host_graph *g) { delete g; }
 
 int asdm_gen_chung_lu(uint32_t n, uint64_t m, double gamma, uint32_t nlabels, double zipf_s, uint64_t seed,
                       asdm_host_graph **out) {
+    return asdm_gen_chung_lu_capped(n, m, gamma, nlabels, zipf_s, 0.0, seed, out);
+}
+
+int asdm_gen_chung_lu_capped(uint32_t n, uint64_t m, double gamma, uint32_t nlabels, double zipf_s, double wmax,
+                             uint64_t seed, asdm_host_graph **out) {
     clear_error();
     if (!out || n < 2 || m == 0 || gamma <= 1.0 || nlabels == 0)
         return fail(ASDM_ERR_INVALID, "bad Chung-Lu parameters");
     if (m > (uint64_t)n * (n - 1) / 4) return fail(ASDM_ERR_INVALID, "too many edges for %u vertices", n);
     const double alpha = 1.0 / (gamma - 1.0);
-    const double target = std::sqrt(2.0 * (double)m);  // structural cutoff: w_max^2 = sum w
+    // default: the structural cutoff w_max^2 = sum w
+    const double target = wmax > 0 ? wmax : std::sqrt(2.0 * (double)m);
     auto wmax_for = [&](double i0) {
         double s = 0;
         for (uint32_t i = 0; i < n; ++i) s += std::pow(i + i0, -alpha);

@@ -80,6 +80,7 @@ int scan_impl(const Tin *in, uint64_t *out, uint64_t n, bool with_total, cudaStr
     uint64_t *sums = nullptr;
     ASDM_TRY(dalloc(&sums, ntiles + 1, s));
     scan_tiles<Tin><<<(unsigned)ntiles, kThreads, 0, s>>>(in, out, sums, n);
+    ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
     int rc = ASDM_OK;
     uint64_t *prefix = nullptr;
@@ -95,6 +96,7 @@ int scan_impl(const Tin *in, uint64_t *out, uint64_t n, bool with_total, cudaStr
         if (rc == ASDM_OK) rc = scan_impl<uint64_t>(sums, prefix, ntiles, true, s);
         if (rc == ASDM_OK) {
             add_tile_prefix<<<(unsigned)ntiles, kThreads, 0, s>>>(out, prefix, n);
+            ::asdm::count_launch();
             if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "scan launch failed");
         }
         if (rc == ASDM_OK && with_total) {

@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the matching and counting path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|c0]
+
+Workload (default ``c2``): the config-1 data graph (seeded Chung-Lu, N=3.77M,
+M=16.5M, degree exponent 2.1, 20 labels Zipf(1.2)) resident in HBM, and the
+config-2 mixed batch of random-walk queries with sizes uniform in 4..32,
+screened to the queries whose exact count is at most 10^9 (the screen and its
+exact counts are in asdmatch_b200/c2_screened.json).  One step = every query
+of the batch through candidate-space construction, planning and exact
+counting, one query per launch sequence (the plain GPU form).  Each step's
+counts are checked against the screened counts.
+
+Multi-GPU: the path shards by query; every rank runs the whole batch on its
+own GPU with no collective on the data path ("scaling": "weak"); the value is
+N x queries / the slowest rank's step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c0"])
+    ap.add_argument("--cpu-sample", type=int, default=1, help="queries in the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def flush_l2(torch, dev):
+    # a 256 MB write evicts the 126 MB L2 between timed steps
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    buf.fill_(1.0)
+    torch.cuda.synchronize(dev)
+    del buf
+
+
+def cpu_baseline(dpath, qpaths, want_counts, timeout_s=120):
+    """The reference's own CPU path (oracle/_ref, ALL_LEVEL build), one process per
+    query as the reference runs, else the oracle port; returns the JSON object."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_count")
+    port = os.path.join(ROOT, "oracle", "_build", "asdm_oracle")
+    exe, kind = (ref, "reference") if os.path.exists(ref) else (port, "port")
+    if not os.path.exists(exe):
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "unavailable",
+                "sample": "neither oracle/_ref nor oracle/_build is built"}
+    done, t0 = 0, time.time()
+    ok = True
+    for qp, want in zip(qpaths, want_counts):
+        try:
+            r = subprocess.run([exe, "-q", qp, "-d", dpath], capture_output=True, text=True, timeout=timeout_s)
+        except subprocess.TimeoutExpired:
+            break
+        got = [int(l.split(":")[1]) for l in r.stdout.splitlines() if l.startswith("Number of matches:")]
+        ok &= bool(got) and got[0] == want
+        done += 1
+    dt = time.time() - t0
+    return {"value": (done / dt) if done else 0.0, "unit": "queries/s", "cores": 1, "kind": kind,
+            "sample": "%d of the batch's queries, one single-threaded process per query (graph load, CFL filter, "
+                      "FHD planning, ALL_LEVEL join), %.1f s wall, counts %s" % (done, dt, "match" if ok else "DIFFER")}
+
+
+def setup_workload(name):
+    import asdmatch_b200 as A
+    from asdmatch_b200 import workloads as W
+    if name == "c0":
+        g = W.graph(W.C0)
+        qs = W.queries(g, 8, 200, W.C0_QUERY_SEED + 800)
+        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as fh:
+            counts = [r["count"] for r in json.load(fh)["sets"]["c0"]]
+        cfg = {"workload": "c0: Chung-Lu N=3112 M=12519 gamma=2.5 71 labels Zipf(1.0); 200 random-walk queries of 8 vertices",
+               "graph": W.C0}
+        return A, W, g, qs, counts, cfg
+    g = W.graph(W.C1)
+    sc = W.load_c2_screen()
+    qs = W.c2_queries(g, sc)
+    counts = [r["count"] for r in sc["queries"]]
+    sizes = [r["size"] for r in sc["queries"]]
+    cfg = {"workload": "c2-screened: config-1 graph (Chung-Lu N=3.77M M=16.5M gamma=2.1, 20 labels Zipf(1.2)) "
+                       "resident in HBM; %d random-walk queries, sizes uniform 4..32 (mixed density), kept when the "
+                       "exact count <= 1e9 (%d of %d candidates)" % (len(qs), len(qs), sc["candidates"]),
+           "graph": W.C1, "queries": len(qs), "query_sizes": [min(sizes), max(sizes)],
+           "count_limit": sc["count_limit"]}
+    return A, W, g, qs, counts, cfg
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import asdmatch_b200 as A  # generators only
+    A_, W, g, qs, counts, cfg = setup_workload(args.workload)
+    ref = os.path.join(ROOT, "oracle", "_ref", "ref_count")
+    port = os.path.join(ROOT, "oracle", "_build", "asdm_oracle")
+    exe, kind = (ref, "reference") if os.path.exists(ref) else (port, "port")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) and oracle port missing"}))
+        return
+    cores = os.cpu_count() or 1
+    tmp = tempfile.mkdtemp(prefix="asdm_ref_")
+    dpath = os.path.join(tmp, "data.graph")
+    g.write(dpath)
+    qpaths = []
+    for i, q in enumerate(qs):
+        p = os.path.join(tmp, "q%d.graph" % i)
+        q.write(p)
+        qpaths.append(p)
+
+    def step(k):
+        # one bounded sample per step: `cores` queries in parallel, one reference process each
+        idx = [(k * cores + j) % len(qs) for j in range(cores)]
+        t0 = time.time()
+        procs = [subprocess.Popen([exe, "-q", qpaths[i], "-d", dpath], stdout=subprocess.PIPE, text=True) for i in idx]
+        good = 0
+        for i, p in zip(idx, procs):
+            out, _ = p.communicate()
+            got = [int(l.split(":")[1]) for l in out.splitlines() if l.startswith("Number of matches:")]
+            good += bool(got) and got[0] == counts[i]
+        return time.time() - t0, good, len(idx)
+
+    for k in range(args.warmup):
+        step(k)
+    t_total, good, n = 0.0, 0, 0
+    for k in range(args.steps):
+        dt, gd, nn = step(args.warmup + k)
+        t_total += dt
+        good += gd
+        n += nn
+    value = n / t_total
+    line = {"metric": "exact-count queries/sec", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint32/uint64",
+            "data": "synthetic", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": kind,
+                             "sample": "%d queries per step on %d cores (one single-threaded reference process per "
+                                       "query), counts correct %d/%d" % (cores, cores, good, n)},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    A, W, g, qs, counts, cfg = setup_workload(args.workload)
+    dg = A.DeviceGraph(g)
+    stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
+    Q = len(qs)
+
+    def one_step():
+        stats = {"kernel_ms": 0.0, "list_bytes": 0, "cs_ms": 0.0, "cs_bytes": 0, "matches": 0, "inter": 0}
+        for q, want in zip(qs, counts):
+            cs = A.CandidateSpace(dg, q)
+            b, ms = cs.build_stats()
+            stats["cs_bytes"] += b
+            stats["cs_ms"] += ms
+            if cs.nonempty:
+                r = A.adaptive_share_join(cs)
+                stats["kernel_ms"] += r.kernel_ms
+                stats["list_bytes"] += r.list_bytes
+                stats["inter"] += r.intersections
+                got = r.count
+            else:
+                got = 0
+            cs.close()
+            if got != want:
+                raise SystemExit("count mismatch: %d != %d" % (got, want))
+            stats["matches"] += got
+        return stats
+
+    for _ in range(args.warmup):
+        one_step()
+    times, agg = [], None
+    sampler = ClockSampler(local)
+    launches0 = A.kernel_launches()
+    sampler.start()
+    for _ in range(args.steps):
+        flush_l2(torch, dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = one_step()
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize(dev)
+        times.append(e0.elapsed_time(e1))
+        agg = st if agg is None else {k: agg[k] + st[k] for k in agg}
+    clocks = sampler.stop()
+    launches = A.kernel_launches() - launches0
+    ms = statistics.mean(times)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # end to end through the one-call C ABI (asdm_run_batch) from host buffers
+    e2e_times = []
+    h2d = sum(4 * (q.n + 1) + 4 * q.m2 + 4 * q.n for q in qs)
+    d2h = Q * (8 + 4)
+    for _ in range(args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        got, status = A.run_batch(dg, qs)
+        e2e_times.append(time.perf_counter() - t0)
+        if got.tolist() != counts or any(status):
+            raise SystemExit("batch counts differ from the screened counts")
+    e2e_s = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = measured_peaks()
+    steps = args.steps
+    enum_ms, cs_ms = agg["kernel_ms"] / steps, agg["cs_ms"] / steps
+    if enum_ms >= cs_ms:
+        dom, bytes_, kms = "enum_kernel (K4-K8 warp DFS)", agg["list_bytes"] / steps, enum_ms
+    else:
+        dom, bytes_, kms = "candidate space K1-K3", agg["cs_bytes"] / steps, cs_ms
+    achieved = bytes_ / (kms * 1e-3) / 1e9 if kms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            traffic = json.load(fh).get(args.workload)
+    line = {
+        "metric": "exact-count queries/sec",
+        "value": world * Q / (ms / 1e3),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "uint32 ids / uint64 counts",
+        "data": "synthetic (seeded generators; no dataset download)",
+        "config": dict(cfg, l2="flushed (256 MB write) before every timed step", form="plain: one query per launch sequence",
+                       matches_per_step=agg["matches"] // steps,
+                       matches_per_s=world * (agg["matches"] // steps) / (ms / 1e3),
+                       intersections_per_step=agg["inter"] // steps,
+                       enum_kernel_ms_per_step=enum_ms, cs_build_ms_per_step=cs_ms),
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes_per_step": bytes_, "device_ms_per_step": kms, "traffic": traffic},
+        "e2e": {"value": world * Q / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "via": "asdm_run_batch (C ABI) from host arrays"},
+        "gpu_launches": launches // steps,
+        "clocks": clocks,
+    }
+    if world == 1:
+        tmp = tempfile.mkdtemp(prefix="asdm_cpu_")
+        dpath = os.path.join(tmp, "data.graph")
+        g.write(dpath)
+        order = sorted(range(Q), key=lambda i: counts[i])  # smallest counts first keeps the sample bounded
+        sample = order[len(order) // 2: len(order) // 2 + args.cpu_sample]
+        qpaths = []
+        for i in sample:
+            p = os.path.join(tmp, "q%d.graph" % i)
+            qs[i].write(p)
+            qpaths.append(p)
+        line["cpu_baseline"] = cpu_baseline(dpath, qpaths, [counts[i] for i in sample])
+    print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

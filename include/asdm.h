@@ -29,6 +29,7 @@ extern "C" {
 #define ASDM_ERR_TIMEOUT 6   /* the run's time limit was reached              */
 #define ASDM_ERR_CAPACITY 7  /* embedding buffer smaller than the match count */
 #define ASDM_ERR_INTERNAL 8  /* device-side consistency check failed          */
+#define ASDM_ERR_LIMIT 9     /* the run's count limit was reached             */
 
 /* ---- run modes (bit mask); the reference selects these at compile time
  *      with ALL_LEVEL / LOCAL_COUNT / COLLECT_RESULT (config/config.h:38-40) */
@@ -45,6 +46,10 @@ typedef struct asdm_plan asdm_plan;             /* matching order + level info *
 const char *asdm_last_error(void);
 /* Library version string. */
 const char *asdm_version(void);
+/* Number of kernels the library has launched since it was loaded (all
+ * threads); lets callers count the device work of a region.  No reference
+ * counterpart (the reference runs on the CPU). */
+uint64_t asdm_kernel_launches(void);
 
 /* ---- host graphs ------------------------------------------------------- */
 
@@ -72,6 +77,10 @@ void asdm_host_graph_free(asdm_host_graph *g);
  * vertex ids randomly permuted.  No reference counterpart (synthetic input). */
 int asdm_gen_chung_lu(uint32_t n, uint64_t m, double gamma, uint32_t nlabels, double zipf_s,
                       uint64_t seed, asdm_host_graph **out);
+/* Same with the largest expected degree set to wmax instead of sqrt(2m)
+ * (wmax <= 0 keeps sqrt(2m)). */
+int asdm_gen_chung_lu_capped(uint32_t n, uint64_t m, double gamma, uint32_t nlabels, double zipf_s,
+                             double wmax, uint64_t seed, asdm_host_graph **out);
 /* Connected query by random walk with restart from a seeded data vertex: the
  * induced subgraph on the first `size` distinct vertices, labels copied.
  * density: 0 any, 1 dense (average degree >= 3), 2 sparse (< 3).  No
@@ -88,6 +97,9 @@ int asdm_gen_query(const asdm_host_graph *g, uint32_t size, int density, uint64_
 int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, const uint32_t *labels,
                       uint32_t n, uint64_t m2, uint32_t nlabels, asdm_graph **out);
 int asdm_graph_free(asdm_graph *g);
+/* The CUDA stream (cudaStream_t) the library runs this graph's work on, so a
+ * caller can record events around it.  No reference counterpart. */
+int asdm_graph_stream(asdm_graph *g, void **stream);
 
 /* ---- candidate space (K1-K3) ------------------------------------------- */
 
@@ -106,6 +118,9 @@ int asdm_cs_read(const asdm_cs *cs, uint32_t u, uint32_t *out, uint32_t capacity
  * *total receives the number of entries; ASDM_ERR_CAPACITY if it exceeds capacity. */
 int asdm_cs_read_edges(const asdm_cs *cs, uint32_t u, uint32_t u2, uint32_t *offsets,
                        uint32_t *vertices, uint64_t capacity, uint64_t *total);
+/* Algorithmic bytes and device milliseconds of the K1-K3 build (the
+ * reference's "Filtering time", main.cpp:38). */
+int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms);
 int asdm_cs_free(asdm_cs *cs);
 
 /* ---- sorted-set intersection (K4) --------------------------------------- */
@@ -138,6 +153,8 @@ typedef struct asdm_run_opts {
     uint64_t *local_counts; /* host |Vg| x |Vq| row-major (MODE_LOCAL) or NULL */
     uint32_t *embeddings;   /* host rows x |Vq|, sorted on return (MODE_EMBED) */
     uint64_t emb_capacity;  /* rows available in `embeddings`                  */
+    uint64_t count_limit;   /* 0 = none; else stop with ASDM_ERR_LIMIT once the
+                               count passes it (stats.count then >= the limit) */
 } asdm_run_opts;
 
 typedef struct asdm_run_stats {

@@ -28,7 +28,7 @@ def workdir(tmp_path_factory):
 @pytest.fixture(scope="session")
 def c0_files(workdir):
     """config-0 graph and its golden queries written as t/v/e files."""
-    import workloads as W
+    from asdmatch_b200 import workloads as W
     g = W.graph(W.C0)
     d = os.path.join(workdir, "c0")
     dpath, _ = W.write_workload(d, g, [])
@@ -39,7 +39,7 @@ def c0_files(workdir):
 
 @pytest.fixture(scope="session")
 def c0d_files(workdir):
-    import workloads as W
+    from asdmatch_b200 import workloads as W
     g = W.graph(W.C0D)
     d = os.path.join(workdir, "c0d")
     dpath, _ = W.write_workload(d, g, [])

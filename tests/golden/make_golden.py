@@ -5,7 +5,7 @@ oracle/_ref/{ref_count,ref_local,ref_embed}:
 
     make -f oracle/ref.mk && python tests/golden/make_golden.py
 
-For every seeded synthetic query (tests/workloads.py) it records the
+For every seeded synthetic query (asdmatch_b200/workloads.py) it records the
 reference's exact count (ALL_LEVEL build), the SHA-256 of its candidate-space
 dump (CandidateSpace::writeToStream plus the candidate sets), and for the
 queries small enough to enumerate, the SHA-256 of its |Vg| x |Vq| LOCAL_COUNT
@@ -28,7 +28,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 
 import asdmatch_b200 as A  # noqa: E402
 import oracle_util as O  # noqa: E402
-import workloads as W  # noqa: E402
+from asdmatch_b200 import workloads as W  # noqa: E402
 
 EMBED_LIMIT = 200_000   # enumerate (CSV + embeddings) only below this many matches
 

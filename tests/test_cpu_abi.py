@@ -9,7 +9,7 @@ import pytest
 
 import asdmatch_b200 as A
 import oracle_util as O
-import workloads as W
+from asdmatch_b200 import workloads as W
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
