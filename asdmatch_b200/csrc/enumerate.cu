@@ -89,7 +89,14 @@ struct EnumArgs {
     unsigned long long *qseq;   // kQueueCap slot sequence numbers
 };
 
-__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb; }
+__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 32; }
+
+// The last level is evaluated one survivor per lane (instead of one warp per
+// survivor) when it has at most this many earlier neighbours and its shortest
+// list is at most kLaneLeafMax long.
+constexpr uint32_t kLaneLeafLists = 4;
+constexpr uint32_t kLaneLeafMax = 96;
+constexpr uint32_t kSelf = 0xFFFFFFFEu;
 
 __host__ __device__ inline uint32_t plan_words(uint32_t n, uint32_t nb, uint32_t nc) {
     return (uint32_t)((n * sizeof(DLevel) + nb * sizeof(DBack)) / 4) + ((nc + 3) & ~3u);
@@ -125,7 +132,7 @@ struct Warp {
     const DLevel *L;
     const DBack *B;
     const uint32_t *CF;
-    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur;
+    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur, *fidx;
     uint32_t lane;
     unsigned long long count = 0, inter = 0, elems = 0;
     bool overflow = false;
@@ -144,6 +151,108 @@ struct Warp {
         sstart = drv + n;
         slen = sstart + a.nb;
         scur = slen + a.nb;
+        fidx = scur + a.nb;
+    }
+
+    __device__ __forceinline__ bool lane_leaf_ok() const {
+        return MODE == ASDM_MODE_COUNT && L[a.n - 1].nback <= kLaneLeafLists;
+    }
+
+    // For the level before the last: the candidate index in C(u_last) of every
+    // earlier vertex the last level must avoid (kNone when it is not a
+    // candidate there, kSelf when it is level d's own vertex).
+    __device__ void prepare_lane_leaf(uint32_t d) {
+        const DLevel lvL = L[a.n - 1];
+        if (lane < lvL.nconf) {
+            const uint32_t c = CF[lvL.conf_first + lane];
+            uint32_t y = kSelf;
+            if (c < d) {
+                const uint32_t v = vid[c];
+                y = lower_bound_u32(lvL.cand, lvL.ncand, v);
+                if (y >= lvL.ncand || lvL.cand[y] != v) y = kNone;
+            }
+            fidx[lane] = y;
+        }
+        __syncwarp();
+    }
+
+    // Last-level count for survivor x of level d = n-2, computed by this lane
+    // alone.  Returns false (and leaves the survivor to the warp-wide path)
+    // when the lists are too long for one lane.
+    __device__ bool lane_leaf(uint32_t d, uint32_t x, unsigned long long &out, unsigned long long &touched) {
+        const DLevel lvL = L[a.n - 1];
+        const uint32_t m = lvL.nback;
+        const uint32_t *p[kLaneLeafLists];
+        uint32_t len[kLaneLeafLists];
+        uint32_t best = 0xFFFFFFFFu, bi = 0, tot = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kLaneLeafLists; ++k) {
+            p[k] = nullptr;
+            len[k] = 0;
+            if (k < m) {
+                const DBack bk = B[lvL.back_first + k];
+                const uint32_t ij = bk.level == d ? x : idx[bk.level];
+                const uint32_t a0 = bk.off[ij], a1 = bk.off[ij + 1];
+                p[k] = bk.list + a0;
+                len[k] = a1 - a0;
+                tot += len[k];
+                if (len[k] < best) { best = len[k]; bi = k; }
+            }
+        }
+        if (m > 1 && best > kLaneLeafMax) return false;
+        touched += tot;
+        unsigned long long c = 0;
+        if (m == 1) {
+            c = len[0];
+        } else if (best) {
+            // the shortest list drives; the others are galloped from cursors
+            const uint32_t *dp = p[0];
+            uint32_t dl = len[0];
+#pragma unroll
+            for (uint32_t k = 1; k < kLaneLeafLists; ++k)
+                if (k == bi) { const uint32_t *tp = p[0]; p[0] = p[k]; p[k] = tp; uint32_t tl = len[0]; len[0] = len[k]; len[k] = tl; }
+            dp = p[0];
+            dl = len[0];
+            uint32_t cur[kLaneLeafLists] = {0, 0, 0, 0};
+            for (uint32_t i = 0; i < dl; ++i) {
+                const uint32_t v = dp[i];
+                bool in = true, done = false;
+#pragma unroll
+                for (uint32_t k = 1; k < kLaneLeafLists; ++k) {
+                    if (k < m && in) {
+                        const uint32_t q = gallop_lb(p[k], cur[k], len[k], v);
+                        cur[k] = q;
+                        if (q >= len[k]) { done = true; in = false; }
+                        else in = p[k][q] == v;
+                    }
+                }
+                c += in;
+                if (done) break;
+            }
+        }
+        if (c && lvL.nconf) {
+            // same-label earlier vertices that sit in every list are not matches
+            for (uint32_t k = 0; k < lvL.nconf; ++k) {
+                uint32_t y = fidx[k];
+                if (y == kSelf) {
+                    const uint32_t v = L[d].cand[x];
+                    y = lower_bound_u32(lvL.cand, lvL.ncand, v);
+                    if (y >= lvL.ncand || lvL.cand[y] != v) y = kNone;
+                }
+                if (y == kNone) continue;
+                bool in = true;
+#pragma unroll
+                for (uint32_t j = 0; j < kLaneLeafLists; ++j) {
+                    if (j < m && in) {
+                        const uint32_t q = lower_bound_u32(p[j], len[j], y);
+                        in = q < len[j] && p[j][q] == y;
+                    }
+                }
+                c -= in;
+            }
+        }
+        out = c;
+        return true;
     }
 
     __device__ __forceinline__ void add_count(unsigned long long c) {
@@ -323,6 +432,22 @@ struct Warp {
             const uint32_t vx = ok ? lv.cand[x] : 0;
             ok = ok && no_conflict(lv, vx);
         }
+        if (d + 2 == a.n && lane_leaf_ok()) {
+            // count the last level of every survivor lane-parallel; survivors
+            // with long lists stay buffered for the warp-wide leaf
+            unsigned long long c = 0, touched = 0;
+            const bool done = ok && lane_leaf(d, x, c, touched);
+            ok = ok && !done;
+            const uint32_t dm = __ballot_sync(kFull, done);
+            inter += (L[a.n - 1].nback >= 2) ? __popc(dm) : 0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                c += __shfl_xor_sync(kFull, c, o);
+                touched += __shfl_xor_sync(kFull, touched, o);
+            }
+            add_count(c);
+            elems += touched;
+        }
         const uint32_t mask = __ballot_sync(kFull, ok);
         if (ok) buf[32 * d + __popc(mask & ((1u << lane) - 1))] = x;
         __syncwarp();
@@ -489,6 +614,8 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
                 d = 1;
             } else if (len == 0) {
                 d = 1;
+            } else if (d + 2 == n && W.lane_leaf_ok()) {
+                W.prepare_lane_leaf(d);
             }
         } else {
             const unsigned long long qpos = W.take_queued();
@@ -505,6 +632,7 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
             __syncwarp();
             d = base;
             W.setup(d);
+            if (d + 2 == n && W.lane_leaf_ok()) W.prepare_lane_leaf(d);
             if (lane == 0) {
                 W.dpos[d] = lo;
                 W.dend[d] = hi;
@@ -544,6 +672,8 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
                     --d;
                 } else if (len == 0) {
                     --d;
+                } else if (d + 2 == n && W.lane_leaf_ok()) {
+                    W.prepare_lane_leaf(d);
                 }
                 continue;
             }

@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c0"])
     ap.add_argument("--cpu-sample", type=int, default=1, help="queries in the CPU-baseline sample")
+    ap.add_argument("--queries", type=int, default=0, help="use only the first K queries (profiling runs)")
+    ap.add_argument("--profile", action="store_true", help="timed steps only: no e2e pass, no CPU baseline")
     return ap.parse_args()
 
 
@@ -230,6 +232,9 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     A, W, g, qs, counts, cfg = setup_workload(args.workload)
+    if args.queries:
+        qs, counts = qs[:args.queries], counts[:args.queries]
+        cfg = dict(cfg, queries=len(qs), subset="first %d queries" % len(qs))
     dg = A.DeviceGraph(g)
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
@@ -281,6 +286,10 @@ def main():
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": ms, "queries": Q, "launches": launches // args.steps}))
+        return
     # end to end through the one-call C ABI (asdm_run_batch) from host buffers
     e2e_times = []
     h2d = sum(4 * (q.n + 1) + 4 * q.m2 + 4 * q.n for q in qs)
