@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 
 #include "cs.cuh"
@@ -931,4 +932,157 @@ extern "C" int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const 
     asdm_plan_free(plan);
     asdm_cs_free(cs);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free counting.
+//
+// Some callers cannot let a library allocate device memory while they run:
+// a serving process whose GPU memory is entirely reserved up front by its own
+// pool allocator (a cudaMalloc there can fail or push a co-tenant out of
+// memory), or a latency-critical loop where cudaMalloc/cudaFree would add
+// implicit device synchronisation.  asdm_run_plan_count_noalloc serves them:
+// it runs the same COUNT-mode enumeration kernel as asdm_run_plan, but its
+// scratch (the run counters, the device copy of the plan and the
+// work-donation ring) lives in the fixed, file-scope device array below.
+// The caller still passes the inputs (a candidate space and a plan) and the
+// output (the stats struct).
+//
+// The array is kNoAllocScratchBytes (about 10 MiB) on every GPU that loads
+// this library, held until the process exits.  Its host-side name is only a
+// stand-in for the device symbol, so the device address is fetched with
+// cudaGetSymbolAddress once per device (with that device current) by the
+// first call made on that device; make that first call before any stream
+// capture.  All calls share the one array and it keeps the last call's
+// contents: every call re-zeroes the counters and re-initialises the ring
+// before its launch.  Calls that overlap on the GPU (from several host
+// threads or several streams) race on the array and must be serialised by
+// the caller.
+namespace asdm {
+namespace {
+
+constexpr uint64_t kNoAllocCtrBytes = 256;
+constexpr uint64_t kNoAllocPlanBytes = 16384;  // >= 32 levels + 496 back edges + 496 conflict levels
+constexpr uint64_t kNoAllocSeqBytes = kQueueCap * sizeof(unsigned long long);
+constexpr uint64_t kNoAllocRingBytes = kQueueCap * kRecWords * sizeof(uint32_t);
+constexpr uint64_t kNoAllocScratchBytes = kNoAllocCtrBytes + kNoAllocPlanBytes + kNoAllocSeqBytes + kNoAllocRingBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (set up once).
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(ASDM_ERR_INVALID, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(ASDM_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return ASDM_OK;
+}
+
+}  // namespace
+}  // namespace asdm
+
+extern "C" int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, double time_limit_s,
+                                           uint64_t count_limit, asdm_run_stats *stats) {
+    using namespace asdm;
+    clear_error();
+    if (!cs || !stats) return fail(ASDM_ERR_INVALID, "null argument");
+    *stats = asdm_run_stats{};
+    if (!cs->nonempty) return ASDM_OK;
+    if (!plan || plan->order.size() != cs->q.n) return fail(ASDM_ERR_INVALID, "plan does not match the query");
+    asdm_graph *G = cs->g;
+    cudaStream_t s = G->stream;
+    const uint32_t n = cs->q.n;
+    // host image of the device plan (same layout as asdm_run_plan's)
+    std::vector<DLevel> lv(n);
+    std::vector<DBack> bk;
+    std::vector<uint32_t> cf;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t u = plan->order[k];
+        lv[k].cand = cs->d_cand + cs->cand_base[u];
+        lv[k].ncand = cs->ncand[u];
+        lv[k].u = u;
+        lv[k].nback = (uint32_t)plan->back[k].size();
+        lv[k].back_first = (uint32_t)bk.size();
+        for (auto &jb : plan->back[k])
+            bk.push_back(DBack{cs->d_eoff + cs->eoff_base[jb.second], cs->d_elist + cs->elist_base[jb.second], jb.first, 0});
+        lv[k].nconf = (uint32_t)plan->conf[k].size();
+        lv[k].conf_first = (uint32_t)cf.size();
+        cf.insert(cf.end(), plan->conf[k].begin(), plan->conf[k].end());
+    }
+    const uint32_t nb = (uint32_t)bk.size(), nc = (uint32_t)cf.size();
+    const uint64_t pbytes = n * sizeof(DLevel) + nb * sizeof(DBack) + nc * sizeof(uint32_t);
+    if (pbytes > kNoAllocPlanBytes)
+        return fail(ASDM_ERR_INVALID, "plan needs %llu bytes; the no-alloc scratch holds %llu",
+                    (unsigned long long)pbytes, (unsigned long long)kNoAllocPlanBytes);
+    std::vector<uint8_t> hp(pbytes);
+    std::memcpy(hp.data(), lv.data(), n * sizeof(DLevel));
+    std::memcpy(hp.data() + n * sizeof(DLevel), bk.data(), nb * sizeof(DBack));
+    std::memcpy(hp.data() + n * sizeof(DLevel) + nb * sizeof(DBack), cf.data(), nc * sizeof(uint32_t));
+
+    int current = -1;
+    ASDM_CUDA(cudaGetDevice(&current));
+    if (current != G->device)
+        return fail(ASDM_ERR_INVALID, "call with the graph's device (%d) current, not %d", G->device, current);
+    unsigned char *base = nullptr;
+    ASDM_TRY(noalloc_scratch(G->device, &base));
+    unsigned long long *d_ctr = reinterpret_cast<unsigned long long *>(base);
+    uint8_t *d_plan = base + kNoAllocCtrBytes;
+    unsigned long long *d_seq = reinterpret_cast<unsigned long long *>(base + kNoAllocCtrBytes + kNoAllocPlanBytes);
+    uint32_t *d_ring = reinterpret_cast<uint32_t *>(base + kNoAllocCtrBytes + kNoAllocPlanBytes + kNoAllocSeqBytes);
+
+    ASDM_CUDA(cudaMemcpyAsync(d_plan, hp.data(), pbytes, cudaMemcpyHostToDevice, s));
+    ASDM_CUDA(cudaMemsetAsync(d_ctr, 0, kCtrN * sizeof(unsigned long long), s));
+    queue_init<<<(unsigned)(kQueueCap / 256), 256, 0, s>>>(d_seq);
+    ::asdm::count_launch();
+    ASDM_CUDA(cudaGetLastError());
+
+    EnumArgs a{};
+    a.lv = reinterpret_cast<const DLevel *>(d_plan);
+    a.bk = reinterpret_cast<const DBack *>(d_plan + n * sizeof(DLevel));
+    a.conf = reinterpret_cast<const uint32_t *>(d_plan + n * sizeof(DLevel) + nb * sizeof(DBack));
+    a.n = n;
+    a.nb = nb;
+    a.nc = nc;
+    a.nq = n;
+    if (n == 1) {
+        a.ntasks = cs->ncand[plan->order[0]];
+    } else {
+        const uint32_t e01 = plan->back[1][0].second;
+        a.off01 = cs->d_eoff + cs->eoff_base[e01];
+        a.list01 = cs->d_elist + cs->elist_base[e01];
+        a.n0 = cs->ncand[plan->order[0]];
+        a.ntasks = cs->etotal[e01];
+    }
+    a.ctr = d_ctr;
+    a.queue = d_ring;
+    a.qseq = d_seq;
+    a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
+    a.count_limit = count_limit;
+    if (a.ntasks) {
+        const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
+        ASDM_TRY(launch<ASDM_MODE_COUNT>(a, smem, G->num_sms, s));
+    }
+    unsigned long long ctr[kCtrN];
+    ASDM_CUDA(cudaMemcpyAsync(ctr, d_ctr, sizeof ctr, cudaMemcpyDeviceToHost, s));
+    ASDM_CUDA(cudaStreamSynchronize(s));
+    stats->count = ctr[kCtrCount];
+    stats->intersections = ctr[kCtrInter];
+    stats->list_bytes = 4ull * ctr[kCtrElems];
+    stats->tasks = std::min<uint64_t>(ctr[kCtrTask], a.ntasks);
+    const uint32_t flags = (uint32_t)ctr[kCtrFlags];
+    if (flags & kFlagInternal) return fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
+    if (flags & kFlagOverflow) return fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1");
+    if (flags & kFlagTimeout) return fail(ASDM_ERR_TIMEOUT, "time limit reached");
+    if (flags & kFlagLimit) return fail(ASDM_ERR_LIMIT, "count limit reached");
+    return ASDM_OK;
 }

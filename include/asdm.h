@@ -173,6 +173,21 @@ typedef struct asdm_run_stats {
 int asdm_run_plan(asdm_cs *cs, const asdm_plan *plan, const asdm_run_opts *opts,
                   asdm_run_stats *stats);
 
+/* Counts like asdm_run_plan in ASDM_MODE_COUNT, but allocates no device memory:
+ * for callers whose GPU memory is fully reserved by their own allocator, or
+ * that cannot afford cudaMalloc/cudaFree (and their implicit synchronisation)
+ * while they run.  The kernel's scratch (counters, device plan, work-donation
+ * ring) is a fixed ~10 MiB file-scope device array, held by every GPU that
+ * loads the library until exit.  The first call on a device looks up that
+ * array's address (cudaGetSymbolAddress) with the graph's device current, so
+ * make it before any stream capture.  Calls share the array and must not
+ * overlap on the GPU; each call resets the parts that must start at zero.
+ * Queries up to 32 vertices (a plan of at most 16 KiB); larger plans are
+ * rejected with ASDM_ERR_INVALID.  No counterpart in the reference, which
+ * allocates with new[] throughout. */
+int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, double time_limit_s,
+                                uint64_t count_limit, asdm_run_stats *stats);
+
 /* One call for a query end to end on a resident graph: candidate space, plan
  * and count (the whole of ASDMatch.out's main(), main.cpp:11-147, without I/O). */
 int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q_nbrs,
