@@ -56,7 +56,8 @@ class RunOpts(C.Structure):
 
 class RunStats(C.Structure):
     _fields_ = [("count", C.c_uint64), ("emb_rows", C.c_uint64), ("intersections", C.c_uint64),
-                ("list_bytes", C.c_uint64), ("tasks", C.c_uint64), ("kernel_ms", C.c_double)]
+                ("list_bytes", C.c_uint64), ("tasks", C.c_uint64), ("kernel_ms", C.c_double),
+                ("build_ms", C.c_double), ("build_bytes", C.c_uint64)]
 
 
 def _sig(name, res, args):
@@ -99,7 +100,7 @@ _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
 _run_batch = _sig("asdm_run_batch", C.c_int, [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p,
-                                              C.c_double, _u64p, C.POINTER(C.c_int)])
+                                              C.c_double, _u64p, C.POINTER(C.c_int), C.POINTER(RunStats)])
 
 
 def _check(rc: int, what: str = ""):
@@ -415,21 +416,39 @@ def leapfrog_join(lists_per_set: Sequence[Sequence[np.ndarray]]) -> List[np.ndar
     return [out[ooff[i]:ooff[i] + cnt[i]].copy() for i in range(len(lists_per_set))]
 
 
-def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):
-    """Counts for many queries against one resident graph; returns (counts, status)."""
-    nq = len(queries)
-    sizes = np.asarray([q.n for q in queries], np.uint32)
-    offs = np.concatenate([q.offsets for q in queries]).astype(np.uint32)
-    nbrs = np.concatenate([q.nbrs for q in queries] + [np.zeros(1, np.uint32)]).astype(np.uint32)
-    labs = np.concatenate([q.labels for q in queries]).astype(np.uint32)
-    ob = np.cumsum([0] + [q.n + 1 for q in queries[:-1]]).astype(np.uint64)
-    nb = np.cumsum([0] + [q.m2 for q in queries[:-1]]).astype(np.uint64)
-    lb = np.cumsum([0] + [q.n for q in queries[:-1]]).astype(np.uint64)
-    counts = np.zeros(nq, np.uint64)
-    status = np.zeros(nq, np.int32)
-    rc = _run_batch(dg._h, nq, _ptr(sizes), _ptr(ob, _u64p), _ptr(offs), _ptr(nb, _u64p), _ptr(nbrs),
-                    _ptr(lb, _u64p), _ptr(labs), time_limit_s, _ptr(counts, _u64p),
-                    status.ctypes.data_as(C.POINTER(C.c_int)))
+class BatchInput:
+    """Queries packed once into the host arrays asdm_run_batch takes."""
+
+    def __init__(self, queries: Sequence[HostGraph]):
+        self.nq = len(queries)
+        self.sizes = np.asarray([q.n for q in queries], np.uint32)
+        self.offs = np.concatenate([q.offsets for q in queries]).astype(np.uint32)
+        self.nbrs = np.concatenate([q.nbrs for q in queries] + [np.zeros(1, np.uint32)]).astype(np.uint32)
+        self.labs = np.concatenate([q.labels for q in queries]).astype(np.uint32)
+        self.ob = np.cumsum([0] + [q.n + 1 for q in queries[:-1]]).astype(np.uint64)
+        self.nb = np.cumsum([0] + [q.m2 for q in queries[:-1]]).astype(np.uint64)
+        self.lb = np.cumsum([0] + [q.n for q in queries[:-1]]).astype(np.uint64)
+        self.counts = np.zeros(self.nq, np.uint64)
+        self.status = np.zeros(self.nq, np.int32)
+
+    def nbytes(self):
+        return int(self.sizes.nbytes + self.offs.nbytes + self.nbrs.nbytes + self.labs.nbytes + self.ob.nbytes +
+                   self.nb.nbytes + self.lb.nbytes)
+
+
+def run_batch_packed(dg: DeviceGraph, b: BatchInput, time_limit_s: float = 0.0) -> RunStats:
+    """Batched counting of pre-packed queries; results land in b.counts / b.status."""
+    st = RunStats()
+    rc = _run_batch(dg._h, b.nq, _ptr(b.sizes), _ptr(b.ob, _u64p), _ptr(b.offs), _ptr(b.nb, _u64p), _ptr(b.nbrs),
+                    _ptr(b.lb, _u64p), _ptr(b.labs), time_limit_s, _ptr(b.counts, _u64p),
+                    b.status.ctypes.data_as(C.POINTER(C.c_int)), C.byref(st))
     if rc == ERR_CUDA:
         _check(rc, "batch")
-    return counts, status
+    return st
+
+
+def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):
+    """Counts for many queries against one resident graph; returns (counts, status)."""
+    b = BatchInput(queries)
+    run_batch_packed(dg, b, time_limit_s)
+    return b.counts.copy(), b.status.copy()

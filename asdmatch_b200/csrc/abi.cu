@@ -157,25 +157,106 @@ extern "C" int asdm_intersect_batch(const uint32_t *values, const uint64_t *list
     return rc;
 }
 
+namespace asdm {
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p);
+int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg);
+}  // namespace asdm
+
+// Candidate-space state a group may hold at once (state words, storage and
+// candidate arrays: 12 bytes per data vertex of each query vertex's label).
+static constexpr uint64_t kGroupStateBytes = 16ull << 30;
+
 extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
                               const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
                               const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
-                              uint64_t *counts, int *status) {
+                              uint64_t *counts, int *status, asdm_run_stats *stats) {
     clear_error();
+    if (stats) *stats = asdm_run_stats{};
     if (!g || (nq && (!q_sizes || !q_off_base || !q_offsets || !q_nbr_base || !q_nbrs || !q_lab_base || !q_labels ||
                       !counts || !status)))
         return fail(ASDM_ERR_INVALID, "null argument");
-    int worst = ASDM_OK;
+    std::vector<std::unique_ptr<asdm_cs>> all(nq);
+    std::vector<uint64_t> state(nq, 0);
     for (uint32_t i = 0; i < nq; ++i) {
-        asdm_run_opts o{};
-        o.mode = ASDM_MODE_COUNT;
-        o.time_limit_s = time_limit_s;
-        asdm_run_stats st{};
-        const int rc = asdm_count_query(g, q_offsets + q_off_base[i], q_nbrs + q_nbr_base[i], q_labels + q_lab_base[i],
-                                        q_sizes[i], &o, &st);
-        status[i] = rc;
-        counts[i] = rc == ASDM_OK ? st.count : 0;
+        counts[i] = 0;
+        status[i] = ASDM_OK;
+        auto c = std::make_unique<asdm_cs>();
+        c->g = g;
+        const int rc = make_query(q_offsets + q_off_base[i], q_nbrs + q_nbr_base[i], q_labels + q_lab_base[i],
+                                  q_sizes[i], c->q);
+        if (rc != ASDM_OK) {
+            status[i] = rc;
+            continue;
+        }
+        for (uint32_t u = 0; u < c->q.n; ++u) {
+            const uint32_t l = c->q.lab[u];
+            if (l < g->d.nlabels) state[i] += 12ull * (g->h_vbl_off[l + 1] - g->h_vbl_off[l]);
+        }
+        all[i] = std::move(c);
+    }
+    int worst = ASDM_OK;
+    for (uint32_t i = 0; i < nq && worst != ASDM_ERR_CUDA; ++i)
+        if (status[i] != ASDM_OK && worst == ASDM_OK) worst = status[i];
+    uint32_t i = 0;
+    while (i < nq) {
+        // next group: consecutive valid queries within the state budget
+        std::vector<uint32_t> ids;
+        uint64_t bytes = 0;
+        for (; i < nq; ++i) {
+            if (!all[i]) continue;
+            if (!ids.empty() && bytes + state[i] > kGroupStateBytes) break;
+            ids.push_back(i);
+            bytes += state[i];
+        }
+        if (ids.empty()) continue;
+        std::vector<asdm_cs *> group;
+        for (uint32_t id : ids) group.push_back(all[id].get());
+        int rc = build_batch(group);
+        if (rc != ASDM_OK) {
+            for (uint32_t id : ids) status[id] = rc;
+            if (worst == ASDM_OK) worst = rc;
+            if (rc == ASDM_ERR_CUDA) break;
+            continue;
+        }
+        std::vector<asdm_plan> plans(ids.size());
+        std::vector<asdm_cs *> run_cs;
+        std::vector<const asdm_plan *> run_plans;
+        std::vector<uint32_t> run_ids;
+        for (size_t k = 0; k < ids.size(); ++k) {
+            if (!group[k]->nonempty) continue;  // count 0, like the reference's early return
+            const int prc = build_plan(*group[k], nullptr, plans[k]);
+            if (prc != ASDM_OK) {
+                status[ids[k]] = prc;
+                if (worst == ASDM_OK) worst = prc;
+                continue;
+            }
+            run_cs.push_back(group[k]);
+            run_plans.push_back(&plans[k]);
+            run_ids.push_back(ids[k]);
+        }
+        std::vector<uint64_t> c(run_ids.size());
+        std::vector<int> st(run_ids.size());
+        asdm_run_stats gs{};
+        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, c.data(), st.data(), &gs);
+        if (stats) {
+            stats->count += gs.count;
+            stats->intersections += gs.intersections;
+            stats->list_bytes += gs.list_bytes;
+            stats->tasks += gs.tasks;
+            stats->kernel_ms += gs.kernel_ms;
+            for (asdm_cs *gc : group) {
+                stats->build_ms += gc->build_ms;
+                stats->build_bytes += gc->build_bytes;
+            }
+        }
+        for (size_t k = 0; k < run_ids.size(); ++k) {
+            counts[run_ids[k]] = c[k];
+            status[run_ids[k]] = st[k];
+            if (st[k] != ASDM_OK && worst == ASDM_OK) worst = st[k];
+        }
         if (rc != ASDM_OK && worst == ASDM_OK) worst = rc;
+        for (uint32_t id : ids) all[id].reset();
         if (rc == ASDM_ERR_CUDA) break;
     }
     return worst;

@@ -1,7 +1,23 @@
 // Candidate space of one query on the device (the product of K1-K3).
 #pragma once
 
+#include <memory>
+
 #include "device.cuh"
+
+// Device arrays of the candidate spaces built together in one group; every
+// asdm_cs of the group holds a reference, the last one frees them.
+struct CsArena {
+    cudaStream_t stream = nullptr;
+    uint32_t *d_cand = nullptr;
+    uint32_t *d_eoff = nullptr;
+    uint32_t *d_elist = nullptr;
+    ~CsArena() {
+        asdm::dfree(d_cand, stream);
+        asdm::dfree(d_eoff, stream);
+        asdm::dfree(d_elist, stream);
+    }
+};
 
 struct asdm_cs {
     asdm_graph *g = nullptr;
@@ -24,7 +40,13 @@ struct asdm_cs {
     uint32_t *d_elist = nullptr;
     uint64_t build_bytes = 0;              // algorithmic bytes of K1-K3 (roofline)
     float build_ms = 0.f;                  // device time of K1-K3
+    std::shared_ptr<CsArena> arena;        // owns d_cand / d_eoff / d_elist
 };
+
+namespace asdm {
+// K1-K3 for a group of queries on the same graph (one launch per phase).
+int build_batch(const std::vector<asdm_cs *> &group);
+}  // namespace asdm
 
 struct asdm_plan {
     std::vector<uint32_t> order;                                   // level -> query vertex

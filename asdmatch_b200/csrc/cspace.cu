@@ -41,22 +41,21 @@ __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ pr
 }
 
 // ---- K1: label + degree + NLC filter --------------------------------------
+// One segment per (query, query vertex) of a batch.
 struct FilterArgs {
     DevGraph g;
     uint32_t *st;
-    const uint64_t *seg;      // nq + 1 prefix of |V_l(u)|
+    const uint64_t *seg;      // nseg + 1 prefix of |V_l(u)|
     const uint32_t *lbase;    // vbl_off[l(u)]
     const uint32_t *qdeg;     // deg(u)
     const uint32_t *qnlc;     // (label, count) pairs
-    const uint32_t *qnlc_off; // nq + 1
-    uint32_t nq;
+    const uint32_t *qnlc_off; // nseg + 1
+    uint32_t nq;              // number of segments
     uint32_t *fcount;         // |F(u)|
 };
 
 __global__ void __launch_bounds__(kBlock) k1_filter(FilterArgs a) {
-    __shared__ uint64_t seg[kMaxQuery + 1];
-    for (uint32_t i = threadIdx.x; i <= a.nq; i += blockDim.x) seg[i] = a.seg[i];
-    __syncthreads();
+    const uint64_t *seg = a.seg;
     const uint64_t total = seg[a.nq];
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -143,7 +142,7 @@ struct CompDesc {
     uint32_t len;         // |V_l(u)|
     uint32_t need;        // required bits
     uint32_t lbase;       // vbl_off[l(u)]
-    uint32_t pad;
+    uint32_t phantom;     // append data vertex 0 when fewer than len survive
 };
 
 __global__ void __launch_bounds__(kBlock) k3_count(const CompDesc *__restrict__ segs, const uint64_t *__restrict__ tile_first,
@@ -206,8 +205,11 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
     for (int k = 0; k < kItems; ++k)
         if (flags & (1u << k)) d.out[pos++] = vbl[d.lbase + (uint32_t)(my + k)];
     // the last tile of a segment records the segment size
-    if (threadIdx.x == 0 && t + 1 == tile_first[sidx + 1])
-        seg_count[sidx] = (uint32_t)(tile_pos[t + 1] - tile_pos[tile_first[sidx]]);
+    if (threadIdx.x == 0 && t + 1 == tile_first[sidx + 1]) {
+        uint32_t size = (uint32_t)(tile_pos[t + 1] - tile_pos[tile_first[sidx]]);
+        if (d.phantom && size < d.len) d.out[size++] = 0;  // the reference's zero-filled storage tail
+        seg_count[sidx] = size;
+    }
 }
 
 // ---- K3b: candidate edges ---------------------------------------------------
@@ -218,13 +220,15 @@ struct EdgeDesc {
     uint32_t label_u2;
 };
 
-__global__ void __launch_bounds__(kBlock) k3_scatter_map(const uint32_t *__restrict__ cand, const uint64_t *__restrict__ cprefix,
-                                                         uint32_t nq, uint32_t *const *__restrict__ maps,
+__global__ void __launch_bounds__(kBlock) k3_scatter_map(const uint32_t *const *__restrict__ cands,
+                                                         const uint64_t *__restrict__ cprefix, uint32_t nseg,
+                                                         uint32_t *const *__restrict__ maps,
                                                          const uint32_t *__restrict__ pos_in_label) {
-    const uint64_t total = cprefix[nq];
+    const uint64_t total = cprefix[nseg];
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t u = find_segment(cprefix, nq, i);
-        maps[u][pos_in_label[cand[i]]] = (uint32_t)(i - cprefix[u]);
+        const uint32_t u = find_segment(cprefix, nseg, i);
+        const uint32_t j = (uint32_t)(i - cprefix[u]);
+        maps[u][pos_in_label[cands[u][j]]] = j;
     }
 }
 
@@ -373,290 +377,364 @@ struct Scratch {
         if (rc == ASDM_OK) ptrs.push_back((void *)*p);
         return rc;
     }
+    template <typename T>
+    int upload(T **p, const std::vector<T> &h) {
+        ASDM_TRY(alloc(p, h.size()));
+        if (!h.empty()) ASDM_CUDA(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+        return ASDM_OK;
+    }
 };
 
-int build(asdm_cs &cs) {
-    asdm_graph *G = cs.g;
+// Host-side plan of one query's CFL build.
+struct QPlan {
+    asdm_cs *cs;
+    uint32_t seg0;                  // first segment (query vertex 0)
+    bool empty = false;
+    std::vector<uint32_t> lsize, lbase, rank, order, wave;
+};
+
+}  // namespace
+
+// Candidate spaces of a group of queries on one graph, one launch per phase
+// for the whole group.  Every phase is the single-query computation applied
+// to all (query, query vertex) segments at once.
+int build_batch(const std::vector<asdm_cs *> &group) {
+    if (group.empty()) return ASDM_OK;
+    asdm_graph *G = group[0]->g;
     const DevGraph &g = G->d;
     cudaStream_t s = G->stream;
-    const QueryGraph &q = cs.q;
-    const uint32_t nq = q.n;
     Scratch scr{s, {}};
     cudaEvent_t ev0, ev1;
     ASDM_CUDA(cudaEventCreate(&ev0));
     ASDM_CUDA(cudaEventCreate(&ev1));
     ASDM_CUDA(cudaEventRecord(ev0, s));
-
-    std::vector<uint32_t> lsize(nq, 0), lbase(nq, 0);
-    for (uint32_t u = 0; u < nq; ++u) {
-        const uint32_t l = q.lab[u];
-        if (l < g.nlabels) {
-            lbase[u] = G->h_vbl_off[l];
-            lsize[u] = G->h_vbl_off[l + 1] - G->h_vbl_off[l];
+    const uint32_t Q = (uint32_t)group.size();
+    std::vector<QPlan> P(Q);
+    uint32_t nseg = 0;
+    for (uint32_t qi = 0; qi < Q; ++qi) {
+        QPlan &qp = P[qi];
+        qp.cs = group[qi];
+        const QueryGraph &q = qp.cs->q;
+        qp.seg0 = nseg;
+        nseg += q.n;
+        qp.lsize.assign(q.n, 0);
+        qp.lbase.assign(q.n, 0);
+        for (uint32_t u = 0; u < q.n; ++u) {
+            const uint32_t l = q.lab[u];
+            if (l < g.nlabels) {
+                qp.lbase[u] = G->h_vbl_off[l];
+                qp.lsize[u] = G->h_vbl_off[l + 1] - G->h_vbl_off[l];
+            }
         }
     }
-    std::vector<uint64_t> seg(nq + 1, 0);
-    for (uint32_t u = 0; u < nq; ++u) seg[u + 1] = seg[u] + lsize[u];
-    // query NLC (label, count), labels ascending (neighbours are (label,id)-sorted)
-    std::vector<uint32_t> qnlc, qnlc_off(nq + 1, 0), qdeg(nq);
-    for (uint32_t u = 0; u < nq; ++u) {
-        qdeg[u] = q.deg(u);
-        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-            const uint32_t l = q.lab[q.nbr[e]];
-            if (qnlc.size() > 2 * qnlc_off[u] && qnlc[qnlc.size() - 2] == l) qnlc.back()++;
-            else { qnlc.push_back(l); qnlc.push_back(1); }
+    // segment tables
+    std::vector<uint64_t> seg(nseg + 1, 0);
+    std::vector<uint32_t> lbase(nseg), qdeg(nseg), qnlc, qnlc_off(nseg + 1, 0);
+    for (const QPlan &qp : P) {
+        const QueryGraph &q = qp.cs->q;
+        for (uint32_t u = 0; u < q.n; ++u) {
+            const uint32_t sg = qp.seg0 + u;
+            seg[sg + 1] = seg[sg] + qp.lsize[u];
+            lbase[sg] = qp.lbase[u];
+            qdeg[sg] = q.deg(u);
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                const uint32_t l = q.lab[q.nbr[e]];
+                if (qnlc.size() > 2 * qnlc_off[sg] && qnlc[qnlc.size() - 2] == l) qnlc.back()++;
+                else { qnlc.push_back(l); qnlc.push_back(1); }
+            }
+            qnlc_off[sg + 1] = (uint32_t)(qnlc.size() / 2);
         }
-        qnlc_off[u + 1] = (uint32_t)(qnlc.size() / 2);
     }
-    uint32_t *st = nullptr, *d_fcount = nullptr, *d_small = nullptr;
+    uint32_t *st = nullptr, *d_fcount = nullptr, *d_lbase = nullptr, *d_qdeg = nullptr, *d_qnlc = nullptr,
+             *d_qnlc_off = nullptr;
     uint64_t *d_seg = nullptr;
     unsigned long long *d_elems = nullptr;
-    ASDM_TRY(scr.alloc(&st, seg[nq]));
-    ASDM_TRY(scr.alloc(&d_seg, nq + 1));
-    ASDM_TRY(scr.alloc(&d_fcount, nq));
+    ASDM_TRY(scr.alloc(&st, seg[nseg]));
+    ASDM_TRY(scr.upload(&d_seg, seg));
+    ASDM_TRY(scr.upload(&d_lbase, lbase));
+    ASDM_TRY(scr.upload(&d_qdeg, qdeg));
+    if (qnlc.empty()) qnlc.push_back(0);
+    ASDM_TRY(scr.upload(&d_qnlc, qnlc));
+    ASDM_TRY(scr.upload(&d_qnlc_off, qnlc_off));
+    ASDM_TRY(scr.alloc(&d_fcount, nseg));
     ASDM_TRY(scr.alloc(&d_elems, 2));
-    const uint64_t small_n = nq + nq + qnlc.size() + nq + 1;
-    ASDM_TRY(scr.alloc(&d_small, small_n));
-    std::vector<uint32_t> small;
-    small.insert(small.end(), lbase.begin(), lbase.end());
-    small.insert(small.end(), qdeg.begin(), qdeg.end());
-    small.insert(small.end(), qnlc.begin(), qnlc.end());
-    small.insert(small.end(), qnlc_off.begin(), qnlc_off.end());
-    ASDM_CUDA(cudaMemcpyAsync(d_small, small.data(), small.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_seg, seg.data(), (nq + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemsetAsync(d_fcount, 0, nq * sizeof(uint32_t), s));
+    ASDM_CUDA(cudaMemsetAsync(d_fcount, 0, nseg * sizeof(uint32_t), s));
     ASDM_CUDA(cudaMemsetAsync(d_elems, 0, 2 * sizeof(unsigned long long), s));
-    if (seg[nq]) {
-        FilterArgs fa{g, st, d_seg, d_small, d_small + nq, d_small + 2 * nq, d_small + 2 * nq + qnlc.size(), nq, d_fcount};
-        k1_filter<<<grid_for(seg[nq], G->num_sms), kBlock, 0, s>>>(fa);
+    if (seg[nseg]) {
+        FilterArgs fa{g, st, d_seg, d_lbase, d_qdeg, d_qnlc, d_qnlc_off, nseg, d_fcount};
+        k1_filter<<<grid_for(seg[nseg], G->num_sms), kBlock, 0, s>>>(fa);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
     }
-    std::vector<uint32_t> fcount(nq, 0);
-    ASDM_CUDA(cudaMemcpyAsync(fcount.data(), d_fcount, nq * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    std::vector<uint32_t> fcount(nseg, 0);
+    ASDM_CUDA(cudaMemcpyAsync(fcount.data(), d_fcount, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     ASDM_CUDA(cudaStreamSynchronize(s));
 
-    // Root: the three smallest |V_l(u)|/deg(u) kept in a max-heap, then the
-    // first strict minimum of |F(u)|/deg(u) in pop order (selectCFLRoot,
-    // relation/candidate_space.cpp:723-763; same container and comparator).
-    auto cmp = [](const std::pair<uint32_t, double> &a, const std::pair<uint32_t, double> &b) { return a.second < b.second; };
-    std::priority_queue<std::pair<uint32_t, double>, std::vector<std::pair<uint32_t, double>>, decltype(cmp)> pq(cmp);
-    for (uint32_t u = 0; u < nq; ++u) pq.emplace(u, lsize[u] / (double)q.deg(u));
-    while (pq.size() > 3) pq.pop();
-    uint32_t root = 0;
-    double best = g.n;
-    while (!pq.empty()) {
-        const uint32_t u = pq.top().first;
-        pq.pop();
-        const double score = fcount[u] / (double)q.deg(u);
-        if (score < best) { best = score; root = u; }
-    }
-    cs.root = root;
-    // BFS levels with discovery order over (label,id)-sorted query neighbours
-    // (buildCFLBFSTree, :765-816).
-    std::vector<uint32_t> order, rank(nq, kNone);
-    {
+    uint32_t maxwave = 0;
+    for (QPlan &qp : P) {
+        asdm_cs &cs = *qp.cs;
+        const QueryGraph &q = cs.q;
+        const uint32_t nq = q.n;
+        // Root: the three smallest |V_l(u)|/deg(u) kept in a max-heap, then the
+        // first strict minimum of |F(u)|/deg(u) in pop order (selectCFLRoot,
+        // relation/candidate_space.cpp:723-763; same container and comparator).
+        auto cmp = [](const std::pair<uint32_t, double> &x, const std::pair<uint32_t, double> &y) {
+            return x.second < y.second;
+        };
+        std::priority_queue<std::pair<uint32_t, double>, std::vector<std::pair<uint32_t, double>>, decltype(cmp)> pq(cmp);
+        for (uint32_t u = 0; u < nq; ++u) pq.emplace(u, qp.lsize[u] / (double)q.deg(u));
+        while (pq.size() > 3) pq.pop();
+        uint32_t root = 0;
+        double best = g.n;
+        while (!pq.empty()) {
+            const uint32_t u = pq.top().first;
+            pq.pop();
+            const double score = fcount[qp.seg0 + u] / (double)q.deg(u);
+            if (score < best) { best = score; root = u; }
+        }
+        cs.root = root;
+        // BFS levels with discovery order over (label,id)-sorted query
+        // neighbours (buildCFLBFSTree, :765-816); rank = position in that order
+        qp.rank.assign(nq, kNone);
+        qp.order.clear();
         std::vector<uint32_t> frontier{root};
-        rank[root] = 0;
+        qp.rank[root] = 0;
         uint32_t r = 1;
         while (!frontier.empty()) {
             std::vector<uint32_t> next;
             for (uint32_t u : frontier) {
-                order.push_back(u);
+                qp.order.push_back(u);
                 for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                     const uint32_t w = q.nbr[e];
-                    if (rank[w] == kNone) { rank[w] = r++; next.push_back(w); }
+                    if (qp.rank[w] == kNone) { qp.rank[w] = r++; next.push_back(w); }
                 }
             }
             frontier.swap(next);
         }
-        // rank[] above is discovery order == BFS order position
-    }
-    cs.bfs_order = order;
-    cs.ncand.assign(nq, 0);
-    cs.cand_base.assign(nq + 1, 0);
-    bool empty = order.size() != nq;  // unreached query vertices get no candidates
-    for (uint32_t u = 0; u < nq; ++u) empty |= fcount[u] == 0;
-    if (empty) {
-        ASDM_CUDA(cudaEventRecord(ev1, s));
-        ASDM_CUDA(cudaEventSynchronize(ev1));
-        cudaEventElapsedTime(&cs.build_ms, ev0, ev1);
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
+        cs.bfs_order = qp.order;
+        cs.ncand.assign(nq, 0);
+        cs.cand_base.assign(nq + 1, 0);
         cs.nonempty = false;
-        return ASDM_OK;
-    }
-    // waves of the top-down pass
-    std::vector<uint32_t> wave(nq, 0);
-    uint32_t maxwave = 0;
-    for (uint32_t u : order) {
-        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-            const uint32_t p = q.nbr[e];
-            if (rank[p] < rank[u]) wave[u] = std::max(wave[u], wave[p] + 1);
+        qp.empty = qp.order.size() != nq;  // unreached query vertices get no candidates
+        for (uint32_t u = 0; u < nq; ++u) qp.empty |= fcount[qp.seg0 + u] == 0;
+        qp.wave.assign(nq, 0);
+        if (qp.empty) continue;
+        for (uint32_t u : qp.order) {
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                const uint32_t p = q.nbr[e];
+                if (qp.rank[p] < qp.rank[u]) qp.wave[u] = std::max(qp.wave[u], qp.wave[p] + 1);
+            }
+            maxwave = std::max(maxwave, qp.wave[u]);
         }
-        maxwave = std::max(maxwave, wave[u]);
     }
-    // storage S(u): Ctd(u) (+ vertex 0)
+    // storage S(u) = Ctd(u) (+ vertex 0), capacity |V_l(u)| + 1 per segment
+    std::vector<uint64_t> sbase(nseg + 1, 0);
+    for (const QPlan &qp : P)
+        for (uint32_t u = 0; u < qp.cs->q.n; ++u) sbase[qp.seg0 + u + 1] = sbase[qp.seg0 + u] + qp.lsize[u] + 1;
     uint32_t *sbuf = nullptr;
-    std::vector<uint64_t> sbase(nq + 1, 0);
-    for (uint32_t u = 0; u < nq; ++u) sbase[u + 1] = sbase[u] + lsize[u] + 1;
-    ASDM_TRY(scr.alloc(&sbuf, sbase[nq]));
-    std::vector<uint64_t> slen(nq, 0);
-    auto before_mask = [&](uint32_t u) {
-        uint32_t m = kFBit;
-        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e)
-            if (rank[q.nbr[e]] < rank[u]) m |= 1u << (e - q.off[u]);
-        return m;
-    };
+    ASDM_TRY(scr.alloc(&sbuf, sbase[nseg]));
+    std::vector<uint64_t> slen(nseg, 0);
     for (uint32_t w = 0; w <= maxwave; ++w) {
         std::vector<PassDesc> passes;
         std::vector<uint64_t> lens;
-        std::vector<uint32_t> us;
-        for (uint32_t u : order) {
-            if (wave[u] != w) continue;
-            us.push_back(u);
-            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-                const uint32_t p = q.nbr[e];
-                if (rank[p] >= rank[u]) continue;
-                passes.push_back(PassDesc{sbuf + sbase[p], st + seg[u], q.lab[u], 1u << (e - q.off[u])});
-                lens.push_back(slen[p]);
+        std::vector<CompDesc> segs;
+        std::vector<uint32_t> seg_ids;
+        for (const QPlan &qp : P) {
+            if (qp.empty) continue;
+            const QueryGraph &q = qp.cs->q;
+            for (uint32_t u : qp.order) {
+                if (qp.wave[u] != w) continue;
+                const uint32_t su = qp.seg0 + u;
+                uint32_t need = kFBit;
+                for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                    const uint32_t p = q.nbr[e];
+                    if (qp.rank[p] >= qp.rank[u]) continue;
+                    const uint32_t bit = 1u << (e - q.off[u]);
+                    need |= bit;
+                    passes.push_back(PassDesc{sbuf + sbase[qp.seg0 + p], st + seg[su], q.lab[u], bit});
+                    lens.push_back(slen[qp.seg0 + p]);
+                }
+                segs.push_back(CompDesc{st + seg[su], sbuf + sbase[su], qp.lsize[u], need, qp.lbase[u], 1});
+                seg_ids.push_back(su);
             }
         }
         ASDM_TRY(run_passes(G, passes, lens, d_elems));
-        std::vector<CompDesc> segs;
-        for (uint32_t u : us) segs.push_back(CompDesc{st + seg[u], sbuf + sbase[u], lsize[u], before_mask(u), lbase[u], 0});
         std::vector<uint32_t> sizes;
         ASDM_TRY(compact(G, segs, sizes));
-        for (size_t i = 0; i < us.size(); ++i) {
-            const uint32_t u = us[i];
-            slen[u] = sizes[i];
-            if (sizes[i] < lsize[u]) {  // phantom parent: data vertex 0
-                ASDM_CUDA(cudaMemsetAsync(sbuf + sbase[u] + sizes[i], 0, sizeof(uint32_t), s));
-                slen[u] += 1;
-            }
-        }
+        for (size_t i = 0; i < seg_ids.size(); ++i) slen[seg_ids[i]] = sizes[i];
     }
-    // remaining passes: neighbours later in the BFS order
+    // remaining passes (neighbours later in the BFS order), all queries at once
     {
         std::vector<PassDesc> passes;
         std::vector<uint64_t> lens;
-        for (uint32_t u = 0; u < nq; ++u)
-            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-                const uint32_t p = q.nbr[e];
-                if (rank[p] < rank[u]) continue;
-                passes.push_back(PassDesc{sbuf + sbase[p], st + seg[u], q.lab[u], 1u << (e - q.off[u])});
-                lens.push_back(slen[p]);
-            }
+        for (const QPlan &qp : P) {
+            if (qp.empty) continue;
+            const QueryGraph &q = qp.cs->q;
+            for (uint32_t u = 0; u < q.n; ++u)
+                for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                    const uint32_t p = q.nbr[e];
+                    if (qp.rank[p] < qp.rank[u]) continue;
+                    passes.push_back(PassDesc{sbuf + sbase[qp.seg0 + p], st + seg[qp.seg0 + u], q.lab[u],
+                                              1u << (e - q.off[u])});
+                    lens.push_back(slen[qp.seg0 + p]);
+                }
+        }
         ASDM_TRY(run_passes(G, passes, lens, d_elems));
     }
-    // final candidate sets
-    ASDM_TRY(dalloc(&cs.d_cand, seg[nq], s));
+    // final candidate sets into the group's arena
+    auto arena = std::make_shared<CsArena>();
+    arena->stream = s;
+    ASDM_TRY(dalloc(&arena->d_cand, seg[nseg], s));
     {
-        std::vector<uint64_t> cbase(nq + 1, 0);
-        for (uint32_t u = 0; u < nq; ++u) cbase[u + 1] = cbase[u] + lsize[u];
         std::vector<CompDesc> segs;
-        for (uint32_t u = 0; u < nq; ++u) {
-            const uint32_t all = q.deg(u) ? ((q.deg(u) == 32 ? 0xFFFFFFFFu : (1u << q.deg(u)) - 1u)) : 0u;
-            segs.push_back(CompDesc{st + seg[u], cs.d_cand + cbase[u], lsize[u], kFBit | all, lbase[u], 0});
+        std::vector<uint32_t> seg_ids;
+        for (const QPlan &qp : P) {
+            if (qp.empty) continue;
+            const QueryGraph &q = qp.cs->q;
+            for (uint32_t u = 0; u < q.n; ++u) {
+                const uint32_t all = q.deg(u) ? ((q.deg(u) == 32 ? 0xFFFFFFFFu : (1u << q.deg(u)) - 1u)) : 0u;
+                const uint32_t su = qp.seg0 + u;
+                segs.push_back(CompDesc{st + seg[su], arena->d_cand + seg[su], qp.lsize[u], kFBit | all, qp.lbase[u], 0});
+                seg_ids.push_back(su);
+            }
         }
         std::vector<uint32_t> sizes;
         ASDM_TRY(compact(G, segs, sizes));
-        cs.cand_base = cbase;
-        cs.ncand = sizes;
-    }
-    cs.nonempty = true;
-    for (uint32_t u = 0; u < nq; ++u) cs.nonempty &= cs.ncand[u] > 0;
-    if (!cs.nonempty) {
-        ASDM_CUDA(cudaEventRecord(ev1, s));
-        ASDM_CUDA(cudaEventSynchronize(ev1));
-        cudaEventElapsedTime(&cs.build_ms, ev0, ev1);
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
-        return ASDM_OK;
+        std::vector<uint32_t> ncand(nseg, 0);
+        for (size_t i = 0; i < seg_ids.size(); ++i) ncand[seg_ids[i]] = sizes[i];
+        for (QPlan &qp : P) {
+            if (qp.empty) continue;
+            asdm_cs &cs = *qp.cs;
+            bool ok = true;
+            for (uint32_t u = 0; u < cs.q.n; ++u) {
+                cs.ncand[u] = ncand[qp.seg0 + u];
+                cs.cand_base[u] = seg[qp.seg0 + u];
+                ok &= cs.ncand[u] > 0;
+            }
+            cs.cand_base[cs.q.n] = seg[qp.seg0 + cs.q.n];
+            qp.empty = !ok;
+        }
     }
     // candidate edges: rank-in-label -> candidate index maps (reuse st)
-    ASDM_CUDA(cudaMemsetAsync(st, 0xFF, seg[nq] * sizeof(uint32_t), s));
+    ASDM_CUDA(cudaMemsetAsync(st, 0xFF, seg[nseg] * sizeof(uint32_t), s));
     {
-        std::vector<uint64_t> cprefix(nq + 1, 0);
-        std::vector<uint32_t *> maps(nq);
-        for (uint32_t u = 0; u < nq; ++u) maps[u] = st + seg[u];
-        // candidates are not contiguous in d_cand (capacity lsize), so scatter per u
-        for (uint32_t u = 0; u < nq; ++u) {
-            std::vector<uint64_t> one{0, cs.ncand[u]};
-            uint64_t *d_one = nullptr;
+        std::vector<const uint32_t *> cands;
+        std::vector<uint32_t *> maps;
+        std::vector<uint64_t> cpre{0};
+        for (const QPlan &qp : P) {
+            if (qp.empty) continue;
+            for (uint32_t u = 0; u < qp.cs->q.n; ++u) {
+                const uint32_t su = qp.seg0 + u;
+                cands.push_back(arena->d_cand + seg[su]);
+                maps.push_back(st + seg[su]);
+                cpre.push_back(cpre.back() + qp.cs->ncand[u]);
+            }
+        }
+        if (cpre.back()) {
+            const uint32_t **d_cands = nullptr;
             uint32_t **d_maps = nullptr;
-            ASDM_TRY(scr.alloc(&d_one, 2));
-            ASDM_TRY(scr.alloc(&d_maps, 1));
-            ASDM_CUDA(cudaMemcpyAsync(d_one, one.data(), 2 * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-            ASDM_CUDA(cudaMemcpyAsync(d_maps, &maps[u], sizeof(uint32_t *), cudaMemcpyHostToDevice, s));
-            k3_scatter_map<<<grid_for(cs.ncand[u], G->num_sms), kBlock, 0, s>>>(cs.d_cand + cs.cand_base[u], d_one, 1,
+            uint64_t *d_cpre = nullptr;
+            ASDM_TRY(scr.upload(&d_cands, cands));
+            ASDM_TRY(scr.upload(&d_maps, maps));
+            ASDM_TRY(scr.upload(&d_cpre, cpre));
+            k3_scatter_map<<<grid_for(cpre.back(), G->num_sms), kBlock, 0, s>>>(d_cands, d_cpre, (uint32_t)cands.size(),
                                                                                d_maps, g.pos_in_label);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         }
     }
-    const uint32_t ne = q.off[nq];
-    std::vector<EdgeDesc> edges(ne);
-    std::vector<uint64_t> item_base(ne + 1, 0);
-    for (uint32_t u = 0; u < nq; ++u)
-        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-            const uint32_t u2 = q.nbr[e];
-            edges[e] = EdgeDesc{cs.d_cand + cs.cand_base[u], st + seg[u2], cs.ncand[u], q.lab[u2]};
-            item_base[e + 1] = item_base[e] + cs.ncand[u] + 1;
-        }
-    const uint64_t nitems = item_base[ne];
-    EdgeDesc *d_edges = nullptr;
-    uint64_t *d_ib = nullptr, *d_wpos = nullptr, *d_estart = nullptr;
-    uint32_t *d_bad = nullptr;
-    ASDM_TRY(scr.alloc(&d_edges, ne));
-    ASDM_TRY(scr.alloc(&d_ib, ne + 1));
-    ASDM_TRY(scr.alloc(&d_wpos, nitems + 1));
-    ASDM_TRY(scr.alloc(&d_estart, ne));
-    ASDM_TRY(scr.alloc(&d_bad, 1));
-    ASDM_TRY(dalloc(&cs.d_eoff, nitems, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_edges, edges.data(), ne * sizeof(EdgeDesc), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_ib, item_base.data(), (ne + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), s));
-    const unsigned egrid = grid_for(nitems, G->num_sms);
-    k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, cs.d_eoff, nullptr, nullptr, d_elems + 1);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
-    ASDM_TRY(scan_exclusive_u32(cs.d_eoff, d_wpos, nitems, true, s));
-    uint64_t total = 0;
-    ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    ASDM_CUDA(cudaStreamSynchronize(s));
-    ASDM_TRY(dalloc(&cs.d_elist, total, s));
-    k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, cs.d_elist, nullptr);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
-    k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, cs.d_eoff, d_estart, d_bad);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
+    std::vector<EdgeDesc> edges;
+    std::vector<uint64_t> item_base{0};
+    std::vector<uint32_t> edge_first(Q, 0);
+    for (uint32_t qi = 0; qi < Q; ++qi) {
+        const QPlan &qp = P[qi];
+        edge_first[qi] = (uint32_t)edges.size();
+        if (qp.empty) continue;
+        const asdm_cs &cs = *qp.cs;
+        const QueryGraph &q = cs.q;
+        for (uint32_t u = 0; u < q.n; ++u)
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                const uint32_t u2 = q.nbr[e];
+                edges.push_back(EdgeDesc{arena->d_cand + seg[qp.seg0 + u], st + seg[qp.seg0 + u2], cs.ncand[u], q.lab[u2]});
+                item_base.push_back(item_base.back() + cs.ncand[u] + 1);
+            }
+    }
+    const uint32_t ne = (uint32_t)edges.size();
+    const uint64_t nitems = item_base.back();
     std::vector<uint64_t> estart(ne, 0);
-    uint32_t bad = 0;
+    uint64_t total = 0;
+    if (ne) {
+        EdgeDesc *d_edges = nullptr;
+        uint64_t *d_ib = nullptr, *d_wpos = nullptr, *d_estart = nullptr;
+        uint32_t *d_bad = nullptr;
+        ASDM_TRY(scr.upload(&d_edges, edges));
+        ASDM_TRY(scr.upload(&d_ib, item_base));
+        ASDM_TRY(scr.alloc(&d_wpos, nitems + 1));
+        ASDM_TRY(scr.alloc(&d_estart, ne));
+        ASDM_TRY(scr.alloc(&d_bad, 1));
+        ASDM_TRY(dalloc(&arena->d_eoff, nitems, s));
+        ASDM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), s));
+        const unsigned egrid = grid_for(nitems, G->num_sms);
+        k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, nullptr, nullptr, d_elems + 1);
+        ::asdm::count_launch();
+        ASDM_CUDA(cudaGetLastError());
+        ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
+        ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        ASDM_CUDA(cudaStreamSynchronize(s));
+        ASDM_TRY(dalloc(&arena->d_elist, total, s));
+        k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, arena->d_elist, nullptr);
+        ::asdm::count_launch();
+        ASDM_CUDA(cudaGetLastError());
+        k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, arena->d_eoff, d_estart, d_bad);
+        ::asdm::count_launch();
+        ASDM_CUDA(cudaGetLastError());
+        uint32_t bad = 0;
+        ASDM_CUDA(cudaMemcpyAsync(estart.data(), d_estart, ne * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        ASDM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        ASDM_CUDA(cudaStreamSynchronize(s));
+        if (bad) return fail(ASDM_ERR_INVALID, "a candidate-edge list exceeds 2^32 entries");
+    }
     unsigned long long elems[2] = {0, 0};
-    ASDM_CUDA(cudaMemcpyAsync(estart.data(), d_estart, ne * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    ASDM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     ASDM_CUDA(cudaMemcpyAsync(elems, d_elems, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     ASDM_CUDA(cudaEventRecord(ev1, s));
     ASDM_CUDA(cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&cs.build_ms, ev0, ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
-    if (bad) return fail(ASDM_ERR_INVALID, "a candidate-edge list exceeds 2^32 entries");
-    cs.eoff_base.assign(ne, 0);
-    cs.elist_base = estart;
-    cs.etotal.assign(ne, 0);
-    for (uint32_t e = 0; e < ne; ++e) {
-        cs.eoff_base[e] = item_base[e];
-        const uint64_t end = (e + 1 < ne) ? estart[e + 1] : total;
-        cs.etotal[e] = end - estart[e];
-    }
     // K2 scans + K3 scans (count and fill read the same runs) + K1 state words
-    cs.build_bytes = 4ull * (elems[0] + 2 * elems[1]) + 4ull * seg[nq];
+    const uint64_t bytes = 4ull * (elems[0] + 2 * elems[1]) + 4ull * seg[nseg];
+    for (uint32_t qi = 0; qi < Q; ++qi) {
+        QPlan &qp = P[qi];
+        asdm_cs &cs = *qp.cs;
+        cs.build_ms = ms / Q;
+        cs.build_bytes = bytes / Q;
+        cs.arena = arena;
+        cs.d_cand = arena->d_cand;
+        cs.d_eoff = arena->d_eoff;
+        cs.d_elist = arena->d_elist;
+        if (qp.empty) {
+            cs.nonempty = false;
+            continue;
+        }
+        cs.nonempty = true;
+        const QueryGraph &q = cs.q;
+        const uint32_t nq_e = q.off[q.n];
+        cs.eoff_base.assign(nq_e, 0);
+        cs.elist_base.assign(nq_e, 0);
+        cs.etotal.assign(nq_e, 0);
+        for (uint32_t k = 0; k < nq_e; ++k) {
+            const uint32_t e = edge_first[qi] + k;
+            cs.eoff_base[k] = item_base[e];
+            cs.elist_base[k] = estart[e];
+            const uint64_t end = (e + 1 < ne) ? estart[e + 1] : total;
+            cs.etotal[k] = end - estart[e];
+        }
+    }
     return ASDM_OK;
 }
 
+namespace {
 }  // namespace
 }  // namespace asdm
 
@@ -669,11 +747,9 @@ extern "C" int asdm_candidate_space(asdm_graph *g, const uint32_t *q_offsets, co
     auto cs = std::make_unique<asdm_cs>();
     cs->g = g;
     ASDM_TRY(make_query(q_offsets, q_nbrs, q_labels, q_n, cs->q));
-    int rc = build(*cs);
+    int rc = build_batch({cs.get()});
     if (rc != ASDM_OK) {
-        dfree(cs->d_cand, g->stream);
-        dfree(cs->d_eoff, g->stream);
-        dfree(cs->d_elist, g->stream);
+        cs.reset();
         cudaStreamSynchronize(g->stream);
         return rc;
     }
@@ -729,10 +805,7 @@ extern "C" int asdm_cs_read_edges(const asdm_cs *cs, uint32_t u, uint32_t u2, ui
 extern "C" int asdm_cs_free(asdm_cs *cs) {
     if (!cs) return ASDM_OK;
     cudaStream_t s = cs->g->stream;
-    dfree(cs->d_cand, s);
-    dfree(cs->d_eoff, s);
-    dfree(cs->d_elist, s);
+    delete cs;  // the group's arena is freed with its last candidate space
     cudaStreamSynchronize(s);
-    delete cs;
     return ASDM_OK;
 }

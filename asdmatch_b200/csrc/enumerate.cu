@@ -47,8 +47,8 @@ enum : int {
     kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrN = 16
 };
 // Work-donation ring (a bounded multi-producer multi-consumer queue with a
-// sequence number per slot): a record is [level s, lo, hi, idx[0..s-1]].
-constexpr uint32_t kRecWords = 3 + 32;
+// sequence number per slot): a record is [query, level s, lo, hi, idx[0..s-1]].
+constexpr uint32_t kRecWords = 4 + 32;
 constexpr uint64_t kQueueCap = 1u << 16;      // power of two
 constexpr uint32_t kIdlePolls = 1u << 20;     // an idle warp gives up after this many polls
 
@@ -88,6 +88,22 @@ struct EnumArgs {
     unsigned long long count_limit;  // 0 = none
     uint32_t *queue;            // kQueueCap records of kRecWords words
     unsigned long long *qseq;   // kQueueCap slot sequence numbers
+    // batches of queries (enum_batch_kernel): one QDesc per query, root tasks
+    // of query q are task_pre[q] .. task_pre[q+1]
+    const struct QDesc *qd;
+    const unsigned long long *task_pre;
+    uint32_t nquery, maxn, maxnb;
+    unsigned long long *qcounts;
+    unsigned int *qflags;
+};
+
+struct QDesc {
+    const DLevel *lv;
+    const DBack *bk;
+    const uint32_t *conf;
+    const uint32_t *off01;
+    const uint32_t *list01;
+    uint32_t n, nb, nc, n0;
 };
 
 __host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 32; }
@@ -127,7 +143,24 @@ __device__ __forceinline__ uint32_t warp_find_row(const uint32_t *__restrict__ o
     return lo + (31 - __clz(m));
 }
 
-template <uint32_t MODE>
+// Largest i in [0, n) with pre[i] <= t (64-bit prefix array).
+__device__ __forceinline__ uint32_t warp_find_row64(const unsigned long long *__restrict__ pre, uint32_t n,
+                                                    unsigned long long t, uint32_t lane) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t p = lo + lane * step;
+        const uint32_t m = __ballot_sync(kFull, p < hi && pre[p] <= t);
+        const uint32_t nlo = lo + (31 - __clz(m)) * step;
+        hi = min(hi, nlo + step);
+        lo = nlo;
+    }
+    const uint32_t p = lo + lane;
+    const uint32_t m = __ballot_sync(kFull, p < hi && pre[p] <= t);
+    return lo + (31 - __clz(m));
+}
+
+template <uint32_t MODE, bool MULTI = false>
 struct Warp {
     const EnumArgs &a;
     const DLevel *L;
@@ -135,35 +168,51 @@ struct Warp {
     const uint32_t *CF;
     uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur, *fidx;
     uint32_t lane;
+    uint32_t n;            // levels of the current query
+    uint32_t q = 0;        // current query (batches)
     unsigned long long count = 0, inter = 0, elems = 0;
     bool overflow = false;
 
-    __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln)
-        : a(args), L(l), B(b), CF(cf), lane(ln) {
-        const uint32_t n = a.n;
+    // w: this warp's shared-memory words, laid out for queries of up to maxn
+    // levels and maxnb backward edges.
+    __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln,
+                    uint32_t levels, uint32_t maxn, uint32_t maxnb)
+        : a(args), L(l), B(b), CF(cf), lane(ln), n(levels) {
         idx = w;
-        vid = idx + n;
-        buf = vid + n;
-        cnt = buf + 32 * n;
-        pos = cnt + n;
-        dpos = pos + n;
-        dend = dpos + n;
-        drv = dend + n;
-        sstart = drv + n;
-        slen = sstart + a.nb;
-        scur = slen + a.nb;
-        fidx = scur + a.nb;
+        vid = idx + maxn;
+        buf = vid + maxn;
+        cnt = buf + 32 * maxn;
+        pos = cnt + maxn;
+        dpos = pos + maxn;
+        dend = dpos + maxn;
+        drv = dend + maxn;
+        sstart = drv + maxn;
+        slen = sstart + maxnb;
+        scur = slen + maxnb;
+        fidx = scur + maxnb;
+    }
+
+    // Switches to query qq of a batch (its plan is read from global memory).
+    __device__ void bind(uint32_t qq) {
+        if (qq == q) return;
+        flush_count();
+        q = qq;
+        const QDesc d = a.qd[qq];
+        L = d.lv;
+        B = d.bk;
+        CF = d.conf;
+        n = d.n;
     }
 
     __device__ __forceinline__ bool lane_leaf_ok() const {
-        return MODE == ASDM_MODE_COUNT && L[a.n - 1].nback <= kLaneLeafLists;
+        return MODE == ASDM_MODE_COUNT && L[n - 1].nback <= kLaneLeafLists;
     }
 
     // For the level before the last: the candidate index in C(u_last) of every
     // earlier vertex the last level must avoid (kNone when it is not a
     // candidate there, kSelf when it is level d's own vertex).
     __device__ void prepare_lane_leaf(uint32_t d) {
-        const DLevel lvL = L[a.n - 1];
+        const DLevel lvL = L[n - 1];
         if (lane < lvL.nconf) {
             const uint32_t c = CF[lvL.conf_first + lane];
             uint32_t y = kSelf;
@@ -181,7 +230,7 @@ struct Warp {
     // alone.  Returns false (and leaves the survivor to the warp-wide path)
     // when the lists are too long for one lane.
     __device__ bool lane_leaf(uint32_t d, uint32_t x, unsigned long long &out, unsigned long long &touched) {
-        const DLevel lvL = L[a.n - 1];
+        const DLevel lvL = L[n - 1];
         const uint32_t m = lvL.nback;
         const uint32_t *p[kLaneLeafLists];
         uint32_t len[kLaneLeafLists];
@@ -266,11 +315,18 @@ struct Warp {
     // uint64 wrap-around and the caller's count limit.
     __device__ void flush_count() {
         if (lane == 0 && (count || overflow)) {
-            const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], count);
-            uint32_t f = 0;
-            if (overflow || old + count < old) f |= kFlagOverflow;
-            if (a.count_limit && old + count > a.count_limit) f |= kFlagLimit;
-            if (f) atomicOr((unsigned int *)&a.ctr[kCtrFlags], f);
+            if (MULTI) {
+                // per-query totals; an overflow marks only that query
+                const unsigned long long old = atomicAdd(&a.qcounts[q], count);
+                if (overflow || old + count < old) atomicOr(&a.qflags[q], kFlagOverflow);
+                atomicAdd(&a.ctr[kCtrCount], count);
+            } else {
+                const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], count);
+                uint32_t f = 0;
+                if (overflow || old + count < old) f |= kFlagOverflow;
+                if (a.count_limit && old + count > a.count_limit) f |= kFlagLimit;
+                if (f) atomicOr((unsigned int *)&a.ctr[kCtrFlags], f);
+            }
         }
         count = 0;
         overflow = false;
@@ -341,11 +397,12 @@ struct Warp {
         if (pos == ~0ull) return;
         const uint32_t lo = dpos[s] + (dend[s] - dpos[s]) / 2, hi = dend[s];
         uint32_t *rec = a.queue + (pos & (kQueueCap - 1)) * kRecWords;
-        if (lane < s) rec[3 + lane] = idx[lane];
+        if (lane < s) rec[4 + lane] = idx[lane];
         if (lane == 0) {
-            rec[0] = s;
-            rec[1] = lo;
-            rec[2] = hi;
+            rec[0] = q;
+            rec[1] = s;
+            rec[2] = lo;
+            rec[3] = hi;
         }
         __threadfence();
         __syncwarp();
@@ -433,14 +490,14 @@ struct Warp {
             const uint32_t vx = ok ? lv.cand[x] : 0;
             ok = ok && no_conflict(lv, vx);
         }
-        if (d + 2 == a.n && lane_leaf_ok()) {
+        if (d + 2 == n && lane_leaf_ok()) {
             // count the last level of every survivor lane-parallel; survivors
             // with long lists stay buffered for the warp-wide leaf
             unsigned long long c = 0, touched = 0;
             const bool done = ok && lane_leaf(d, x, c, touched);
             ok = ok && !done;
             const uint32_t dm = __ballot_sync(kFull, done);
-            inter += (L[a.n - 1].nback >= 2) ? __popc(dm) : 0;
+            inter += (L[n - 1].nback >= 2) ? __popc(dm) : 0;
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
                 c += __shfl_xor_sync(kFull, c, o);
@@ -467,7 +524,7 @@ struct Warp {
         if (ok) {
             const unsigned long long r = base + __popc(mask & ((1u << lane) - 1));
             if (r < a.row_cap) {
-                uint32_t *row = a.rows + r * a.nq;
+                uint32_t *row = a.rows + r * n;
                 for (uint32_t j = 0; j < d; ++j) row[L[j].u] = vid[j];
                 row[L[d].u] = vx;
             } else {
@@ -522,11 +579,11 @@ struct Warp {
                 ok = ok && no_conflict(lv, vx);
                 const uint32_t mask = __ballot_sync(kFull, ok);
                 total += __popc(mask);
-                if ((MODE & ASDM_MODE_LOCAL) && ok) atomicAdd(&a.local[(unsigned long long)vx * a.nq + lv.u], 1ull);
+                if ((MODE & ASDM_MODE_LOCAL) && ok) atomicAdd(&a.local[(unsigned long long)vx * n + lv.u], 1ull);
                 if (MODE & ASDM_MODE_EMBED) emit_rows(d, vx, ok, mask);
             }
             if ((MODE & ASDM_MODE_LOCAL) && total && lane < d)
-                atomicAdd(&a.local[(unsigned long long)vid[lane] * a.nq + L[lane].u], total);
+                atomicAdd(&a.local[(unsigned long long)vid[lane] * n + L[lane].u], total);
         }
         add_count(total);
     }
@@ -535,7 +592,7 @@ struct Warp {
     __device__ void single(uint32_t d) {
         add_count(1);
         if (MODE & ASDM_MODE_LOCAL) {
-            if (lane <= d) atomicAdd(&a.local[(unsigned long long)vid[lane] * a.nq + L[lane].u], 1ull);
+            if (lane <= d) atomicAdd(&a.local[(unsigned long long)vid[lane] * n + L[lane].u], 1ull);
         }
         if (MODE & ASDM_MODE_EMBED) {
             const uint32_t vx = vid[d];
@@ -544,27 +601,11 @@ struct Warp {
     }
 };
 
-template <uint32_t MODE>
-__global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
-    extern __shared__ __align__(16) uint32_t sm[];
-    DLevel *L = reinterpret_cast<DLevel *>(sm);
-    DBack *B = reinterpret_cast<DBack *>(L + a.n);
-    uint32_t *CF = reinterpret_cast<uint32_t *>(B + a.nb);
-    {
-        const uint32_t *src_l = reinterpret_cast<const uint32_t *>(a.lv);
-        uint32_t *dst_l = reinterpret_cast<uint32_t *>(L);
-        for (uint32_t i = threadIdx.x; i < a.n * (uint32_t)(sizeof(DLevel) / 4); i += blockDim.x) dst_l[i] = src_l[i];
-        const uint32_t *src_b = reinterpret_cast<const uint32_t *>(a.bk);
-        uint32_t *dst_b = reinterpret_cast<uint32_t *>(B);
-        for (uint32_t i = threadIdx.x; i < a.nb * (uint32_t)(sizeof(DBack) / 4); i += blockDim.x) dst_b[i] = src_b[i];
-        for (uint32_t i = threadIdx.x; i < a.nc; i += blockDim.x) CF[i] = a.conf[i];
-    }
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t *wmem = sm + plan_words(a.n, a.nb, a.nc) + warp * warp_words(a.n, a.nb);
-    Warp<MODE> W(a, L, B, CF, wmem, lane);
-    const uint32_t n = a.n;
+// The warp loop shared by the single-query kernel and the batch kernel.
+template <uint32_t MODE, bool MULTI>
+__device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane) {
     volatile unsigned int *flags = reinterpret_cast<volatile unsigned int *>(&a.ctr[kCtrFlags]);
+    const unsigned long long ntasks = MULTI ? a.task_pre[a.nquery] : a.ntasks;
     uint32_t iter = 0;
     bool stop = false, roots_left = true;
     uint64_t deadline = 0;
@@ -577,24 +618,34 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
             if (lane == 0) {
                 atomicAdd(&a.ctr[kCtrActive], 1ull);
                 t = atomicAdd(&a.ctr[kCtrTask], 1ull);
-                if (t >= a.ntasks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+                if (t >= ntasks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
             }
             t = __shfl_sync(kFull, t, 0);
-            if (t < a.ntasks) {
+            if (t < ntasks) {
                 have = true;
+                const uint32_t *off01 = a.off01, *list01 = a.list01;
+                uint32_t n0 = a.n0;
+                if (MULTI) {
+                    const uint32_t qq = warp_find_row64(a.task_pre, a.nquery, t, lane);
+                    W.bind(qq);
+                    t -= a.task_pre[qq];
+                    off01 = a.qd[qq].off01;
+                    list01 = a.qd[qq].list01;
+                    n0 = a.qd[qq].n0;
+                }
                 uint32_t i0, i1 = 0;
-                if (n == 1) {
+                if (W.n == 1) {
                     i0 = (uint32_t)t;
                 } else {
-                    i0 = warp_find_row(a.off01, a.n0, t, lane);
-                    i1 = a.list01[t];
+                    i0 = warp_find_row(off01, n0, t, lane);
+                    i1 = list01[t];
                 }
                 if (lane == 0) {
                     W.idx[0] = i0;
-                    W.vid[0] = L[0].cand[i0];
-                    if (n > 1) {
+                    W.vid[0] = W.L[0].cand[i0];
+                    if (W.n > 1) {
                         W.idx[1] = i1;
-                        W.vid[1] = L[1].cand[i1];
+                        W.vid[1] = W.L[1].cand[i1];
                     }
                 }
                 __syncwarp();
@@ -604,42 +655,44 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
         }
         uint32_t d = 2;
         if (have) {
-            if (n <= 2) {
-                W.single(n - 1);
+            if (W.n <= 2) {
+                W.single(W.n - 1);
                 if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
                 continue;
             }
             const uint32_t len = W.setup(d);
-            if (d == n - 1) {
+            if (d == W.n - 1) {
                 if (len) W.leaf(d);
                 d = 1;
             } else if (len == 0) {
                 d = 1;
-            } else if (d + 2 == n && W.lane_leaf_ok()) {
+            } else if (d + 2 == W.n && W.lane_leaf_ok()) {
                 W.prepare_lane_leaf(d);
             }
         } else {
             const unsigned long long qpos = W.take_queued();
             if (qpos == ~0ull) break;
             const volatile uint32_t *rec = a.queue + (qpos & (kQueueCap - 1)) * kRecWords;
-            base = rec[0];
-            const uint32_t lo = rec[1], hi = rec[2];
+            if (MULTI) W.bind(rec[0]);
+            base = rec[1];
+            const uint32_t lo = rec[2], hi = rec[3];
             if (lane < base) {
-                const uint32_t x = rec[3 + lane];
+                const uint32_t x = rec[4 + lane];
                 W.idx[lane] = x;
-                W.vid[lane] = L[lane].cand[x];
+                W.vid[lane] = W.L[lane].cand[x];
             }
             W.release(qpos);
             __syncwarp();
             d = base;
             W.setup(d);
-            if (d + 2 == n && W.lane_leaf_ok()) W.prepare_lane_leaf(d);
+            if (d + 2 == W.n && W.lane_leaf_ok()) W.prepare_lane_leaf(d);
             if (lane == 0) {
                 W.dpos[d] = lo;
                 W.dend[d] = hi;
             }
             __syncwarp();
         }
+        const uint32_t n = W.n;
         while (d >= base) {
             if ((++iter & 63u) == 0) {
                 uint32_t st = 0, want = 0;
@@ -663,7 +716,7 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
                 if (lane == 0) {
                     W.pos[d] += 1;
                     W.idx[d] = x;
-                    W.vid[d] = L[d].cand[x];
+                    W.vid[d] = W.L[d].cand[x];
                 }
                 __syncwarp();
                 ++d;
@@ -692,6 +745,40 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
         atomicAdd(&a.ctr[kCtrInter], W.inter);
         atomicAdd(&a.ctr[kCtrElems], W.elems);
     }
+}
+
+template <uint32_t MODE>
+__global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    DLevel *L = reinterpret_cast<DLevel *>(sm);
+    DBack *B = reinterpret_cast<DBack *>(L + a.n);
+    uint32_t *CF = reinterpret_cast<uint32_t *>(B + a.nb);
+    {
+        const uint32_t *src_l = reinterpret_cast<const uint32_t *>(a.lv);
+        uint32_t *dst_l = reinterpret_cast<uint32_t *>(L);
+        for (uint32_t i = threadIdx.x; i < a.n * (uint32_t)(sizeof(DLevel) / 4); i += blockDim.x) dst_l[i] = src_l[i];
+        const uint32_t *src_b = reinterpret_cast<const uint32_t *>(a.bk);
+        uint32_t *dst_b = reinterpret_cast<uint32_t *>(B);
+        for (uint32_t i = threadIdx.x; i < a.nb * (uint32_t)(sizeof(DBack) / 4); i += blockDim.x) dst_b[i] = src_b[i];
+        for (uint32_t i = threadIdx.x; i < a.nc; i += blockDim.x) CF[i] = a.conf[i];
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *wmem = sm + plan_words(a.n, a.nb, a.nc) + warp * warp_words(a.n, a.nb);
+    Warp<MODE, false> W(a, L, B, CF, wmem, lane, a.n, a.n, a.nb);
+    warp_loop<MODE, false>(a, W, lane);
+}
+
+// Many queries in one persistent launch (COUNT mode): root tasks of every
+// query form one range claimed by atomicAdd, plans are read from global
+// memory, counts go to per-query totals.
+__global__ void __launch_bounds__(kThreads) enum_batch_kernel(EnumArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *wmem = sm + warp * warp_words(a.maxn, a.maxnb);
+    const QDesc d0 = a.qd[0];
+    Warp<ASDM_MODE_COUNT, true> W(a, d0.lv, d0.bk, d0.conf, wmem, lane, d0.n, a.maxn, a.maxnb);
+    warp_loop<ASDM_MODE_COUNT, true>(a, W, lane);
 }
 
 __global__ void queue_init(unsigned long long *seq) {
@@ -891,6 +978,183 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cleanup();
+    cudaStreamSynchronize(s);
+    return rc;
+}
+
+
+// Batched form: one persistent launch counts every query of a group.
+// counts[i] / status[i] receive each query's result.
+int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg) {
+    cudaStream_t s = G->stream;
+    const uint32_t Q = (uint32_t)cs.size();
+    std::vector<uint32_t> live;  // queries with a non-empty candidate space
+    for (uint32_t i = 0; i < Q; ++i) {
+        counts[i] = 0;
+        status[i] = ASDM_OK;
+        if (cs[i]->nonempty) live.push_back(i);
+    }
+    if (agg) *agg = asdm_run_stats{};
+    if (live.empty()) return ASDM_OK;
+    const uint32_t L = (uint32_t)live.size();
+    // host images of all plans, then one upload
+    std::vector<uint8_t> hp;
+    struct Off { uint64_t lv, bk, cf; };
+    std::vector<Off> offs(L);
+    std::vector<QDesc> qd(L);
+    std::vector<unsigned long long> task_pre(L + 1, 0);
+    uint32_t maxn = 1, maxnb = 1;
+    auto append = [&](const void *src, size_t bytes) {
+        const uint64_t at = (hp.size() + 15) & ~15ull;
+        hp.resize(at + bytes);
+        if (bytes && src) std::memcpy(hp.data() + at, src, bytes);
+        return at;
+    };
+    for (uint32_t li = 0; li < L; ++li) {
+        const asdm_cs &c = *cs[live[li]];
+        const asdm_plan &plan = *plans[live[li]];
+        const uint32_t n = c.q.n;
+        std::vector<DLevel> lv(n);
+        std::vector<DBack> bk;
+        std::vector<uint32_t> cf;
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t u = plan.order[k];
+            lv[k].cand = c.d_cand + c.cand_base[u];
+            lv[k].ncand = c.ncand[u];
+            lv[k].u = u;
+            lv[k].nback = (uint32_t)plan.back[k].size();
+            lv[k].back_first = (uint32_t)bk.size();
+            for (auto &jb : plan.back[k])
+                bk.push_back(DBack{c.d_eoff + c.eoff_base[jb.second], c.d_elist + c.elist_base[jb.second], jb.first, 0});
+            lv[k].nconf = (uint32_t)plan.conf[k].size();
+            lv[k].conf_first = (uint32_t)cf.size();
+            cf.insert(cf.end(), plan.conf[k].begin(), plan.conf[k].end());
+        }
+        offs[li].lv = append(lv.data(), lv.size() * sizeof(DLevel));
+        offs[li].bk = append(bk.data(), bk.size() * sizeof(DBack));
+        offs[li].cf = append(cf.data(), cf.size() * sizeof(uint32_t));
+        qd[li].n = n;
+        qd[li].nb = (uint32_t)bk.size();
+        qd[li].nc = (uint32_t)cf.size();
+        unsigned long long nt;
+        if (n == 1) {
+            nt = c.ncand[plan.order[0]];
+        } else {
+            const uint32_t e01 = plan.back[1][0].second;
+            qd[li].off01 = c.d_eoff + c.eoff_base[e01];
+            qd[li].list01 = c.d_elist + c.elist_base[e01];
+            qd[li].n0 = c.ncand[plan.order[0]];
+            nt = c.etotal[e01];
+        }
+        task_pre[li + 1] = task_pre[li] + nt;
+        maxn = std::max(maxn, n);
+        maxnb = std::max(maxnb, (uint32_t)bk.size());
+    }
+    const uint64_t qd_at = append(nullptr, L * sizeof(QDesc));
+    const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
+    uint8_t *d_buf = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr;
+    uint32_t *d_queue = nullptr;
+    unsigned int *d_qflags = nullptr;
+    int rc = ASDM_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    do {
+        if ((rc = dalloc(&d_buf, hp.size(), s)) || (rc = dalloc(&d_ctr, kCtrN, s)) || (rc = dalloc(&d_qcounts, L, s)) ||
+            (rc = dalloc(&d_qflags, L, s)) || (rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s)))
+            break;
+        for (uint32_t li = 0; li < L; ++li) {
+            qd[li].lv = reinterpret_cast<const DLevel *>(d_buf + offs[li].lv);
+            qd[li].bk = reinterpret_cast<const DBack *>(d_buf + offs[li].bk);
+            qd[li].conf = reinterpret_cast<const uint32_t *>(d_buf + offs[li].cf);
+        }
+        std::memcpy(hp.data() + qd_at, qd.data(), L * sizeof(QDesc));
+        if (cudaMemcpyAsync(d_buf, hp.data(), hp.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemsetAsync(d_ctr, 0, kCtrN * sizeof(unsigned long long), s) != cudaSuccess ||
+            cudaMemsetAsync(d_qcounts, 0, L * sizeof(unsigned long long), s) != cudaSuccess ||
+            cudaMemsetAsync(d_qflags, 0, L * sizeof(unsigned int), s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "batch upload failed");
+            break;
+        }
+        unsigned long long *d_seq = reinterpret_cast<unsigned long long *>(d_queue + kQueueCap * kRecWords);
+        queue_init<<<(unsigned)(kQueueCap / 256), 256, 0, s>>>(d_seq);
+        ::asdm::count_launch();
+        EnumArgs a{};
+        a.ctr = d_ctr;
+        a.queue = d_queue;
+        a.qseq = d_seq;
+        a.qd = reinterpret_cast<const QDesc *>(d_buf + qd_at);
+        a.task_pre = reinterpret_cast<const unsigned long long *>(d_buf + tp_at);
+        a.nquery = L;
+        a.maxn = maxn;
+        a.maxnb = maxnb;
+        a.qcounts = d_qcounts;
+        a.qflags = d_qflags;
+        a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
+        const uint32_t smem = 4u * kWarps * warp_words(maxn, maxnb);
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+        if (task_pre[L]) {
+            if (cudaFuncSetAttribute(enum_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "shared-memory opt-in failed");
+                break;
+            }
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enum_batch_kernel, kThreads, smem);
+            if (per_sm <= 0) {
+                rc = fail(ASDM_ERR_INVALID, "batch plans too large for shared memory (%u bytes)", smem);
+                break;
+            }
+            enum_batch_kernel<<<(unsigned)(per_sm * G->num_sms), kThreads, smem, s>>>(a);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "batch kernel launch failed");
+                break;
+            }
+        }
+        cudaEventRecord(e1, s);
+        unsigned long long ctr[kCtrN];
+        std::vector<unsigned long long> qc(L);
+        std::vector<unsigned int> qf(L);
+        if (cudaMemcpyAsync(ctr, d_ctr, sizeof ctr, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(qc.data(), d_qcounts, L * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(qf.data(), d_qflags, L * sizeof(unsigned int), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "batch readback failed");
+            break;
+        }
+        cudaError_t se = cudaStreamSynchronize(s);
+        if (se != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "batch kernel failed: %s", cudaGetErrorString(se));
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const uint32_t gflags = (uint32_t)ctr[kCtrFlags];
+        for (uint32_t li = 0; li < L; ++li) {
+            const uint32_t i = live[li];
+            counts[i] = qc[li];
+            if (gflags & kFlagInternal) status[i] = ASDM_ERR_INTERNAL;
+            else if (gflags & kFlagTimeout) status[i] = ASDM_ERR_TIMEOUT;
+            else if (qf[li] & kFlagOverflow) status[i] = ASDM_ERR_OVERFLOW;
+        }
+        if (agg) {
+            agg->count = ctr[kCtrCount];
+            agg->intersections = ctr[kCtrInter];
+            agg->list_bytes = 4ull * ctr[kCtrElems];
+            agg->tasks = task_pre[L];
+            agg->kernel_ms = ms;
+        }
+        if (gflags & kFlagInternal) rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
+        else if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
+    } while (false);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    dfree(d_buf, s);
+    dfree(d_ctr, s);
+    dfree(d_qcounts, s);
+    dfree(d_qflags, s);
+    dfree(d_queue, s);
     cudaStreamSynchronize(s);
     return rc;
 }

@@ -239,13 +239,14 @@ def main():
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
 
-    def one_step():
+    def plain_step():
+        """The plain form: one query per launch sequence (candidate space, plan, count)."""
         stats = {"kernel_ms": 0.0, "list_bytes": 0, "cs_ms": 0.0, "cs_bytes": 0, "matches": 0, "inter": 0}
         for q, want in zip(qs, counts):
             cs = A.CandidateSpace(dg, q)
-            b, ms = cs.build_stats()
+            b, ms_ = cs.build_stats()
             stats["cs_bytes"] += b
-            stats["cs_ms"] += ms
+            stats["cs_ms"] += ms_
             if cs.nonempty:
                 r = A.adaptive_share_join(cs)
                 stats["kernel_ms"] += r.kernel_ms
@@ -260,46 +261,64 @@ def main():
             stats["matches"] += got
         return stats
 
+    packed = A.BatchInput(qs)
+
+    def batched_step():
+        """The batched form: the whole batch through asdm_run_batch."""
+        st = A.run_batch_packed(dg, packed)
+        if packed.counts.tolist() != counts or packed.status.any():
+            raise SystemExit("batched counts differ from the screened counts")
+        return {"kernel_ms": st.kernel_ms, "list_bytes": st.list_bytes, "cs_ms": st.build_ms,
+                "cs_bytes": st.build_bytes, "matches": st.count, "inter": st.intersections}
+
+    def timed(step_fn, steps):
+        times, agg = [], None
+        for _ in range(steps):
+            flush_l2(torch, dev)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = step_fn()
+            e1.record(stream)
+            e1.synchronize()
+            torch.cuda.synchronize(dev)
+            times.append(e0.elapsed_time(e1))
+            agg = st if agg is None else {k: agg[k] + st[k] for k in agg}
+        ms_ = statistics.mean(times)
+        if world > 1:
+            t = torch.tensor([ms_], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_ = float(t.item())
+        return ms_, agg
+
     for _ in range(args.warmup):
-        one_step()
-    times, agg = [], None
+        batched_step()
     sampler = ClockSampler(local)
     launches0 = A.kernel_launches()
     sampler.start()
-    for _ in range(args.steps):
-        flush_l2(torch, dev)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st = one_step()
-        e1.record(stream)
-        e1.synchronize()
-        torch.cuda.synchronize(dev)
-        times.append(e0.elapsed_time(e1))
-        agg = st if agg is None else {k: agg[k] + st[k] for k in agg}
+    ms, agg = timed(batched_step, args.steps)
     clocks = sampler.stop()
     launches = A.kernel_launches() - launches0
-    ms = statistics.mean(times)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": ms, "queries": Q, "launches": launches // args.steps}))
         return
+    # the plain form, for the batched / plain ratio
+    for _ in range(max(1, args.warmup // 2)):
+        plain_step()
+    plain_ms, plain_agg = timed(plain_step, args.steps)
     # end to end through the one-call C ABI (asdm_run_batch) from host buffers
     e2e_times = []
-    h2d = sum(4 * (q.n + 1) + 4 * q.m2 + 4 * q.n for q in qs)
+    h2d = packed.nbytes()
     d2h = Q * (8 + 4)
     for _ in range(args.steps):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        got, status = A.run_batch(dg, qs)
+        A.run_batch_packed(dg, packed)
         e2e_times.append(time.perf_counter() - t0)
-        if got.tolist() != counts or any(status):
+        if packed.counts.tolist() != counts or packed.status.any():
             raise SystemExit("batch counts differ from the screened counts")
     e2e_s = statistics.mean(e2e_times)
     if world > 1:
@@ -315,7 +334,7 @@ def main():
     steps = args.steps
     enum_ms, cs_ms = agg["kernel_ms"] / steps, agg["cs_ms"] / steps
     if enum_ms >= cs_ms:
-        dom, bytes_, kms = "enum_kernel (K4-K8 warp DFS)", agg["list_bytes"] / steps, enum_ms
+        dom, bytes_, kms = "enum_batch_kernel (K4-K8 warp DFS, batched)", agg["list_bytes"] / steps, enum_ms
     else:
         dom, bytes_, kms = "candidate space K1-K3", agg["cs_bytes"] / steps, cs_ms
     achieved = bytes_ / (kms * 1e-3) / 1e9 if kms > 0 else 0.0
@@ -337,16 +356,24 @@ def main():
         "vs_baseline": None,
         "dtype": "uint32 ids / uint64 counts",
         "data": "synthetic (seeded generators; no dataset download)",
-        "config": dict(cfg, l2="flushed (256 MB write) before every timed step", form="plain: one query per launch sequence",
+        "config": dict(cfg, l2="flushed (256 MB write) before every timed step",
+                       form="batched: asdm_run_batch (one launch per CFL phase for the group, one persistent "
+                            "enumeration kernel over all (query, root task) pairs); planner: candidate-size cost model",
                        matches_per_step=agg["matches"] // steps,
                        matches_per_s=world * (agg["matches"] // steps) / (ms / 1e3),
                        intersections_per_step=agg["inter"] // steps,
-                       enum_kernel_ms_per_step=enum_ms, cs_build_ms_per_step=cs_ms),
+                       enum_kernel_ms_per_step=enum_ms, cs_build_ms_per_step=cs_ms,
+                       plain_form={"queries_per_s": world * Q / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                                   "enum_kernel_ms_per_step": plain_agg["kernel_ms"] / steps,
+                                   "cs_build_ms_per_step": plain_agg["cs_ms"] / steps,
+                                   "what": "one query per launch sequence (asdm_candidate_space, asdm_plan_create, "
+                                           "asdm_run_plan)"},
+                       batched_over_plain=plain_ms / ms),
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bytes_, "device_ms_per_step": kms, "traffic": traffic},
         "e2e": {"value": world * Q / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "via": "asdm_run_batch (C ABI) from host arrays"},
+                "via": "asdm_run_batch (C ABI) from host arrays, wall clock"},
         "gpu_launches": launches // steps,
         "clocks": clocks,
     }

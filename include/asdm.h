@@ -164,6 +164,8 @@ typedef struct asdm_run_stats {
     uint64_t list_bytes;     /* algorithmic bytes of lists read by the kernels  */
     uint64_t tasks;          /* root tasks processed                            */
     double kernel_ms;        /* device time of the enumeration kernels          */
+    double build_ms;         /* device time of the candidate-space build (K1-K3) */
+    uint64_t build_bytes;    /* algorithmic bytes of that build                  */
 } asdm_run_stats;
 
 /* Exact enumeration of one query over its candidate space.  Replaces
@@ -194,15 +196,19 @@ int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q
                      const uint32_t *q_labels, uint32_t q_n, const asdm_run_opts *opts,
                      asdm_run_stats *stats);
 
-/* Many queries against one resident data graph (no reference counterpart; the
- * reference runs one query per process).  Query i is the CSR slice
- * q_offsets[q_off_base[i] ..], q_nbrs[q_nbr_base[i] ..], q_labels[q_lab_base[i] ..]
- * with q_sizes[i] vertices.  counts[i] and status[i] receive each query's
- * result; the call returns ASDM_OK when every status is ASDM_OK. */
+/* Many queries against one resident data graph, batched (no reference
+ * counterpart; the reference runs one query per process).  Query i is the CSR
+ * slice q_offsets[q_off_base[i] ..], q_nbrs[q_nbr_base[i] ..],
+ * q_labels[q_lab_base[i] ..] with q_sizes[i] vertices.  Queries are grouped
+ * (up to 16 GiB of candidate-space state per group); each group builds its
+ * candidate spaces with one launch per CFL phase and counts with one
+ * persistent kernel over all (query, root task) pairs.  counts[i] and
+ * status[i] receive each query's result; stats (nullable) the totals; the
+ * call returns ASDM_OK when every status is ASDM_OK. */
 int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
                    const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
                    const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
-                   uint64_t *counts, int *status);
+                   uint64_t *counts, int *status, asdm_run_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -189,3 +189,37 @@ def test_disconnected_query_has_no_candidates(dg_c0):
     q = A.HostGraph.from_edges(4, [0, 0, 0, 0], [(0, 1), (2, 3)])
     r = A.match(dg_c0, q)
     assert r.count == 0 and not r.nonempty
+
+
+def test_batched_form_matches_golden(golden, c0_files, c0d_files, dg_c0, dg_c0d, edge_files):
+    _, _, qs, _ = c0_files
+    counts, status = A.run_batch(dg_c0, qs)
+    assert status.tolist() == [0] * len(qs)
+    assert counts.tolist() == [r["count"] for r in golden["sets"]["c0"]]
+    _, _, by_size = c0d_files
+    recs = golden["sets"]["c0d"]
+    counts, status = A.run_batch(dg_c0d, [by_size[r["size"]][0][r["index"]] for r in recs])
+    assert status.tolist() == [0] * len(recs)
+    assert counts.tolist() == [r["count"] for r in recs]
+    # hand-built corner cases (2-vertex query, empty candidate spaces, cliques) in one batch,
+    # interleaved with ordinary queries
+    recs = golden["sets"]["edge"]
+    mixed = []
+    for i, r in enumerate(recs):
+        mixed.append(edge_files[r["name"]][0])
+        mixed.append(qs[i])
+    want = []
+    for i, r in enumerate(recs):
+        want += [r["count"], golden["sets"]["c0"][i]["count"]]
+    counts, status = A.run_batch(dg_c0, mixed)
+    assert status.tolist() == [0] * len(mixed)
+    assert counts.tolist() == want
+
+
+def test_batched_time_limit_marks_every_query(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    heavy = sorted(golden["sets"]["c0d"], key=lambda r: -r["count"])[:3]
+    counts, status = A.run_batch(dg_c0d, [by_size[r["size"]][0][r["index"]] for r in heavy], time_limit_s=1e-7)
+    assert all(s == A.ERR_TIMEOUT for s in status.tolist())
+    counts, status = A.run_batch(dg_c0d, [by_size[r["size"]][0][r["index"]] for r in heavy])
+    assert counts.tolist() == [r["count"] for r in heavy]
