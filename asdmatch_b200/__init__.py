@@ -96,6 +96,12 @@ _plan_free = _sig("asdm_plan_free", C.c_int, [_vp])
 _run_plan = _sig("asdm_run_plan", C.c_int, [_vp, _vp, C.POINTER(RunOpts), C.POINTER(RunStats)])
 _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(RunOpts),
                                                   C.POINTER(RunStats)])
+class Tuning(C.Structure):
+    _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32)]
+
+
+_set_tuning = _sig("asdm_graph_set_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
+_get_tuning = _sig("asdm_graph_get_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -201,6 +207,14 @@ class DeviceGraph:
         self._h = h
         self.n = g.n
         self.host = g
+
+    def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int):
+        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max))), "tuning")
+
+    def tuning(self):
+        t = Tuning()
+        _check(_get_tuning(self._h, C.byref(t)))
+        return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max}
 
     def stream(self) -> int:
         """cudaStream_t (as an int) the library uses for this graph."""
@@ -452,3 +466,34 @@ def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float
     b = BatchInput(queries)
     run_batch_packed(dg, b, time_limit_s)
     return b.counts.copy(), b.status.copy()
+
+
+def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
+             min_blocks=(1, 4, 5, 6), lane_leaf=(32, 96, 256)):
+    """Times the caller's batch under every kernel configuration and keeps the
+    fastest on `dg` (device time between CUDA events on the library's stream).
+    Returns (best, table)."""
+    import torch
+    stream = torch.cuda.ExternalStream(dg.stream())
+    want = None
+    table = []
+    for mb in min_blocks:
+        for ll in lane_leaf:
+            dg.set_tuning(mb, ll)
+            run_batch_packed(dg, batch)  # warm
+            if want is None:
+                want = batch.counts.copy()
+            elif not np.array_equal(batch.counts, want):
+                raise AsdmError(ERR_INTERNAL, "tuning changed a count")
+            times = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                run_batch_packed(dg, batch)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "ms": min(times)})
+    best = min(table, key=lambda r: r["ms"])
+    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"])
+    return best, table

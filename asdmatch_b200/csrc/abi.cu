@@ -89,6 +89,21 @@ extern "C" int asdm_graph_stream(asdm_graph *g, void **stream) {
     return ASDM_OK;
 }
 
+extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
+    if (!g || !t) return fail(ASDM_ERR_INVALID, "null argument");
+    if (t->enum_min_blocks != 1 && (t->enum_min_blocks < 4 || t->enum_min_blocks > 6))
+        return fail(ASDM_ERR_INVALID, "enum_min_blocks must be 1, 4, 5 or 6");
+    if (t->lane_leaf_max > 4096) return fail(ASDM_ERR_INVALID, "lane_leaf_max must be <= 4096");
+    g->tuning = *t;
+    return ASDM_OK;
+}
+
+extern "C" int asdm_graph_get_tuning(const asdm_graph *g, asdm_tuning *t) {
+    if (!g || !t) return fail(ASDM_ERR_INVALID, "null argument");
+    *t = g->tuning;
+    return ASDM_OK;
+}
+
 extern "C" int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms) {
     if (!cs) return fail(ASDM_ERR_INVALID, "null argument");
     if (build_bytes) *build_bytes = cs->build_bytes;

@@ -86,6 +86,7 @@ struct EnumArgs {
     uint64_t row_cap;
     uint64_t limit_ns;          // 0 = none; else per-warp wall-clock budget
     unsigned long long count_limit;  // 0 = none
+    uint32_t lane_leaf_max;     // longest shortest-list a lane evaluates alone at the last level
     uint32_t *queue;            // kQueueCap records of kRecWords words
     unsigned long long *qseq;   // kQueueCap slot sequence numbers
     // batches of queries (enum_batch_kernel): one QDesc per query, root tasks
@@ -112,7 +113,6 @@ __host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { ret
 // survivor) when it has at most this many earlier neighbours and its shortest
 // list is at most kLaneLeafMax long.
 constexpr uint32_t kLaneLeafLists = 4;
-constexpr uint32_t kLaneLeafMax = 96;
 constexpr uint32_t kSelf = 0xFFFFFFFEu;
 
 __host__ __device__ inline uint32_t plan_words(uint32_t n, uint32_t nb, uint32_t nc) {
@@ -249,7 +249,7 @@ struct Warp {
                 if (len[k] < best) { best = len[k]; bi = k; }
             }
         }
-        if (m > 1 && best > kLaneLeafMax) return false;
+        if (m > 1 && best > a.lane_leaf_max) return false;
         touched += tot;
         unsigned long long c = 0;
         if (m == 1) {
@@ -772,7 +772,8 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
 // Many queries in one persistent launch (COUNT mode): root tasks of every
 // query form one range claimed by atomicAdd, plans are read from global
 // memory, counts go to per-query totals.
-__global__ void __launch_bounds__(kThreads) enum_batch_kernel(EnumArgs a) {
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) enum_batch_kernel(EnumArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *wmem = sm + warp * warp_words(a.maxn, a.maxnb);
@@ -904,6 +905,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         a.qseq = reinterpret_cast<unsigned long long *>(d_queue + kQueueCap * kRecWords);
         a.limit_ns = opt.time_limit_s > 0 ? (uint64_t)(opt.time_limit_s * 1e9) : 0;
         a.count_limit = opt.count_limit;
+        a.lane_leaf_max = G->tuning.lane_leaf_max;
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -1095,18 +1097,27 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
+        a.lane_leaf_max = G->tuning.lane_leaf_max;
         if (task_pre[L]) {
-            if (cudaFuncSetAttribute(enum_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            // register-budget variant chosen by the tuner (min blocks per SM)
+            void (*k)(EnumArgs) = enum_batch_kernel<1>;
+            switch (G->tuning.enum_min_blocks) {
+                case 4: k = enum_batch_kernel<4>; break;
+                case 5: k = enum_batch_kernel<5>; break;
+                case 6: k = enum_batch_kernel<6>; break;
+                default: break;
+            }
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
                 rc = fail(ASDM_ERR_CUDA, "shared-memory opt-in failed");
                 break;
             }
             int per_sm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enum_batch_kernel, kThreads, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
             if (per_sm <= 0) {
                 rc = fail(ASDM_ERR_INVALID, "batch plans too large for shared memory (%u bytes)", smem);
                 break;
             }
-            enum_batch_kernel<<<(unsigned)(per_sm * G->num_sms), kThreads, smem, s>>>(a);
+            k<<<(unsigned)(per_sm * G->num_sms), kThreads, smem, s>>>(a);
             ::asdm::count_launch();
             if (cudaGetLastError() != cudaSuccess) {
                 rc = fail(ASDM_ERR_CUDA, "batch kernel launch failed");
@@ -1332,6 +1343,7 @@ extern "C" int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, d
     a.qseq = d_seq;
     a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
     a.count_limit = count_limit;
+    a.lane_leaf_max = G->tuning.lane_leaf_max;
     if (a.ntasks) {
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         ASDM_TRY(launch<ASDM_MODE_COUNT>(a, smem, G->num_sms, s));

@@ -262,6 +262,7 @@ def main():
         return stats
 
     packed = A.BatchInput(qs)
+    tune_best, tune_table = A.autotune(dg, packed)  # untimed: picks the kernel knobs on this batch
 
     def batched_step():
         """The batched form: the whole batch through asdm_run_batch."""
@@ -368,7 +369,8 @@ def main():
                                    "cs_build_ms_per_step": plain_agg["cs_ms"] / steps,
                                    "what": "one query per launch sequence (asdm_candidate_space, asdm_plan_create, "
                                            "asdm_run_plan)"},
-                       batched_over_plain=plain_ms / ms),
+                       batched_over_plain=plain_ms / ms,
+                       autotune={"chosen": tune_best, "table": tune_table}),
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": bytes_, "device_ms_per_step": kms, "traffic": traffic},

@@ -97,6 +97,23 @@ int asdm_gen_query(const asdm_host_graph *g, uint32_t size, int density, uint64_
 int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, const uint32_t *labels,
                       uint32_t n, uint64_t m2, uint32_t nlabels, asdm_graph **out);
 int asdm_graph_free(asdm_graph *g);
+/* Knobs of the enumeration kernels, per data graph; chosen by the autotuner
+ * (asdmatch_b200.autotune) by timing the caller's own batch.
+ *   enum_min_blocks: register budget of the batched enumeration kernel, as
+ *     resident 256-thread blocks per SM it must allow (1 = compiler's choice,
+ *     4, 5 or 6); more blocks hide more load latency but spill registers.
+ *   lane_leaf_max: the last query level is evaluated one partial match per
+ *     lane (instead of one per warp) when its shortest list has at most this
+ *     many entries (the merge / gallop split of the intersection).
+ * No reference counterpart (the reference's intersection method is a
+ * compile-time switch, config/config.h:16-20). */
+typedef struct asdm_tuning {
+    uint32_t enum_min_blocks;
+    uint32_t lane_leaf_max;
+} asdm_tuning;
+int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t);
+int asdm_graph_get_tuning(const asdm_graph *g, asdm_tuning *t);
+
 /* The CUDA stream (cudaStream_t) the library runs this graph's work on, so a
  * caller can record events around it.  No reference counterpart. */
 int asdm_graph_stream(asdm_graph *g, void **stream);

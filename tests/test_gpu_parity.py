@@ -223,3 +223,18 @@ def test_batched_time_limit_marks_every_query(golden, c0d_files, dg_c0d):
     assert all(s == A.ERR_TIMEOUT for s in status.tolist())
     counts, status = A.run_batch(dg_c0d, [by_size[r["size"]][0][r["index"]] for r in heavy])
     assert counts.tolist() == [r["count"] for r in heavy]
+
+
+def test_every_tuning_gives_the_same_counts(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    recs = golden["sets"]["c0d"]
+    b = A.BatchInput([by_size[r["size"]][0][r["index"]] for r in recs])
+    want = [r["count"] for r in recs]
+    for mb in (1, 4, 5, 6):
+        for ll in (0, 32, 4096):
+            dg_c0d.set_tuning(mb, ll)
+            A.run_batch_packed(dg_c0d, b)
+            assert b.counts.tolist() == want, (mb, ll)
+    best, table = A.autotune(dg_c0d, b, reps=1, lane_leaf=(96,))
+    assert len(table) == 4 and best in table
+    dg_c0d.set_tuning(1, 96)
