@@ -20,8 +20,8 @@
 // the completion count to every prefix vertex (produceResult's
 // ++gLocalCount[φ(u)][u], matching/join.cpp:1035-1041); EMBED mode also
 // writes each match as a row indexed by query vertex (COLLECT_RESULT,
-// :1032-1034).  Root tasks are the candidate edges of the first two levels,
-// claimed with one atomicAdd each, so power-law hubs are split across warps.
+// :1032-1034).  Root tasks are the candidates of the first level, claimed
+// with one atomicAdd each; hubs are split across warps by work donation.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -76,10 +76,9 @@ struct EnumArgs {
     const DBack *bk;
     const uint32_t *conf;
     uint32_t n, nb, nc, nq;
-    uint64_t ntasks;
-    const uint32_t *off01;   // candidate-edge offsets of the level-0 -> level-1 edge
-    const uint32_t *list01;
-    uint32_t n0;
+    unsigned long long ntasks;  // root blocks
+    unsigned long long pairs;   // (level-0, level-1) candidate pairs (level-0 candidates when n == 1)
+    unsigned long long blk;     // pairs per root block
     unsigned long long *ctr;
     unsigned long long *local;  // |Vg| x nq, MODE_LOCAL
     uint32_t *rows;             // row_cap x nq, MODE_EMBED
@@ -102,9 +101,8 @@ struct QDesc {
     const DLevel *lv;
     const DBack *bk;
     const uint32_t *conf;
-    const uint32_t *off01;
-    const uint32_t *list01;
-    uint32_t n, nb, nc, n0;
+    unsigned long long pairs, blk;
+    uint32_t n, nb, nc, pad;
 };
 
 __host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 32; }
@@ -125,15 +123,15 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
-// Largest i in [0, n0) with off[i] <= t, given off[0] <= t < off[n0]:
+// Largest i in [0, n) with off[i] <= t, given off[0] <= t < off[n]:
 // 32-way search, every lane probes one point per round.
-__device__ __forceinline__ uint32_t warp_find_row(const uint32_t *__restrict__ off, uint32_t n0, uint64_t t, uint32_t lane) {
-    uint32_t lo = 0, hi = n0;
+__device__ __forceinline__ uint32_t warp_find_row32(const uint32_t *__restrict__ off, uint32_t n, unsigned long long t,
+                                                    uint32_t lane) {
+    uint32_t lo = 0, hi = n;
     while (hi - lo > 32) {
         const uint32_t step = (hi - lo + 31) / 32;
         const uint32_t p = lo + lane * step;
-        const bool pred = p < hi && off[p] <= t;
-        const uint32_t m = __ballot_sync(kFull, pred);
+        const uint32_t m = __ballot_sync(kFull, p < hi && off[p] <= t);
         const uint32_t nlo = lo + (31 - __clz(m)) * step;
         hi = min(hi, nlo + step);
         lo = nlo;
@@ -535,20 +533,21 @@ struct Warp {
 
     // The last level: count (and in LOCAL/EMBED modes, emit) its matches.
     __device__ void leaf(uint32_t d) {
+        // driver positions [lo, hi): the whole list, or a root block's part of it
         const DLevel lv = L[d];
         const uint32_t dslot = lv.back_first + drv[d];
         const uint32_t *dl = B[dslot].list + sstart[dslot];
-        const uint32_t dlen = slen[dslot];
+        const uint32_t lo = dpos[d], hi = dend[d];
         unsigned long long total = 0;
         if (MODE == ASDM_MODE_COUNT) {
             if (lv.nback == 1) {
-                total = dlen;
+                total = hi - lo;
             } else {
-                for (uint32_t p0 = 0; p0 < dlen; p0 += 32) {
+                for (uint32_t p0 = lo; p0 < hi; p0 += 32) {
                     const uint32_t p = p0 + lane;
-                    const bool valid = p < dlen;
+                    const bool valid = p < hi;
                     const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
-                    const bool ok = probe(lv, dslot, x, valid, min(31u, dlen - 1 - p0));
+                    const bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0));
                     total += __popc(__ballot_sync(kFull, ok));
                 }
             }
@@ -564,17 +563,17 @@ struct Warp {
                         const uint32_t *lst = B[sl].list + sstart[sl];
                         const uint32_t len = slen[sl];
                         const uint32_t q = lower_bound_u32(lst, len, y);
-                        present = q < len && lst[q] == y;
+                        present = q < len && lst[q] == y && (sl != dslot || (q >= lo && q < hi));
                     }
                 }
                 total -= __popc(__ballot_sync(kFull, present));
             }
         } else {
-            for (uint32_t p0 = 0; p0 < dlen; p0 += 32) {
+            for (uint32_t p0 = lo; p0 < hi; p0 += 32) {
                 const uint32_t p = p0 + lane;
-                const bool valid = p < dlen;
+                const bool valid = p < hi;
                 const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
-                bool ok = probe(lv, dslot, x, valid, min(31u, dlen - 1 - p0));
+                bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0));
                 const uint32_t vx = ok ? lv.cand[x] : 0;
                 ok = ok && no_conflict(lv, vx);
                 const uint32_t mask = __ballot_sync(kFull, ok);
@@ -601,142 +600,161 @@ struct Warp {
     }
 };
 
+// Depth-first search from level `base` (already set up) down to the last
+// level; returns false when a stop flag (overflow, time or count limit,
+// internal error) ended it early.
+template <uint32_t MODE, bool MULTI>
+__device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint32_t base, uint32_t &iter,
+                    uint64_t deadline) {
+    volatile unsigned int *flags = reinterpret_cast<volatile unsigned int *>(&a.ctr[kCtrFlags]);
+    const uint32_t n = W.n;
+    uint32_t d = base;
+    while (d >= base) {
+        if ((++iter & 63u) == 0) {
+            uint32_t st = 0, want = 0;
+            W.flush_count();
+            if (lane == 0) {
+                st = *flags & kStopFlags;
+                if (!st && deadline && globaltimer() > deadline) {
+                    atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagTimeout);
+                    st = kFlagTimeout;
+                }
+                volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
+                const unsigned long long idle = vc[kCtrIdle], pend = vc[kCtrTail] - vc[kCtrHead];
+                want = idle > pend && (long long)pend >= 0;
+            }
+            if (__shfl_sync(kFull, st, 0)) return false;
+            if (__shfl_sync(kFull, want, 0)) W.try_donate(base, d);
+        }
+        if (W.pos[d] < W.cnt[d]) {
+            const uint32_t x = W.buf[32 * d + W.pos[d]];
+            __syncwarp();
+            if (lane == 0) {
+                W.pos[d] += 1;
+                W.idx[d] = x;
+                W.vid[d] = W.L[d].cand[x];
+            }
+            __syncwarp();
+            ++d;
+            const uint32_t len = W.setup(d);
+            if (d == n - 1) {
+                if (len) W.leaf(d);
+                --d;
+            } else if (len == 0) {
+                --d;
+            } else if (d + 2 == n && W.lane_leaf_ok()) {
+                W.prepare_lane_leaf(d);
+            }
+            continue;
+        }
+        if (W.dpos[d] < W.dend[d]) {
+            W.fill_chunk(d);
+            continue;
+        }
+        --d;
+    }
+    return true;
+}
+
+// Level `s` set up from the prefix in W.idx[0..s-1], restricted to driver
+// positions [lo, hi); then searched to the end.
+template <uint32_t MODE, bool MULTI>
+__device__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint32_t s, uint32_t lo, uint32_t hi,
+                          uint32_t &iter, uint64_t deadline) {
+    W.setup(s);
+    if (lane == 0) {
+        W.dpos[s] = lo;
+        W.dend[s] = hi;
+    }
+    __syncwarp();
+    if (s == W.n - 1) {
+        if (hi > lo) W.leaf(s);
+        return true;
+    }
+    if (s + 2 == W.n && W.lane_leaf_ok()) W.prepare_lane_leaf(s);
+    return dfs(a, W, lane, s, iter, deadline);
+}
+
 // The warp loop shared by the single-query kernel and the batch kernel.
+// Root tasks are blocks of consecutive (level-0, level-1) candidate pairs of
+// one query (pairs ordered by level-0 candidate, then by position in its
+// level-1 list); a block is decoded with one warp-wide search and run as
+// level-1 ranges.  When roots run out, warps steal donated ranges.
 template <uint32_t MODE, bool MULTI>
 __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane) {
-    volatile unsigned int *flags = reinterpret_cast<volatile unsigned int *>(&a.ctr[kCtrFlags]);
-    const unsigned long long ntasks = MULTI ? a.task_pre[a.nquery] : a.ntasks;
+    const unsigned long long nblocks = MULTI ? a.task_pre[a.nquery] : a.ntasks;
     uint32_t iter = 0;
     bool stop = false, roots_left = true;
     uint64_t deadline = 0;
     if (a.limit_ns && lane == 0) deadline = globaltimer() + a.limit_ns;
     while (!stop) {
-        uint32_t base = 2;
-        bool have = false;
         if (roots_left) {
-            unsigned long long t = 0;
+            unsigned long long b = 0;
             if (lane == 0) {
                 atomicAdd(&a.ctr[kCtrActive], 1ull);
-                t = atomicAdd(&a.ctr[kCtrTask], 1ull);
-                if (t >= ntasks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+                b = atomicAdd(&a.ctr[kCtrTask], 1ull);
+                if (b >= nblocks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
             }
-            t = __shfl_sync(kFull, t, 0);
-            if (t < ntasks) {
-                have = true;
-                const uint32_t *off01 = a.off01, *list01 = a.list01;
-                uint32_t n0 = a.n0;
+            b = __shfl_sync(kFull, b, 0);
+            if (b < nblocks) {
+                unsigned long long K = a.blk, P = a.pairs;
                 if (MULTI) {
-                    const uint32_t qq = warp_find_row64(a.task_pre, a.nquery, t, lane);
+                    const uint32_t qq = warp_find_row64(a.task_pre, a.nquery, b, lane);
                     W.bind(qq);
-                    t -= a.task_pre[qq];
-                    off01 = a.qd[qq].off01;
-                    list01 = a.qd[qq].list01;
-                    n0 = a.qd[qq].n0;
+                    b -= a.task_pre[qq];
+                    K = a.qd[qq].blk;
+                    P = a.qd[qq].pairs;
                 }
-                uint32_t i0, i1 = 0;
+                unsigned long long t = b * K;
+                const unsigned long long t_end = min(t + K, P);
                 if (W.n == 1) {
-                    i0 = (uint32_t)t;
+                    for (; t < t_end; ++t) {
+                        if (lane == 0) {
+                            W.idx[0] = (uint32_t)t;
+                            W.vid[0] = W.L[0].cand[(uint32_t)t];
+                        }
+                        __syncwarp();
+                        W.single(0);
+                    }
                 } else {
-                    i0 = warp_find_row(off01, n0, t, lane);
-                    i1 = list01[t];
-                }
-                if (lane == 0) {
-                    W.idx[0] = i0;
-                    W.vid[0] = W.L[0].cand[i0];
-                    if (W.n > 1) {
-                        W.idx[1] = i1;
-                        W.vid[1] = W.L[1].cand[i1];
+                    // level-1 lists of the level-0 candidates, as CSR offsets
+                    const uint32_t *off01 = W.B[W.L[1].back_first].off;
+                    uint32_t i0 = warp_find_row32(off01, W.L[0].ncand, t, lane);
+                    while (t < t_end && !stop) {
+                        const uint32_t r0 = off01[i0], r1 = off01[i0 + 1];
+                        if (r1 <= t) {
+                            ++i0;
+                            continue;
+                        }
+                        const uint32_t seg_hi = (uint32_t)min((unsigned long long)r1, t_end);
+                        if (lane == 0) {
+                            W.idx[0] = i0;
+                            W.vid[0] = W.L[0].cand[i0];
+                        }
+                        __syncwarp();
+                        stop = !run_range(a, W, lane, 1, (uint32_t)t - r0, seg_hi - r0, iter, deadline);
+                        t = seg_hi;
+                        ++i0;
                     }
                 }
-                __syncwarp();
-            } else {
-                roots_left = false;
-            }
-        }
-        uint32_t d = 2;
-        if (have) {
-            if (W.n <= 2) {
-                W.single(W.n - 1);
                 if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
                 continue;
             }
-            const uint32_t len = W.setup(d);
-            if (d == W.n - 1) {
-                if (len) W.leaf(d);
-                d = 1;
-            } else if (len == 0) {
-                d = 1;
-            } else if (d + 2 == W.n && W.lane_leaf_ok()) {
-                W.prepare_lane_leaf(d);
-            }
-        } else {
-            const unsigned long long qpos = W.take_queued();
-            if (qpos == ~0ull) break;
-            const volatile uint32_t *rec = a.queue + (qpos & (kQueueCap - 1)) * kRecWords;
-            if (MULTI) W.bind(rec[0]);
-            base = rec[1];
-            const uint32_t lo = rec[2], hi = rec[3];
-            if (lane < base) {
-                const uint32_t x = rec[4 + lane];
-                W.idx[lane] = x;
-                W.vid[lane] = W.L[lane].cand[x];
-            }
-            W.release(qpos);
-            __syncwarp();
-            d = base;
-            W.setup(d);
-            if (d + 2 == W.n && W.lane_leaf_ok()) W.prepare_lane_leaf(d);
-            if (lane == 0) {
-                W.dpos[d] = lo;
-                W.dend[d] = hi;
-            }
-            __syncwarp();
+            roots_left = false;
         }
-        const uint32_t n = W.n;
-        while (d >= base) {
-            if ((++iter & 63u) == 0) {
-                uint32_t st = 0, want = 0;
-                W.flush_count();
-                if (lane == 0) {
-                    st = *flags & kStopFlags;
-                    if (!st && deadline && globaltimer() > deadline) {
-                        atomicOr((unsigned int *)&a.ctr[kCtrFlags], kFlagTimeout);
-                        st = kFlagTimeout;
-                    }
-                    volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
-                    const unsigned long long idle = vc[kCtrIdle], pend = vc[kCtrTail] - vc[kCtrHead];
-                    want = idle > pend && (long long)pend >= 0;
-                }
-                if (__shfl_sync(kFull, st, 0)) { stop = true; break; }
-                if (__shfl_sync(kFull, want, 0)) W.try_donate(base, d);
-            }
-            if (W.pos[d] < W.cnt[d]) {
-                const uint32_t x = W.buf[32 * d + W.pos[d]];
-                __syncwarp();
-                if (lane == 0) {
-                    W.pos[d] += 1;
-                    W.idx[d] = x;
-                    W.vid[d] = W.L[d].cand[x];
-                }
-                __syncwarp();
-                ++d;
-                const uint32_t len = W.setup(d);
-                if (d == n - 1) {
-                    if (len) W.leaf(d);
-                    --d;
-                } else if (len == 0) {
-                    --d;
-                } else if (d + 2 == n && W.lane_leaf_ok()) {
-                    W.prepare_lane_leaf(d);
-                }
-                continue;
-            }
-            if (W.dpos[d] < W.dend[d]) {
-                W.fill_chunk(d);
-                continue;
-            }
-            --d;
+        const unsigned long long qpos = W.take_queued();
+        if (qpos == ~0ull) break;
+        const volatile uint32_t *rec = a.queue + (qpos & (kQueueCap - 1)) * kRecWords;
+        if (MULTI) W.bind(rec[0]);
+        const uint32_t s = rec[1], lo = rec[2], hi = rec[3];
+        if (lane < s) {
+            const uint32_t x = rec[4 + lane];
+            W.idx[lane] = x;
+            W.vid[lane] = W.L[lane].cand[x];
         }
+        W.release(qpos);
+        __syncwarp();
+        stop = !run_range(a, W, lane, s, lo, hi, iter, deadline);
         if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
     }
     // flush per-warp totals
@@ -803,6 +821,19 @@ int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
 }
 
 }  // namespace
+
+// Root tasks: blocks of consecutive (level-0, level-1) candidate pairs, about
+// 64K pairs per block count, between 1 and 256 pairs per block.
+void root_blocks(const asdm_cs &cs, const asdm_plan &plan, unsigned long long &pairs, unsigned long long &blk,
+                 unsigned long long &nblocks) {
+    if (cs.q.n == 1) {
+        pairs = cs.ncand[plan.order[0]];
+    } else {
+        pairs = cs.etotal[plan.back[1][0].second];
+    }
+    blk = std::min<unsigned long long>(256, std::max<unsigned long long>(1, pairs / 65536));
+    nblocks = (pairs + blk - 1) / blk;
+}
 
 int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_run_stats &st) {
     asdm_graph *G = cs.g;
@@ -888,15 +919,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         a.nb = nb;
         a.nc = nc;
         a.nq = n;
-        if (n == 1) {
-            a.ntasks = cs.ncand[plan.order[0]];
-        } else {
-            const uint32_t e01 = plan.back[1][0].second;
-            a.off01 = cs.d_eoff + cs.eoff_base[e01];
-            a.list01 = cs.d_elist + cs.elist_base[e01];
-            a.n0 = cs.ncand[plan.order[0]];
-            a.ntasks = cs.etotal[e01];
-        }
+        root_blocks(cs, plan, a.pairs, a.blk, a.ntasks);
         a.ctr = d_ctr;
         a.local = d_local;
         a.rows = d_rows;
@@ -1039,16 +1062,8 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         qd[li].n = n;
         qd[li].nb = (uint32_t)bk.size();
         qd[li].nc = (uint32_t)cf.size();
-        unsigned long long nt;
-        if (n == 1) {
-            nt = c.ncand[plan.order[0]];
-        } else {
-            const uint32_t e01 = plan.back[1][0].second;
-            qd[li].off01 = c.d_eoff + c.eoff_base[e01];
-            qd[li].list01 = c.d_elist + c.elist_base[e01];
-            qd[li].n0 = c.ncand[plan.order[0]];
-            nt = c.etotal[e01];
-        }
+        unsigned long long nt = 0;
+        root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt);
         task_pre[li + 1] = task_pre[li] + nt;
         maxn = std::max(maxn, n);
         maxnb = std::max(maxnb, (uint32_t)bk.size());
@@ -1329,15 +1344,7 @@ extern "C" int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, d
     a.nb = nb;
     a.nc = nc;
     a.nq = n;
-    if (n == 1) {
-        a.ntasks = cs->ncand[plan->order[0]];
-    } else {
-        const uint32_t e01 = plan->back[1][0].second;
-        a.off01 = cs->d_eoff + cs->eoff_base[e01];
-        a.list01 = cs->d_elist + cs->elist_base[e01];
-        a.n0 = cs->ncand[plan->order[0]];
-        a.ntasks = cs->etotal[e01];
-    }
+    root_blocks(*cs, *plan, a.pairs, a.blk, a.ntasks);
     a.ctr = d_ctr;
     a.queue = d_ring;
     a.qseq = d_seq;
