@@ -9,8 +9,12 @@ config-2 mixed batch of random-walk queries with sizes uniform in 4..32,
 screened to the queries whose exact count is at most 10^9 (the screen and its
 exact counts are in asdmatch_b200/c2_screened.json).  One step = every query
 of the batch through candidate-space construction, planning and exact
-counting, one query per launch sequence (the plain GPU form).  Each step's
-counts are checked against the screened counts.
+counting.  ``value`` is the batched form (asdm_run_batch: one launch per CFL
+phase for the whole batch, one persistent enumeration kernel over every
+(query, root block)), with the kernel knobs picked by the autotuner before
+timing; the plain form (one query per launch sequence) is timed too and
+reported in ``config.plain_form``.  Every step's counts are checked against
+the screened counts.
 
 Multi-GPU: the path shards by query; every rank runs the whole batch on its
 own GPU with no collective on the data path ("scaling": "weak"); the value is
