@@ -102,6 +102,9 @@ class Tuning(C.Structure):
 
 _set_tuning = _sig("asdm_graph_set_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
 _get_tuning = _sig("asdm_graph_get_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
+_run_batch_local = _sig("asdm_run_batch_local", C.c_int,
+                        [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, C.c_double, _u64p,
+                         C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(RunStats)])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -459,6 +462,20 @@ def run_batch_packed(dg: DeviceGraph, b: BatchInput, time_limit_s: float = 0.0) 
     if rc == ERR_CUDA:
         _check(rc, "batch")
     return st
+
+
+def run_batch_local(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):
+    """Batched LOCAL_COUNT: returns (counts, status, [|Vg| x |Vq_i| uint64 matrices])."""
+    b = BatchInput(queries)
+    mats = [np.zeros((dg.n, q.n), np.uint64) for q in queries]
+    ptrs = (_u64p * max(1, len(mats)))(*[_ptr(m, _u64p) for m in mats])
+    st = RunStats()
+    rc = _run_batch_local(dg._h, b.nq, _ptr(b.sizes), _ptr(b.ob, _u64p), _ptr(b.offs), _ptr(b.nb, _u64p), _ptr(b.nbrs),
+                          _ptr(b.lb, _u64p), _ptr(b.labs), time_limit_s, _ptr(b.counts, _u64p),
+                          b.status.ctypes.data_as(C.POINTER(C.c_int)), ptrs, C.byref(st))
+    if rc == ERR_CUDA:
+        _check(rc, "batch")
+    return b.counts.copy(), b.status.copy(), mats
 
 
 def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):

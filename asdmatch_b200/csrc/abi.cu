@@ -175,17 +175,18 @@ extern "C" int asdm_intersect_batch(const uint32_t *values, const uint64_t *list
 namespace asdm {
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
-                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg);
+                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg,
+                    uint64_t *const *local_out);
 }  // namespace asdm
 
 // Candidate-space state a group may hold at once (state words, storage and
 // candidate arrays: 12 bytes per data vertex of each query vertex's label).
 static constexpr uint64_t kGroupStateBytes = 16ull << 30;
 
-extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
-                              const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
-                              const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
-                              uint64_t *counts, int *status, asdm_run_stats *stats) {
+static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                          const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                          const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
+                          uint64_t *counts, int *status, asdm_run_stats *stats, uint64_t *const *local_out) {
     clear_error();
     if (stats) *stats = asdm_run_stats{};
     if (!g || (nq && (!q_sizes || !q_off_base || !q_offsets || !q_nbr_base || !q_nbrs || !q_lab_base || !q_labels ||
@@ -207,6 +208,10 @@ extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_size
         for (uint32_t u = 0; u < c->q.n; ++u) {
             const uint32_t l = c->q.lab[u];
             if (l < g->d.nlabels) state[i] += 12ull * (g->h_vbl_off[l + 1] - g->h_vbl_off[l]);
+        }
+        if (local_out) {
+            state[i] += 8ull * g->d.n * c->q.n;  // the query's local-count block
+            if (local_out[i]) std::fill(local_out[i], local_out[i] + (uint64_t)g->d.n * c->q.n, 0ull);
         }
         all[i] = std::move(c);
     }
@@ -252,8 +257,12 @@ extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_size
         }
         std::vector<uint64_t> c(run_ids.size());
         std::vector<int> st(run_ids.size());
+        std::vector<uint64_t *> lo;
+        if (local_out)
+            for (uint32_t id : run_ids) lo.push_back(local_out[id]);
         asdm_run_stats gs{};
-        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, c.data(), st.data(), &gs);
+        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, c.data(), st.data(), &gs,
+                             local_out ? lo.data() : nullptr);
         if (stats) {
             stats->count += gs.count;
             stats->intersections += gs.intersections;
@@ -275,4 +284,22 @@ extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_size
         if (rc == ASDM_ERR_CUDA) break;
     }
     return worst;
+}
+
+extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                              const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                              const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
+                              uint64_t *counts, int *status, asdm_run_stats *stats) {
+    return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
+                          time_limit_s, counts, status, stats, nullptr);
+}
+
+extern "C" int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                                    const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                                    const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
+                                    uint64_t *counts, int *status, uint64_t *const *local_counts,
+                                    asdm_run_stats *stats) {
+    if (nq && !local_counts) return fail(ASDM_ERR_INVALID, "null local-count array");
+    return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
+                          time_limit_s, counts, status, stats, local_counts);
 }

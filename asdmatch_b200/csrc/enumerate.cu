@@ -101,6 +101,7 @@ struct QDesc {
     const DLevel *lv;
     const DBack *bk;
     const uint32_t *conf;
+    unsigned long long *local;  // |Vg| x n (MODE_LOCAL batches)
     unsigned long long pairs, blk;
     uint32_t n, nb, nc, pad;
 };
@@ -168,6 +169,7 @@ struct Warp {
     uint32_t lane;
     uint32_t n;            // levels of the current query
     uint32_t q = 0;        // current query (batches)
+    unsigned long long *local;  // |Vg| x n local counts of the current query (MODE_LOCAL)
     unsigned long long count = 0, inter = 0, elems = 0;
     bool overflow = false;
 
@@ -175,7 +177,7 @@ struct Warp {
     // levels and maxnb backward edges.
     __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln,
                     uint32_t levels, uint32_t maxn, uint32_t maxnb)
-        : a(args), L(l), B(b), CF(cf), lane(ln), n(levels) {
+        : a(args), L(l), B(b), CF(cf), lane(ln), n(levels), local(args.local) {
         idx = w;
         vid = idx + maxn;
         buf = vid + maxn;
@@ -200,6 +202,7 @@ struct Warp {
         B = d.bk;
         CF = d.conf;
         n = d.n;
+        local = d.local;
     }
 
     __device__ __forceinline__ bool lane_leaf_ok() const {
@@ -578,11 +581,11 @@ struct Warp {
                 ok = ok && no_conflict(lv, vx);
                 const uint32_t mask = __ballot_sync(kFull, ok);
                 total += __popc(mask);
-                if ((MODE & ASDM_MODE_LOCAL) && ok) atomicAdd(&a.local[(unsigned long long)vx * n + lv.u], 1ull);
+                if ((MODE & ASDM_MODE_LOCAL) && ok) atomicAdd(&local[(unsigned long long)vx * n + lv.u], 1ull);
                 if (MODE & ASDM_MODE_EMBED) emit_rows(d, vx, ok, mask);
             }
             if ((MODE & ASDM_MODE_LOCAL) && total && lane < d)
-                atomicAdd(&a.local[(unsigned long long)vid[lane] * n + L[lane].u], total);
+                atomicAdd(&local[(unsigned long long)vid[lane] * n + L[lane].u], total);
         }
         add_count(total);
     }
@@ -591,7 +594,7 @@ struct Warp {
     __device__ void single(uint32_t d) {
         add_count(1);
         if (MODE & ASDM_MODE_LOCAL) {
-            if (lane <= d) atomicAdd(&a.local[(unsigned long long)vid[lane] * n + L[lane].u], 1ull);
+            if (lane <= d) atomicAdd(&local[(unsigned long long)vid[lane] * n + L[lane].u], 1ull);
         }
         if (MODE & ASDM_MODE_EMBED) {
             const uint32_t vx = vid[d];
@@ -790,14 +793,15 @@ __global__ void __launch_bounds__(kThreads) enum_kernel(EnumArgs a) {
 // Many queries in one persistent launch (COUNT mode): root tasks of every
 // query form one range claimed by atomicAdd, plans are read from global
 // memory, counts go to per-query totals.
-template <int MINB>
+template <int MINB, uint32_t MODE = ASDM_MODE_COUNT>
 __global__ void __launch_bounds__(kThreads, MINB) enum_batch_kernel(EnumArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t *wmem = sm + warp * warp_words(a.maxn, a.maxnb);
     const QDesc d0 = a.qd[0];
-    Warp<ASDM_MODE_COUNT, true> W(a, d0.lv, d0.bk, d0.conf, wmem, lane, d0.n, a.maxn, a.maxnb);
-    warp_loop<ASDM_MODE_COUNT, true>(a, W, lane);
+    Warp<MODE, true> W(a, d0.lv, d0.bk, d0.conf, wmem, lane, d0.n, a.maxn, a.maxnb);
+    W.local = d0.local;
+    warp_loop<MODE, true>(a, W, lane);
 }
 
 __global__ void queue_init(unsigned long long *seq) {
@@ -1011,7 +1015,8 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
 // Batched form: one persistent launch counts every query of a group.
 // counts[i] / status[i] receive each query's result.
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
-                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg) {
+                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg,
+                    uint64_t *const *local_out) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
     std::vector<uint32_t> live;  // queries with a non-empty candidate space
@@ -1071,12 +1076,24 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     const uint64_t qd_at = append(nullptr, L * sizeof(QDesc));
     const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
     uint8_t *d_buf = nullptr;
-    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr;
     uint32_t *d_queue = nullptr;
     unsigned int *d_qflags = nullptr;
     int rc = ASDM_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // local counts (LOCAL mode): one |Vg| x n block per live query
+    const bool local_mode = local_out != nullptr;
+    std::vector<uint64_t> local_base(L + 1, 0);
+    for (uint32_t li = 0; li < L; ++li)
+        local_base[li + 1] = local_base[li] + (local_mode ? (uint64_t)G->d.n * cs[live[li]]->q.n : 0);
     do {
+        if (local_mode) {
+            if ((rc = dalloc(&d_local, local_base[L], s))) break;
+            if (cudaMemsetAsync(d_local, 0, local_base[L] * sizeof(unsigned long long), s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "local-count reset failed");
+                break;
+            }
+        }
         if ((rc = dalloc(&d_buf, hp.size(), s)) || (rc = dalloc(&d_ctr, kCtrN, s)) || (rc = dalloc(&d_qcounts, L, s)) ||
             (rc = dalloc(&d_qflags, L, s)) || (rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s)))
             break;
@@ -1084,6 +1101,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             qd[li].lv = reinterpret_cast<const DLevel *>(d_buf + offs[li].lv);
             qd[li].bk = reinterpret_cast<const DBack *>(d_buf + offs[li].bk);
             qd[li].conf = reinterpret_cast<const uint32_t *>(d_buf + offs[li].cf);
+            qd[li].local = local_mode ? d_local + local_base[li] : nullptr;
         }
         std::memcpy(hp.data() + qd_at, qd.data(), L * sizeof(QDesc));
         if (cudaMemcpyAsync(d_buf, hp.data(), hp.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -1122,6 +1140,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
                 case 6: k = enum_batch_kernel<6>; break;
                 default: break;
             }
+            if (local_mode) k = enum_batch_kernel<1, ASDM_MODE_LOCAL>;
             if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
                 rc = fail(ASDM_ERR_CUDA, "shared-memory opt-in failed");
                 break;
@@ -1173,6 +1192,15 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         }
         if (gflags & kFlagInternal) rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
         else if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
+        if (rc == ASDM_OK && local_mode) {
+            for (uint32_t li = 0; li < L && rc == ASDM_OK; ++li)
+                if (local_out[live[li]] &&
+                    cudaMemcpyAsync(local_out[live[li]], d_local + local_base[li],
+                                    (local_base[li + 1] - local_base[li]) * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, s) != cudaSuccess)
+                    rc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+            if (rc == ASDM_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+        }
     } while (false);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1181,6 +1209,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     dfree(d_qcounts, s);
     dfree(d_qflags, s);
     dfree(d_queue, s);
+    dfree(d_local, s);
     cudaStreamSynchronize(s);
     return rc;
 }

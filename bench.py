@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=1, help="queries in the CPU-baseline sample")
     ap.add_argument("--queries", type=int, default=0, help="use only the first K queries (profiling runs)")
     ap.add_argument("--profile", action="store_true", help="timed steps only: no e2e pass, no CPU baseline")
+    ap.add_argument("--no-c4", action="store_true", help="skip the config-4 local-counting measurement")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default kernel knobs (profiling runs)")
     return ap.parse_args()
 
 
@@ -109,6 +111,17 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(x, world, device):
+    """The slowest rank's value (every rank calls this at the same point)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def flush_l2(torch, dev):
     # a 256 MB write evicts the 126 MB L2 between timed steps
     buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
@@ -140,6 +153,42 @@ def cpu_baseline(dpath, qpaths, want_counts, timeout_s=120):
     return {"value": (done / dt) if done else 0.0, "unit": "queries/s", "cores": 1, "kind": kind,
             "sample": "%d of the batch's queries, one single-threaded process per query (graph load, CFL filter, "
                       "FHD planning, ALL_LEVEL join), %.1f s wall, counts %s" % (done, dt, "match" if ok else "DIFFER")}
+
+
+def measure_c4(A, W, torch, dev, steps):
+    """Config 4: the screened 8-vertex queries on the 1M/10M graph, batched LOCAL_COUNT
+    (asdm_run_batch_local); checked every step (counts, and every local-count column sums
+    to the count)."""
+    import numpy as np
+    g = W.graph(W.C4)
+    sc = W.load_c4_screen()
+    qs = W.c4_queries(g, sc)
+    want = [r["count"] for r in sc["queries"]]
+    dg = A.DeviceGraph(g)
+    stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
+    A.run_batch_local(dg, qs)  # warm
+    times = []
+    for _ in range(steps):
+        flush_l2(torch, dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        counts, status, mats = A.run_batch_local(dg, qs)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        if counts.tolist() != want or status.any():
+            raise SystemExit("config-4 counts differ from the screened counts")
+        for c, m in zip(want, mats):
+            if any(int(x) != c for x in m.sum(axis=0, dtype=np.uint64)):
+                raise SystemExit("config-4 local counts do not sum to the count")
+    ms = statistics.mean(times)
+    dg.close()
+    return {"workload": "c4-screened: Chung-Lu N=1.0M M=10M gamma=2.3, 32 labels Zipf(1.0); %d random-walk queries "
+                        "of %d vertices with <= 1e9 matches (%d of %d candidates; no 10-vertex query qualified)"
+                        % (len(qs), sc["size"], len(qs), sc["candidates"]),
+            "queries_per_s": len(qs) / (ms / 1e3), "ms_per_step": ms, "matches_per_step": int(sum(want)),
+            "local_count_bytes_per_step": 8 * g.n * sum(q.n for q in qs),
+            "via": "asdm_run_batch_local, |Vg| x |Vq| uint64 matrices copied to host every step"}
 
 
 def setup_workload(name):
@@ -266,7 +315,10 @@ def main():
         return stats
 
     packed = A.BatchInput(qs)
-    tune_best, tune_table = A.autotune(dg, packed)  # untimed: picks the kernel knobs on this batch
+    if args.no_tune:
+        tune_best, tune_table = dg.tuning(), []
+    else:
+        tune_best, tune_table = A.autotune(dg, packed)  # untimed: picks the kernel knobs on this batch
 
     def batched_step():
         """The batched form: the whole batch through asdm_run_batch."""
@@ -291,12 +343,7 @@ def main():
             torch.cuda.synchronize(dev)
             times.append(e0.elapsed_time(e1))
             agg = st if agg is None else {k: agg[k] + st[k] for k in agg}
-        ms_ = statistics.mean(times)
-        if world > 1:
-            t = torch.tensor([ms_], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_ = float(t.item())
-        return ms_, agg
+        return max_over_ranks(statistics.mean(times), world, dev), agg
 
     for _ in range(args.warmup):
         batched_step()
@@ -325,11 +372,7 @@ def main():
         e2e_times.append(time.perf_counter() - t0)
         if packed.counts.tolist() != counts or packed.status.any():
             raise SystemExit("batch counts differ from the screened counts")
-    e2e_s = statistics.mean(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), world, dev)
     if rank != 0:
         if world > 1:
             dist.barrier()
@@ -383,6 +426,9 @@ def main():
         "gpu_launches": launches // steps,
         "clocks": clocks,
     }
+    # config 4: batched local subgraph counting (LOCAL_COUNT), secondary measurement
+    if world == 1 and not args.no_c4 and os.path.exists(W.C4_SCREEN_FILE):
+        line["config"]["local_counting_c4"] = measure_c4(A, W, torch, dev, args.steps)
     if world == 1:
         tmp = tempfile.mkdtemp(prefix="asdm_cpu_")
         dpath = os.path.join(tmp, "data.graph")

@@ -226,6 +226,16 @@ int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const ui
                    const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
                    const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
                    uint64_t *counts, int *status, asdm_run_stats *stats);
+/* The same, also producing each query's |Vg| x |Vq_i| local-count matrix
+ * (the reference's LOCAL_COUNT output, matching/join.cpp:1035-1041, one
+ * process per query there) into local_counts[i] (row-major, may be NULL to
+ * skip a query's matrix); the matrices of a group live on the device until
+ * the group finishes. */
+int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                         const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                         const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
+                         uint64_t *counts, int *status, uint64_t *const *local_counts,
+                         asdm_run_stats *stats);
 
 #ifdef __cplusplus
 }

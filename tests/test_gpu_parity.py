@@ -238,3 +238,34 @@ def test_every_tuning_gives_the_same_counts(golden, c0d_files, dg_c0d):
     best, table = A.autotune(dg_c0d, b, reps=1, lane_leaf=(96,))
     assert len(table) == 4 and best in table
     dg_c0d.set_tuning(1, 96)
+
+
+def test_batched_local_counts_match_golden_csv(golden, c0_files, c0d_files, dg_c0, dg_c0d, edge_files):
+    _, _, qs, _ = c0_files
+    recs = [r for r in golden["sets"]["c0"] if "csv_sha" in r]
+    counts, status, mats = A.run_batch_local(dg_c0, [qs[r["index"]] for r in recs])
+    assert status.tolist() == [0] * len(recs)
+    for r, c, m in zip(recs, counts.tolist(), mats):
+        assert c == r["count"]
+        assert csv_sha(m) == r["csv_sha"], r["index"]
+    _, _, by_size = c0d_files
+    recs = [r for r in golden["sets"]["c0d"] if "csv_sha" in r]
+    counts, status, mats = A.run_batch_local(dg_c0d, [by_size[r["size"]][0][r["index"]] for r in recs])
+    for r, c, m in zip(recs, counts.tolist(), mats):
+        assert c == r["count"] and csv_sha(m) == r["csv_sha"], r
+    recs = [r for r in golden["sets"]["edge"] if "csv_sha" in r]
+    counts, status, mats = A.run_batch_local(dg_c0, [edge_files[r["name"]][0] for r in recs])
+    for r, c, m in zip(recs, counts.tolist(), mats):
+        assert c == r["count"] and csv_sha(m) == r["csv_sha"], r["name"]
+
+
+def test_batched_local_counts_agree_with_single_query_mode(golden, c0d_files, dg_c0d):
+    _, _, by_size = c0d_files
+    recs = sorted(golden["sets"]["c0d"], key=lambda r: -r["count"])[:6]   # heaviest, beyond the golden CSVs
+    qs = [by_size[r["size"]][0][r["index"]] for r in recs]
+    counts, status, mats = A.run_batch_local(dg_c0d, qs)
+    for r, q, c, m in zip(recs, qs, counts.tolist(), mats):
+        single = A.match(dg_c0d, q, mode=A.MODE_LOCAL)
+        assert c == r["count"] == single.count
+        assert np.array_equal(m, single.local_counts)
+        assert all(int(x) == r["count"] for x in m.sum(axis=0, dtype=np.uint64))
