@@ -105,6 +105,14 @@ _get_tuning = _sig("asdm_graph_get_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
 _run_batch_local = _sig("asdm_run_batch_local", C.c_int,
                         [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, C.c_double, _u64p,
                          C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(RunStats)])
+_card_load = _sig("asdm_card_load", C.c_int, [C.c_char_p, C.POINTER(_vp)])
+_card_create = _sig("asdm_card_create", C.c_int, [C.POINTER(_vp)])
+_card_set = _sig("asdm_card_set", C.c_int, [_vp, C.c_uint64, C.c_double])
+_card_lookup = _sig("asdm_card_lookup", C.c_int, [_vp, C.c_uint64, C.POINTER(C.c_double)])
+_card_info = _sig("asdm_card_info", C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_double)])
+_card_write = _sig("asdm_card_write", C.c_int, [_vp, C.c_char_p, C.c_double])
+_card_free = _sig("asdm_card_free", None, [_vp])
+_plan_create_card = _sig("asdm_plan_create_card", C.c_int, [_vp, _vp, C.POINTER(_vp)])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -314,13 +322,52 @@ class CandidateSpace:
             pass
 
 
+class Card:
+    """The .card plan cache: subset bitmask (bit u = query vertex u) -> cardinality."""
+
+    def __init__(self, path: Optional[str] = None):
+        h = _vp()
+        if path is None:
+            _check(_card_create(C.byref(h)))
+        else:
+            _check(_card_load(path.encode(), C.byref(h)), path)
+        self._h = h
+
+    def info(self):
+        b, e, t = C.c_uint32(), C.c_uint64(), C.c_double()
+        _check(_card_info(self._h, C.byref(b), C.byref(e), C.byref(t)))
+        return {"bags": b.value, "entries": e.value, "plan_seconds": t.value}
+
+    def __setitem__(self, subset: int, card: float):
+        _check(_card_set(self._h, subset, card))
+
+    def __getitem__(self, subset: int) -> float:
+        v = C.c_double()
+        _check(_card_lookup(self._h, subset, C.byref(v)))
+        return v.value
+
+    def write(self, path: str, plan_seconds: float = 0.0):
+        _check(_card_write(self._h, path.encode(), plan_seconds), path)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _card_free(h)
+            self._h = None
+
+
 class Plan:
-    def __init__(self, cs: CandidateSpace, order: Optional[Sequence[int]] = None):
+    def __init__(self, cs: CandidateSpace, order: Optional[Sequence[int]] = None, card: Optional[Card] = None):
         h = _vp()
         o = None
         if order is not None:
             arr = np.ascontiguousarray(order, dtype=np.uint32)
             o = _ptr(arr)
+        if card is not None:
+            _check(_plan_create_card(cs._h, card._h, C.byref(h)), "plan")
+            self._h = h
+            self.n = cs.q.n
+            return
         _check(_plan_create(cs._h, o, C.byref(h)), "plan")
         self._h = h
         self.n = cs.q.n

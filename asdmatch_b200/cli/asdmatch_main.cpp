@@ -81,13 +81,18 @@ int main(int argc, char **argv) {
     if (!nonempty) return 0;  // buildCandCFL() == false: the reference returns silently
     out << "Filtering time (s): " << since(t0) << std::endl;
     out << "FHD time (s): " << 0.0 << std::endl;
+    asdm_card *cache = nullptr;
     if (!card.empty()) {
-        std::ifstream probe(card, std::ios::binary);
-        if (probe.good()) out << "dp time: " << 0.0 << std::endl;
+        // -s: the plan cache replaces cardinality estimation (main.cpp:88-99)
+        if ((rc = asdm_card_load(card.c_str(), &cache))) die("card", rc);
+        double secs = 0;
+        asdm_card_info(cache, nullptr, nullptr, &secs);
+        out << "dp time: " << secs << std::endl;
     }
     t0 = std::chrono::steady_clock::now();
     asdm_plan *plan = nullptr;
-    if ((rc = asdm_plan_create(cs, nullptr, &plan))) die("plan", rc);
+    if ((rc = cache ? asdm_plan_create_card(cs, cache, &plan) : asdm_plan_create(cs, nullptr, &plan))) die("plan", rc);
+    asdm_card_free(cache);
     out << "Planning Time: " << since(t0) << std::endl;
     out << "cost: " << 0 << std::endl;
 

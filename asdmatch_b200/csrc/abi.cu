@@ -173,7 +173,7 @@ extern "C" int asdm_intersect_batch(const uint32_t *values, const uint64_t *list
 }
 
 namespace asdm {
-int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p);
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg,
                     uint64_t *const *local_out);

@@ -32,7 +32,7 @@
 
 namespace asdm {
 
-int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p);
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
 
 namespace {
 

@@ -17,6 +17,8 @@
 
 #include "cs.cuh"
 
+double card_lookup_or(const asdm_card *c, uint64_t subset, double fallback);
+
 namespace asdm {
 
 namespace {
@@ -27,13 +29,17 @@ double avg_len(const asdm_cs &cs, uint32_t from, uint32_t to) {
     return cs.ncand[from] ? (double)cs.etotal[e] / (double)cs.ncand[from] : 0.0;
 }
 
-void greedy_from(const asdm_cs &cs, uint32_t start, std::vector<uint32_t> &order, double &cost) {
+// With a cardinality cache (`.card`), a prefix whose vertex set is in the
+// cache uses the cached cardinality instead of the model's estimate.
+void greedy_from(const asdm_cs &cs, const asdm_card *card, uint32_t start, std::vector<uint32_t> &order,
+                 double &cost) {
     const QueryGraph &q = cs.q;
     const uint32_t n = q.n;
     std::vector<char> in(n, 0);
     order.assign(1, start);
     in[start] = 1;
-    double N = (double)cs.ncand[start];
+    uint64_t mask = 1ull << start;
+    double N = card_lookup_or(card, mask, (double)cs.ncand[start]);
     cost = 0.0;
     for (uint32_t k = 1; k < n; ++k) {
         int best = -1;
@@ -57,7 +63,7 @@ void greedy_from(const asdm_cs &cs, uint32_t start, std::vector<uint32_t> &order
                 if (!skipped && a == drv) { skipped = true; continue; }
                 factor *= std::min(1.0, a / std::max(1.0, (double)cs.ncand[u]));
             }
-            const double Nu = N * factor;
+            const double Nu = card_lookup_or(card, mask | (1ull << u), N * factor);
             const double work = N * (1.0 + lens.size() * std::ceil(std::max(drv, 1.0) / 32.0));
             const uint32_t B = (uint32_t)lens.size();
             if (best < 0 || Nu < bestN || (Nu == bestN && B > bestB)) {
@@ -70,6 +76,7 @@ void greedy_from(const asdm_cs &cs, uint32_t start, std::vector<uint32_t> &order
         if (best < 0) { cost = INFINITY; return; }  // disconnected
         order.push_back((uint32_t)best);
         in[best] = 1;
+        mask |= 1ull << best;
         cost += bestWork + (k + 1 < n ? bestN : 0.0);
         N = std::max(bestN, 1e-9);
     }
@@ -77,7 +84,7 @@ void greedy_from(const asdm_cs &cs, uint32_t start, std::vector<uint32_t> &order
 
 }  // namespace
 
-int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p) {
+int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card) {
     const QueryGraph &q = cs.q;
     const uint32_t n = q.n;
     if (!cs.nonempty) return fail(ASDM_ERR_INVALID, "cannot plan over an empty candidate space");
@@ -94,7 +101,7 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p) {
         for (uint32_t s = 0; s < n; ++s) {
             std::vector<uint32_t> o;
             double c;
-            greedy_from(cs, s, o, c);
+            greedy_from(cs, card, s, o, c);
             if (o.size() == n && c < best) {
                 best = c;
                 p.order = o;
@@ -128,7 +135,16 @@ extern "C" int asdm_plan_create(const asdm_cs *cs, const uint32_t *order, asdm_p
     clear_error();
     if (!cs || !out) return fail(ASDM_ERR_INVALID, "null argument");
     auto p = std::make_unique<asdm_plan>();
-    ASDM_TRY(build_plan(*cs, order, *p));
+    ASDM_TRY(build_plan(*cs, order, *p, nullptr));
+    *out = p.release();
+    return ASDM_OK;
+}
+
+extern "C" int asdm_plan_create_card(const asdm_cs *cs, const asdm_card *card, asdm_plan **out) {
+    clear_error();
+    if (!cs || !out) return fail(ASDM_ERR_INVALID, "null argument");
+    auto p = std::make_unique<asdm_plan>();
+    ASDM_TRY(build_plan(*cs, nullptr, *p, card));
     *out = p.release();
     return ASDM_OK;
 }

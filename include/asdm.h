@@ -41,6 +41,7 @@ typedef struct asdm_host_graph asdm_host_graph; /* host CSR, reference layout  *
 typedef struct asdm_graph asdm_graph;           /* device-resident data graph  */
 typedef struct asdm_cs asdm_cs;                 /* device candidate space      */
 typedef struct asdm_plan asdm_plan;             /* matching order + level info */
+typedef struct asdm_card asdm_card;             /* .card cardinality cache     */
 
 /* Returns a static, thread-local description of the last failure. */
 const char *asdm_last_error(void);
@@ -159,6 +160,27 @@ int asdm_intersect_batch(const uint32_t *values, const uint64_t *list_off, uint6
  * connected permutation of the query vertices. */
 int asdm_plan_create(const asdm_cs *cs, const uint32_t *order, asdm_plan **out);
 int asdm_plan_order(const asdm_plan *p, uint32_t *order);
+/* Planner guided by a cardinality cache: prefixes whose vertex set is in the
+ * cache use the cached cardinality (ASDMatch.out -s; the reference loads the
+ * same map with loadSubsetToCard, plan/estimator.cpp:994-1008). */
+int asdm_plan_create_card(const asdm_cs *cs, const asdm_card *card, asdm_plan **out);
+
+/* ---- .card plan cache ---------------------------------------------------- */
+
+/* Reads a .card file: the reference's (prepare.out, executable/prepare.cpp:12-73:
+ * per-bag SubsetStructure records, plan/subset_structure.cpp:455-560, then the
+ * subset-cardinality map, plan/estimator.cpp:981-992, then the planning time)
+ * or one written by asdm_card_write (no bag records). */
+int asdm_card_load(const char *path, asdm_card **out);
+int asdm_card_create(asdm_card **out);
+/* subset = bitmask of query vertices (bit u = vertex u), as the reference keys it. */
+int asdm_card_set(asdm_card *c, uint64_t subset, double card);
+int asdm_card_lookup(const asdm_card *c, uint64_t subset, double *card);
+int asdm_card_info(const asdm_card *c, uint32_t *bags, uint64_t *entries, double *plan_seconds);
+/* Writes the map (values truncated to two decimals like saveSubsetToCard) and
+ * the planning time, with no bag records. */
+int asdm_card_write(const asdm_card *c, const char *path, double plan_seconds);
+void asdm_card_free(asdm_card *c);
 int asdm_plan_free(asdm_plan *p);
 
 /* ---- enumeration and counting (K5-K8) ----------------------------------- */
