@@ -113,6 +113,8 @@ _card_info = _sig("asdm_card_info", C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_d
 _card_write = _sig("asdm_card_write", C.c_int, [_vp, C.c_char_p, C.c_double])
 _card_free = _sig("asdm_card_free", None, [_vp])
 _plan_create_card = _sig("asdm_plan_create_card", C.c_int, [_vp, _vp, C.POINTER(_vp)])
+_gemm = _sig("asdm_gemm_bf16", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
+                                         C.POINTER(C.c_float)])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -132,6 +134,28 @@ def _ptr(a: np.ndarray, ty=_u32p):
 
 def version() -> str:
     return _version().decode()
+
+
+def to_bf16_bits(x: np.ndarray) -> np.ndarray:
+    """Round-to-nearest-even float32 -> bfloat16 bit patterns (uint16)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    r = ((u >> 16) & 1) + 0x7FFF
+    return ((u + r) >> 16).astype(np.uint16)
+
+
+def from_bf16_bits(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, np.uint32) << 16).view(np.float32)
+
+
+def gemm_bf16(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """C = A @ B^T on the tcgen05 tensor cores (A: M x K, B: N x K, bf16 inputs, fp32 out)."""
+    M, K = a.shape
+    N = b.shape[0]
+    ab, bb = to_bf16_bits(a), to_bf16_bits(b)
+    c = np.zeros((M, N), np.float32)
+    _check(_gemm(M, N, K, ab.ctypes.data_as(C.POINTER(C.c_uint16)), bb.ctypes.data_as(C.POINTER(C.c_uint16)),
+                 c.ctypes.data_as(C.POINTER(C.c_float))), "gemm")
+    return c
 
 
 def kernel_launches() -> int:

@@ -259,6 +259,14 @@ int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, co
                          uint64_t *counts, int *status, uint64_t *const *local_counts,
                          asdm_run_stats *stats);
 
+/* ---- learned cardinality estimator ------------------------------------- */
+
+/* The estimator's tensor-core GEMM on its own, for testing: C[M][N] =
+ * sum_k A[m][k] * B[n][k] with A, B given as bf16 bit patterns (host arrays)
+ * and C in fp32.  No reference counterpart (the reference estimates by
+ * sampling, plan/estimator.cpp:173-291). */
+int asdm_gemm_bf16(int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C);
+
 #ifdef __cplusplus
 }
 #endif
