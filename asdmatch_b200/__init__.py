@@ -115,6 +115,34 @@ _card_free = _sig("asdm_card_free", None, [_vp])
 _plan_create_card = _sig("asdm_plan_create_card", C.c_int, [_vp, _vp, C.POINTER(_vp)])
 _gemm = _sig("asdm_gemm_bf16", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
                                          C.POINTER(C.c_float)])
+class BatchOpts(C.Structure):
+    _fields_ = [("time_limit_s", C.c_double), ("count_limit", C.c_uint64), ("cards", C.POINTER(_vp)),
+                ("estimator", _vp), ("learned_max_subset", C.c_uint32)]
+
+
+_run_batch_ex = _sig("asdm_run_batch_ex", C.c_int,
+                     [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, C.POINTER(BatchOpts), _u64p,
+                      C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(RunStats)])
+_cs_edge_totals = _sig("asdm_cs_edge_totals", C.c_int, [_vp, _u64p])
+_est_create = _sig("asdm_est_create", C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(_vp)])
+_est_train = _sig("asdm_est_train_step", C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_float), _u32p, _u32p, _u32p,
+                                                   C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)])
+_est_predict = _sig("asdm_est_predict", C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_float), _u32p, _u32p, _u32p,
+                                                  C.POINTER(C.c_float)])
+_est_params = _sig("asdm_est_params", C.c_int, [_vp, C.POINTER(C.c_float), C.c_uint64, _u64p])
+_est_set_params = _sig("asdm_est_set_params", C.c_int, [_vp, C.POINTER(C.c_float), C.c_uint64])
+_est_free = _sig("asdm_est_free", None, [_vp])
+_prefix_counts = _sig("asdm_prefix_counts", C.c_int, [_vp, C.c_uint32, _u32p, _u32p, C.c_double, C.c_uint64, _u64p,
+                                                      C.POINTER(C.c_int)])
+_cs_batch = _sig("asdm_candidate_space_batch", C.c_int, [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p,
+                                                         _u32p, C.POINTER(_vp), C.POINTER(C.c_int), C.POINTER(C.c_int)])
+_run_planned = _sig("asdm_run_planned", C.c_int, [C.c_uint32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(BatchOpts),
+                                                  _u64p, C.POINTER(C.c_int), C.POINTER(RunStats)])
+EST_FEATURES = 44
+_est_features = _sig("asdm_est_features", C.c_int, [_vp, C.c_uint32, _u64p, C.POINTER(C.c_float), _u32p, _u32p,
+                                                    C.c_uint64, _u32p, _u64p, _u64p])
+_plan_learned = _sig("asdm_plan_create_learned", C.c_int, [C.c_uint32, C.POINTER(_vp), _vp, C.c_uint32,
+                                                           C.POINTER(_vp)])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -285,6 +313,40 @@ class CandidateSpace:
     def build_cand_cfl(self) -> bool:
         """The reference's return value: False when some candidate set is empty."""
         return self.nonempty
+
+    def edge_totals(self) -> np.ndarray:
+        """Candidate-edge entries per directed query edge, query-CSR order."""
+        out = np.zeros(max(int(self.q.offsets[-1]), 1), np.uint64)
+        _check(_cs_edge_totals(self._h, _ptr(out, _u64p)))
+        return out[:int(self.q.offsets[-1])]
+
+    def prefix_counts(self, orders: Sequence[Sequence[int]], time_limit_s: float = 0.0, count_limit: int = 0):
+        """Partial-match counts of each prefix (a connected sequence of query
+        vertices) inside this candidate space, in one batched launch.
+        Returns (counts uint64, status int32)."""
+        n = self.q.n
+        k = len(orders)
+        mat = np.zeros((max(k, 1), n), np.uint32)
+        depths = np.zeros(max(k, 1), np.uint32)
+        for i, o in enumerate(orders):
+            mat[i, :len(o)] = o
+            depths[i] = len(o)
+        counts = np.zeros(max(k, 1), np.uint64)
+        status = np.zeros(max(k, 1), np.int32)
+        rc = _prefix_counts(self._h, k, _ptr(mat), _ptr(depths), time_limit_s, count_limit, _ptr(counts, _u64p),
+                            status.ctypes.data_as(C.POINTER(C.c_int)))
+        if rc == ERR_CUDA:
+            _check(rc, "prefix counts")
+        return counts[:k], status[:k]
+
+    @classmethod
+    def _wrap(cls, h: int, q: HostGraph, dg: DeviceGraph, nonempty: bool) -> "CandidateSpace":
+        obj = cls.__new__(cls)
+        obj._h = _vp(h)
+        obj.q = q
+        obj.dg = dg
+        obj.nonempty = nonempty
+        return obj
 
     def build_stats(self):
         """(algorithmic bytes, device ms) of the candidate-space build."""
@@ -547,6 +609,149 @@ def run_batch_local(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s:
     if rc == ERR_CUDA:
         _check(rc, "batch")
     return b.counts.copy(), b.status.copy(), mats
+
+
+def run_batch_ex(dg: DeviceGraph, b: BatchInput, time_limit_s: float = 0.0, count_limit: int = 0,
+                 cards: Optional[Sequence[Optional["Card"]]] = None, estimator: Optional["Estimator"] = None,
+                 learned_max_subset: int = 0) -> RunStats:
+    """Batched counting with per-query count limits, plan caches or learned
+    plans; results in b.counts / b.status."""
+    opts = BatchOpts()
+    opts.time_limit_s = time_limit_s
+    opts.count_limit = count_limit
+    if estimator is not None:
+        opts.estimator = estimator._h
+        opts.learned_max_subset = learned_max_subset
+    keep = None
+    if cards is not None:
+        keep = (_vp * max(1, b.nq))(*[(c._h if c is not None else _vp()) for c in cards])
+        opts.cards = C.cast(keep, C.POINTER(_vp))
+    st = RunStats()
+    rc = _run_batch_ex(dg._h, b.nq, _ptr(b.sizes), _ptr(b.ob, _u64p), _ptr(b.offs), _ptr(b.nb, _u64p), _ptr(b.nbrs),
+                       _ptr(b.lb, _u64p), _ptr(b.labs), C.byref(opts), _ptr(b.counts, _u64p),
+                       b.status.ctypes.data_as(C.POINTER(C.c_int)), None, C.byref(st))
+    if rc == ERR_CUDA:
+        _check(rc, "batch")
+    return st
+
+
+def candidate_spaces(dg: DeviceGraph, queries: Sequence[HostGraph], b: Optional[BatchInput] = None):
+    """Candidate spaces of many queries built in groups; None where a build failed."""
+    b = b or BatchInput(queries)
+    nq = b.nq
+    hs = (_vp * max(1, nq))()
+    ne = np.zeros(max(1, nq), np.int32)
+    st = np.zeros(max(1, nq), np.int32)
+    rc = _cs_batch(dg._h, nq, _ptr(b.sizes), _ptr(b.ob, _u64p), _ptr(b.offs), _ptr(b.nb, _u64p), _ptr(b.nbrs),
+                   _ptr(b.lb, _u64p), _ptr(b.labs), hs, ne.ctypes.data_as(C.POINTER(C.c_int)),
+                   st.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc == ERR_CUDA:
+        _check(rc, "candidate spaces")
+    return [CandidateSpace._wrap(hs[i], queries[i], dg, bool(ne[i])) if st[i] == OK and hs[i] else None
+            for i in range(nq)]
+
+
+def run_planned(css: Sequence[CandidateSpace], plans: Sequence[Optional["Plan"]], time_limit_s: float = 0.0,
+                count_limit: int = 0):
+    """One persistent launch over given candidate spaces and plans: (counts, status, RunStats)."""
+    nq = len(css)
+    ch = (_vp * max(1, nq))(*[c._h for c in css])
+    ph = (_vp * max(1, nq))(*[(p._h if p is not None else _vp()) for p in plans])
+    opts = BatchOpts()
+    opts.time_limit_s = time_limit_s
+    opts.count_limit = count_limit
+    counts = np.zeros(max(1, nq), np.uint64)
+    status = np.zeros(max(1, nq), np.int32)
+    st = RunStats()
+    rc = _run_planned(nq, ch, ph, C.byref(opts), _ptr(counts, _u64p), status.ctypes.data_as(C.POINTER(C.c_int)),
+                      C.byref(st))
+    if rc == ERR_CUDA:
+        _check(rc, "planned batch")
+    return counts[:nq], status[:nq], st
+
+
+def subset_features(cs: CandidateSpace, masks: Sequence[int]):
+    """The estimator's input for sub-queries (vertex bitmasks) of cs's query:
+    (x [nodes, EST_FEATURES] float32, adj_off, adj, node_graph)."""
+    m = np.ascontiguousarray(masks, np.uint64)
+    nn, na = C.c_uint64(), C.c_uint64()
+    _check(_est_features(cs._h, len(m), _ptr(m, _u64p), None, None, None, 0, None, C.byref(nn), C.byref(na)),
+           "features")
+    x = np.zeros((max(nn.value, 1), EST_FEATURES), np.float32)
+    off = np.zeros(nn.value + 1, np.uint32)
+    adj = np.zeros(max(na.value, 1), np.uint32)
+    gid = np.zeros(max(nn.value, 1), np.uint32)
+    _check(_est_features(cs._h, len(m), _ptr(m, _u64p), x.ctypes.data_as(C.POINTER(C.c_float)), _ptr(off), _ptr(adj),
+                         adj.size, _ptr(gid), C.byref(nn), C.byref(na)), "features")
+    return x[:nn.value], off, adj[:na.value], gid[:nn.value]
+
+
+def plans_learned(css: Sequence[CandidateSpace], est: "Estimator", max_subset: int = 0) -> List["Plan"]:
+    """Plans from learned cardinalities, all queries planned in lockstep."""
+    nq = len(css)
+    ch = (_vp * max(1, nq))(*[c._h for c in css])
+    out = (_vp * max(1, nq))()
+    _check(_plan_learned(nq, ch, est._h, max_subset, out), "learned plans")
+    plans = []
+    for i in range(nq):
+        p = Plan.__new__(Plan)
+        p._h = _vp(out[i])
+        p.n = css[i].q.n
+        plans.append(p)
+    return plans
+
+
+class Estimator:
+    """The learned cardinality estimator: a 3-layer message-passing network on
+    the device (BF16 tcgen05 GEMMs, FP32 accumulation), predicting
+    log(1 + cardinality) of a (sub-)query graph from per-node features."""
+
+    def __init__(self, in_features: int, seed: int = 0):
+        h = _vp()
+        _check(_est_create(in_features, seed, C.byref(h)), "estimator")
+        self._h = h
+        self.in_features = in_features
+
+    @staticmethod
+    def _batch(x, adj_off, adj, node_graph):
+        x = np.ascontiguousarray(x, np.float32)
+        adj_off = np.ascontiguousarray(adj_off, np.uint32)
+        adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1), np.uint32)
+        node_graph = np.ascontiguousarray(node_graph, np.uint32)
+        return x, adj_off, adj, node_graph
+
+    def train_step(self, x, adj_off, adj, node_graph, target, lr: float = 1e-3) -> float:
+        x, adj_off, adj, node_graph = self._batch(x, adj_off, adj, node_graph)
+        t = np.ascontiguousarray(target, np.float32)
+        loss = C.c_float()
+        _check(_est_train(self._h, x.shape[0], len(t), x.ctypes.data_as(C.POINTER(C.c_float)), _ptr(adj_off),
+                          _ptr(adj), _ptr(node_graph), t.ctypes.data_as(C.POINTER(C.c_float)), lr, C.byref(loss)),
+               "estimator step")
+        return loss.value
+
+    def predict(self, x, adj_off, adj, node_graph, n_graphs: int) -> np.ndarray:
+        x, adj_off, adj, node_graph = self._batch(x, adj_off, adj, node_graph)
+        out = np.zeros(n_graphs, np.float32)
+        _check(_est_predict(self._h, x.shape[0], n_graphs, x.ctypes.data_as(C.POINTER(C.c_float)), _ptr(adj_off),
+                            _ptr(adj), _ptr(node_graph), out.ctypes.data_as(C.POINTER(C.c_float))), "estimator")
+        return out
+
+    def params(self) -> np.ndarray:
+        cnt = C.c_uint64()
+        _check(_est_params(self._h, None, 0, C.byref(cnt)))
+        out = np.zeros(cnt.value, np.float32)
+        _check(_est_params(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), cnt.value, C.byref(cnt)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(_est_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size), "estimator params")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _est_free(h)
+            self._h = None
 
 
 def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0):

@@ -104,6 +104,13 @@ extern "C" int asdm_graph_get_tuning(const asdm_graph *g, asdm_tuning *t) {
     return ASDM_OK;
 }
 
+extern "C" int asdm_cs_edge_totals(const asdm_cs *cs, uint64_t *totals) {
+    if (!cs || !totals) return fail(ASDM_ERR_INVALID, "null argument");
+    const uint32_t ne = cs->q.off[cs->q.n];
+    for (uint32_t e = 0; e < ne; ++e) totals[e] = cs->nonempty ? cs->etotal[e] : 0;
+    return ASDM_OK;
+}
+
 extern "C" int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms) {
     if (!cs) return fail(ASDM_ERR_INVALID, "null argument");
     if (build_bytes) *build_bytes = cs->build_bytes;
@@ -174,9 +181,12 @@ extern "C" int asdm_intersect_batch(const uint32_t *values, const uint64_t *list
 
 namespace asdm {
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
+int build_prefix_plan(const asdm_cs &cs, const uint32_t *order, uint32_t depth, asdm_plan &p);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
-                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg,
+                    double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
                     uint64_t *const *local_out);
+int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
+                       std::vector<asdm_plan> &plans);
 }  // namespace asdm
 
 // Candidate-space state a group may hold at once (state words, storage and
@@ -186,7 +196,9 @@ static constexpr uint64_t kGroupStateBytes = 16ull << 30;
 static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
                           const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
                           const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
-                          uint64_t *counts, int *status, asdm_run_stats *stats, uint64_t *const *local_out) {
+                          uint64_t count_limit, const asdm_card *const *cards, asdm_estimator *est,
+                          uint32_t est_kmax, uint64_t *counts, int *status, asdm_run_stats *stats,
+                          uint64_t *const *local_out) {
     clear_error();
     if (stats) *stats = asdm_run_stats{};
     if (!g || (nq && (!q_sizes || !q_off_base || !q_offsets || !q_nbr_base || !q_nbrs || !q_lab_base || !q_labels ||
@@ -243,9 +255,15 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
         std::vector<asdm_cs *> run_cs;
         std::vector<const asdm_plan *> run_plans;
         std::vector<uint32_t> run_ids;
+        int learned_rc = ASDM_OK;
+        if (est) learned_rc = plan_batch_learned(group, est, est_kmax, plans);
         for (size_t k = 0; k < ids.size(); ++k) {
             if (!group[k]->nonempty) continue;  // count 0, like the reference's early return
-            const int prc = build_plan(*group[k], nullptr, plans[k]);
+            int prc;
+            if (!est) prc = build_plan(*group[k], nullptr, plans[k], cards ? cards[ids[k]] : nullptr);
+            else if (learned_rc != ASDM_OK) prc = learned_rc;
+            else if (plans[k].order.size() != group[k]->q.n) prc = fail(ASDM_ERR_INVALID, "query is not connected");
+            else prc = ASDM_OK;
             if (prc != ASDM_OK) {
                 status[ids[k]] = prc;
                 if (worst == ASDM_OK) worst = prc;
@@ -261,7 +279,7 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
         if (local_out)
             for (uint32_t id : run_ids) lo.push_back(local_out[id]);
         asdm_run_stats gs{};
-        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, c.data(), st.data(), &gs,
+        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, count_limit, c.data(), st.data(), &gs,
                              local_out ? lo.data() : nullptr);
         if (stats) {
             stats->count += gs.count;
@@ -291,7 +309,17 @@ extern "C" int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_size
                               const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
                               uint64_t *counts, int *status, asdm_run_stats *stats) {
     return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
-                          time_limit_s, counts, status, stats, nullptr);
+                          time_limit_s, 0, nullptr, nullptr, 0, counts, status, stats, nullptr);
+}
+
+extern "C" int asdm_run_batch_ex(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                                 const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                                 const uint64_t *q_lab_base, const uint32_t *q_labels, const asdm_batch_opts *opts,
+                                 uint64_t *counts, int *status, uint64_t *const *local_counts, asdm_run_stats *stats) {
+    if (!opts) return fail(ASDM_ERR_INVALID, "null options");
+    return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
+                          opts->time_limit_s, opts->count_limit, opts->cards, opts->estimator,
+                          opts->learned_max_subset, counts, status, stats, local_counts);
 }
 
 extern "C" int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
@@ -301,5 +329,153 @@ extern "C" int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *
                                     asdm_run_stats *stats) {
     if (nq && !local_counts) return fail(ASDM_ERR_INVALID, "null local-count array");
     return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
-                          time_limit_s, counts, status, stats, local_counts);
+                          time_limit_s, 0, nullptr, nullptr, 0, counts, status, stats, local_counts);
+}
+
+// Partial-match counts of many prefixes of one query in one batched launch.
+extern "C" int asdm_prefix_counts(asdm_cs *cs, uint32_t nprefix, const uint32_t *orders, const uint32_t *depths,
+                                  double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status) {
+    clear_error();
+    if (!cs || (nprefix && (!orders || !depths || !counts || !status))) return fail(ASDM_ERR_INVALID, "null argument");
+    const uint32_t n = cs->q.n;
+    std::vector<asdm_plan> plans(nprefix);
+    std::vector<asdm_cs *> run_cs;
+    std::vector<const asdm_plan *> run_plans;
+    std::vector<uint32_t> run_ids;
+    int worst = ASDM_OK;
+    for (uint32_t i = 0; i < nprefix; ++i) {
+        counts[i] = 0;
+        status[i] = build_prefix_plan(*cs, orders + (uint64_t)i * n, depths[i], plans[i]);
+        if (status[i] != ASDM_OK) {
+            if (worst == ASDM_OK) worst = status[i];
+            continue;
+        }
+        if (!cs->nonempty) continue;  // an empty candidate space has no partial matches
+        if (depths[i] == 1) {
+            counts[i] = cs->ncand[orders[(uint64_t)i * n]];
+            if (count_limit && counts[i] > count_limit) status[i] = ASDM_ERR_LIMIT;
+            continue;
+        }
+        run_cs.push_back(cs);
+        run_plans.push_back(&plans[i]);
+        run_ids.push_back(i);
+    }
+    if (run_ids.empty()) return worst;
+    std::vector<uint64_t> c(run_ids.size());
+    std::vector<int> st(run_ids.size());
+    const int rc = run_batch_count(cs->g, run_cs, run_plans, time_limit_s, count_limit, c.data(), st.data(), nullptr,
+                                   nullptr);
+    for (size_t k = 0; k < run_ids.size(); ++k) {
+        counts[run_ids[k]] = c[k];
+        status[run_ids[k]] = st[k];
+        if (st[k] != ASDM_OK && worst == ASDM_OK) worst = st[k];
+    }
+    if (rc != ASDM_OK && (worst == ASDM_OK || rc == ASDM_ERR_CUDA)) worst = rc;
+    return worst;
+}
+
+// Candidate spaces of many queries, built in groups (one K1-K3 launch per
+// phase per group), for callers that plan between filtering and enumeration.
+extern "C" int asdm_candidate_space_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes,
+                                          const uint64_t *q_off_base, const uint32_t *q_offsets,
+                                          const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                                          const uint64_t *q_lab_base, const uint32_t *q_labels, asdm_cs **out,
+                                          int *nonempty, int *status) {
+    clear_error();
+    if (!g || (nq && (!q_sizes || !q_off_base || !q_offsets || !q_nbr_base || !q_nbrs || !q_lab_base || !q_labels ||
+                      !out || !nonempty || !status)))
+        return fail(ASDM_ERR_INVALID, "null argument");
+    std::vector<std::unique_ptr<asdm_cs>> all(nq);
+    std::vector<uint64_t> state(nq, 0);
+    int worst = ASDM_OK;
+    for (uint32_t i = 0; i < nq; ++i) {
+        out[i] = nullptr;
+        nonempty[i] = 0;
+        auto c = std::make_unique<asdm_cs>();
+        c->g = g;
+        status[i] = make_query(q_offsets + q_off_base[i], q_nbrs + q_nbr_base[i], q_labels + q_lab_base[i], q_sizes[i],
+                               c->q);
+        if (status[i] != ASDM_OK) {
+            if (worst == ASDM_OK) worst = status[i];
+            continue;
+        }
+        for (uint32_t u = 0; u < c->q.n; ++u) {
+            const uint32_t l = c->q.lab[u];
+            if (l < g->d.nlabels) state[i] += 12ull * (g->h_vbl_off[l + 1] - g->h_vbl_off[l]);
+        }
+        all[i] = std::move(c);
+    }
+    uint32_t i = 0;
+    while (i < nq) {
+        std::vector<uint32_t> ids;
+        uint64_t bytes = 0;
+        for (; i < nq; ++i) {
+            if (!all[i]) continue;
+            if (!ids.empty() && bytes + state[i] > kGroupStateBytes) break;
+            ids.push_back(i);
+            bytes += state[i];
+        }
+        if (ids.empty()) continue;
+        std::vector<asdm_cs *> group;
+        for (uint32_t id : ids) group.push_back(all[id].get());
+        const int rc = build_batch(group);
+        for (uint32_t id : ids) {
+            status[id] = rc;
+            if (rc == ASDM_OK) {
+                nonempty[id] = all[id]->nonempty ? 1 : 0;
+                out[id] = all[id].release();
+            } else {
+                all[id].reset();
+            }
+        }
+        if (rc != ASDM_OK && worst == ASDM_OK) worst = rc;
+        if (rc == ASDM_ERR_CUDA) break;
+    }
+    return worst;
+}
+
+// One persistent launch over candidate spaces and plans the caller built.
+extern "C" int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans,
+                                const asdm_batch_opts *opts, uint64_t *counts, int *status, asdm_run_stats *stats) {
+    clear_error();
+    if (stats) *stats = asdm_run_stats{};
+    if (nq && (!cs || !plans || !counts || !status)) return fail(ASDM_ERR_INVALID, "null argument");
+    asdm_graph *g = nullptr;
+    std::vector<asdm_cs *> run_cs;
+    std::vector<const asdm_plan *> run_plans;
+    std::vector<uint32_t> run_ids;
+    int worst = ASDM_OK;
+    for (uint32_t i = 0; i < nq; ++i) {
+        counts[i] = 0;
+        status[i] = ASDM_OK;
+        if (!cs[i] || !plans[i]) {
+            status[i] = fail(ASDM_ERR_INVALID, "query %u has no candidate space or plan", i);
+        } else if (g && cs[i]->g != g) {
+            status[i] = fail(ASDM_ERR_INVALID, "query %u is on another graph", i);
+        } else if (plans[i]->order.size() != cs[i]->q.n) {
+            status[i] = fail(ASDM_ERR_INVALID, "plan %u does not match its query", i);
+        }
+        if (status[i] != ASDM_OK) {
+            if (worst == ASDM_OK) worst = status[i];
+            continue;
+        }
+        g = cs[i]->g;
+        if (!cs[i]->nonempty) continue;
+        run_cs.push_back(cs[i]);
+        run_plans.push_back(plans[i]);
+        run_ids.push_back(i);
+    }
+    if (run_ids.empty()) return worst;
+    std::vector<uint64_t> c(run_ids.size());
+    std::vector<int> st(run_ids.size());
+    const double tl = opts ? opts->time_limit_s : 0.0;
+    const uint64_t cl = opts ? opts->count_limit : 0;
+    const int rc = run_batch_count(g, run_cs, run_plans, tl, cl, c.data(), st.data(), stats, nullptr);
+    for (size_t k = 0; k < run_ids.size(); ++k) {
+        counts[run_ids[k]] = c[k];
+        status[run_ids[k]] = st[k];
+        if (st[k] != ASDM_OK && worst == ASDM_OK) worst = st[k];
+    }
+    if (rc != ASDM_OK && (worst == ASDM_OK || rc == ASDM_ERR_CUDA)) worst = rc;
+    return worst;
 }

@@ -54,3 +54,24 @@ struct asdm_plan {
     std::vector<std::vector<uint32_t>> conf;                       // level -> earlier same-label, non-adjacent levels
     double cost = 0.0;                                             // planner's estimate
 };
+
+namespace asdm {
+// The planner's greedy order search, in steps, so that a batched caller can
+// supply its own cardinalities for the candidates of a step.
+struct GreedyState {
+    std::vector<uint32_t> order;
+    std::vector<char> in;
+    uint64_t mask = 0;   // bit u = query vertex u in the prefix
+    double N = 0.0;      // estimated partial matches of the prefix
+    double cost = 0.0;   // estimated work so far
+};
+struct GreedyCand {
+    uint32_t u;
+    double Nu;    // estimated partial matches with u appended
+    double work;  // estimated work of the step
+    uint32_t B;   // backward edges of u
+};
+void greedy_start(const asdm_cs &cs, uint32_t start, GreedyState &st);
+void greedy_candidates(const asdm_cs &cs, const GreedyState &st, std::vector<GreedyCand> &out);
+bool greedy_take(const asdm_cs &cs, GreedyState &st, const std::vector<GreedyCand> &cands);
+}  // namespace asdm

@@ -320,6 +320,7 @@ struct Warp {
                 // per-query totals; an overflow marks only that query
                 const unsigned long long old = atomicAdd(&a.qcounts[q], count);
                 if (overflow || old + count < old) atomicOr(&a.qflags[q], kFlagOverflow);
+                if (a.count_limit && old + count > a.count_limit) atomicOr(&a.qflags[q], kFlagLimit);
                 atomicAdd(&a.ctr[kCtrCount], count);
             } else {
                 const unsigned long long old = atomicAdd(&a.ctr[kCtrCount], count);
@@ -627,6 +628,11 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
                 want = idle > pend && (long long)pend >= 0;
             }
             if (__shfl_sync(kFull, st, 0)) return false;
+            if (MULTI && a.count_limit) {
+                uint32_t lim = 0;
+                if (lane == 0) lim = *(volatile unsigned int *)&a.qflags[W.q] & kFlagLimit;
+                if (__shfl_sync(kFull, lim, 0)) return true;  // abandon this query's subtree
+            }
             if (__shfl_sync(kFull, want, 0)) W.try_donate(base, d);
         }
         if (W.pos[d] < W.cnt[d]) {
@@ -709,7 +715,9 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                     P = a.qd[qq].pairs;
                 }
                 unsigned long long t = b * K;
-                const unsigned long long t_end = min(t + K, P);
+                unsigned long long t_end = min(t + K, P);
+                // a query past its count limit is abandoned
+                if (MULTI && a.count_limit && (*(volatile unsigned int *)&a.qflags[W.q] & kFlagLimit)) t_end = t;
                 if (W.n == 1) {
                     for (; t < t_end; ++t) {
                         if (lane == 0) {
@@ -830,7 +838,7 @@ int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
 // 64K pairs per block count, between 1 and 256 pairs per block.
 void root_blocks(const asdm_cs &cs, const asdm_plan &plan, unsigned long long &pairs, unsigned long long &blk,
                  unsigned long long &nblocks) {
-    if (cs.q.n == 1) {
+    if (plan.order.size() == 1) {
         pairs = cs.ncand[plan.order[0]];
     } else {
         pairs = cs.etotal[plan.back[1][0].second];
@@ -1015,7 +1023,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
 // Batched form: one persistent launch counts every query of a group.
 // counts[i] / status[i] receive each query's result.
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
-                    double time_limit_s, uint64_t *counts, int *status, asdm_run_stats *agg,
+                    double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
                     uint64_t *const *local_out) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
@@ -1044,7 +1052,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     for (uint32_t li = 0; li < L; ++li) {
         const asdm_cs &c = *cs[live[li]];
         const asdm_plan &plan = *plans[live[li]];
-        const uint32_t n = c.q.n;
+        const uint32_t n = (uint32_t)plan.order.size();  // q.n, or a prefix's depth
         std::vector<DLevel> lv(n);
         std::vector<DBack> bk;
         std::vector<uint32_t> cf;
@@ -1126,6 +1134,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         a.qcounts = d_qcounts;
         a.qflags = d_qflags;
         a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
+        a.count_limit = count_limit;
         const uint32_t smem = 4u * kWarps * warp_words(maxn, maxnb);
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -1182,6 +1191,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             if (gflags & kFlagInternal) status[i] = ASDM_ERR_INTERNAL;
             else if (gflags & kFlagTimeout) status[i] = ASDM_ERR_TIMEOUT;
             else if (qf[li] & kFlagOverflow) status[i] = ASDM_ERR_OVERFLOW;
+            else if (qf[li] & kFlagLimit) status[i] = ASDM_ERR_LIMIT;
         }
         if (agg) {
             agg->count = ctr[kCtrCount];

@@ -29,57 +29,85 @@ double avg_len(const asdm_cs &cs, uint32_t from, uint32_t to) {
     return cs.ncand[from] ? (double)cs.etotal[e] / (double)cs.ncand[from] : 0.0;
 }
 
+}  // namespace
+
+// One step of the greedy order search: every vertex u adjacent to the prefix
+// with the model's estimate of the extended prefix's cardinality.
+void greedy_candidates(const asdm_cs &cs, const GreedyState &st, std::vector<GreedyCand> &out) {
+    const QueryGraph &q = cs.q;
+    out.clear();
+    std::vector<double> lens;
+    for (uint32_t u = 0; u < q.n; ++u) {
+        if (st.in[u]) continue;
+        double drv = INFINITY;
+        lens.clear();
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            const uint32_t j = q.nbr[e];
+            if (!st.in[j]) continue;
+            const double a = avg_len(cs, j, u);
+            lens.push_back(a);
+            drv = std::min(drv, a);
+        }
+        if (lens.empty()) continue;
+        double factor = drv;
+        bool skipped = false;
+        for (double a : lens) {
+            if (!skipped && a == drv) { skipped = true; continue; }
+            factor *= std::min(1.0, a / std::max(1.0, (double)cs.ncand[u]));
+        }
+        GreedyCand c;
+        c.u = u;
+        c.Nu = st.N * factor;
+        c.work = st.N * (1.0 + lens.size() * std::ceil(std::max(drv, 1.0) / 32.0));
+        c.B = (uint32_t)lens.size();
+        out.push_back(c);
+    }
+}
+
+void greedy_start(const asdm_cs &cs, uint32_t start, GreedyState &st) {
+    st.in.assign(cs.q.n, 0);
+    st.order.assign(1, start);
+    st.in[start] = 1;
+    st.mask = 1ull << start;
+    st.N = (double)cs.ncand[start];
+    st.cost = 0.0;
+}
+
+// Takes the candidate with the smallest estimate (more backward edges on a
+// tie); false when the prefix cannot grow (the query is disconnected).
+bool greedy_take(const asdm_cs &cs, GreedyState &st, const std::vector<GreedyCand> &cands) {
+    const GreedyCand *best = nullptr;
+    for (const GreedyCand &c : cands)
+        if (!best || c.Nu < best->Nu || (c.Nu == best->Nu && c.B > best->B)) best = &c;
+    if (!best) {
+        st.cost = INFINITY;
+        return false;
+    }
+    st.order.push_back(best->u);
+    st.in[best->u] = 1;
+    st.mask |= 1ull << best->u;
+    st.cost += best->work + (st.order.size() < cs.q.n ? best->Nu : 0.0);
+    st.N = std::max(best->Nu, 1e-9);
+    return true;
+}
+
+namespace {
+
 // With a cardinality cache (`.card`), a prefix whose vertex set is in the
 // cache uses the cached cardinality instead of the model's estimate.
 void greedy_from(const asdm_cs &cs, const asdm_card *card, uint32_t start, std::vector<uint32_t> &order,
                  double &cost) {
-    const QueryGraph &q = cs.q;
-    const uint32_t n = q.n;
-    std::vector<char> in(n, 0);
-    order.assign(1, start);
-    in[start] = 1;
-    uint64_t mask = 1ull << start;
-    double N = card_lookup_or(card, mask, (double)cs.ncand[start]);
-    cost = 0.0;
-    for (uint32_t k = 1; k < n; ++k) {
-        int best = -1;
-        double bestN = 0, bestWork = 0;
-        uint32_t bestB = 0;
-        for (uint32_t u = 0; u < n; ++u) {
-            if (in[u]) continue;
-            double drv = INFINITY;
-            std::vector<double> lens;
-            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-                const uint32_t j = q.nbr[e];
-                if (!in[j]) continue;
-                const double a = avg_len(cs, j, u);
-                lens.push_back(a);
-                drv = std::min(drv, a);
-            }
-            if (lens.empty()) continue;
-            double factor = drv;
-            bool skipped = false;
-            for (double a : lens) {
-                if (!skipped && a == drv) { skipped = true; continue; }
-                factor *= std::min(1.0, a / std::max(1.0, (double)cs.ncand[u]));
-            }
-            const double Nu = card_lookup_or(card, mask | (1ull << u), N * factor);
-            const double work = N * (1.0 + lens.size() * std::ceil(std::max(drv, 1.0) / 32.0));
-            const uint32_t B = (uint32_t)lens.size();
-            if (best < 0 || Nu < bestN || (Nu == bestN && B > bestB)) {
-                best = (int)u;
-                bestN = Nu;
-                bestWork = work;
-                bestB = B;
-            }
-        }
-        if (best < 0) { cost = INFINITY; return; }  // disconnected
-        order.push_back((uint32_t)best);
-        in[best] = 1;
-        mask |= 1ull << best;
-        cost += bestWork + (k + 1 < n ? bestN : 0.0);
-        N = std::max(bestN, 1e-9);
+    GreedyState st;
+    greedy_start(cs, start, st);
+    st.N = card_lookup_or(card, st.mask, st.N);
+    std::vector<GreedyCand> cands;
+    for (uint32_t k = 1; k < cs.q.n; ++k) {
+        greedy_candidates(cs, st, cands);
+        for (GreedyCand &c : cands) c.Nu = card_lookup_or(card, st.mask | (1ull << c.u), c.Nu);
+        if (!greedy_take(cs, st, cands)) break;
     }
+    order = st.order;
+    cost = st.cost;
 }
 
 }  // namespace
@@ -123,6 +151,37 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
             else if (q.lab[w] == q.lab[u]) p.conf[k].push_back(j);
         }
         if (k > 0 && p.back[k].empty()) return fail(ASDM_ERR_INVALID, "order is not connected at level %u", k);
+    }
+    return ASDM_OK;
+}
+
+// A plan over the first `depth` levels only: `order` lists distinct query
+// vertices, each after the first adjacent to an earlier one.  Enumerating it
+// counts the partial matches of the sub-query these vertices induce inside the
+// candidate space, which is what the reference's estimator approximates by
+// sampling (cardEstimateLabeled, plan/estimator.cpp:173-291).
+int build_prefix_plan(const asdm_cs &cs, const uint32_t *order, uint32_t depth, asdm_plan &p) {
+    const QueryGraph &q = cs.q;
+    const uint32_t n = q.n;
+    if (depth == 0 || depth > n) return fail(ASDM_ERR_INVALID, "prefix depth %u outside 1..%u", depth, n);
+    p.order.assign(order, order + depth);
+    std::vector<char> seen(n, 0);
+    for (uint32_t k = 0; k < depth; ++k) {
+        if (p.order[k] >= n || seen[p.order[k]]) return fail(ASDM_ERR_INVALID, "prefix repeats or leaves the query");
+        seen[p.order[k]] = 1;
+    }
+    p.cost = 0;
+    p.back.assign(depth, {});
+    p.conf.assign(depth, {});
+    for (uint32_t k = 0; k < depth; ++k) {
+        const uint32_t u = p.order[k];
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t w = p.order[j];
+            const int slot = q.slot(w, u);
+            if (slot >= 0) p.back[k].push_back({j, q.off[w] + (uint32_t)slot});
+            else if (q.lab[w] == q.lab[u]) p.conf[k].push_back(j);
+        }
+        if (k > 0 && p.back[k].empty()) return fail(ASDM_ERR_INVALID, "prefix is not connected at level %u", k);
     }
     return ASDM_OK;
 }

@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--profile", action="store_true", help="timed steps only: no e2e pass, no CPU baseline")
     ap.add_argument("--no-c4", action="store_true", help="skip the config-4 local-counting measurement")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel knobs (profiling runs)")
+    ap.add_argument("--estimator", default="", help="learned-estimator parameters (.npy); default: the trained "
+                                                    "config-1 model shipped with the package, when present")
+    ap.add_argument("--learned-max", type=int, default=0, help="largest prefix the estimator is asked about (0 = 6)")
     return ap.parse_args()
 
 
@@ -328,6 +331,23 @@ def main():
         return {"kernel_ms": st.kernel_ms, "list_bytes": st.list_bytes, "cs_ms": st.build_ms,
                 "cs_bytes": st.build_bytes, "matches": st.count, "inter": st.intersections}
 
+    est = None
+    est_path = args.estimator
+    if not est_path:
+        from asdmatch_b200 import estimator as E
+        est_path = E.DEFAULT_PARAMS if os.path.exists(E.DEFAULT_PARAMS) else ""
+    if est_path:
+        est = A.Estimator(A.EST_FEATURES, 0)
+        est.set_params(np.load(est_path))
+
+    def learned_step():
+        """Batched + learned: asdm_run_batch_ex with the estimator planning every query."""
+        st = A.run_batch_ex(dg, packed, estimator=est, learned_max_subset=args.learned_max)
+        if packed.counts.tolist() != counts or packed.status.any():
+            raise SystemExit("learned-plan counts differ from the screened counts")
+        return {"kernel_ms": st.kernel_ms, "list_bytes": st.list_bytes, "cs_ms": st.build_ms,
+                "cs_bytes": st.build_bytes, "matches": st.count, "inter": st.intersections}
+
     def timed(step_fn, steps):
         times, agg = [], None
         for _ in range(steps):
@@ -361,6 +381,21 @@ def main():
     for _ in range(max(1, args.warmup // 2)):
         plain_step()
     plain_ms, plain_agg = timed(plain_step, args.steps)
+    learned = None
+    if est is not None:
+        for _ in range(max(1, args.warmup // 2)):
+            learned_step()
+        learned_ms, learned_agg = timed(learned_step, args.steps)
+        learned = {"queries_per_s": world * Q / (learned_ms / 1e3), "ms_per_step": learned_ms,
+                   "enum_kernel_ms_per_step": learned_agg["kernel_ms"] / args.steps,
+                   "cs_build_ms_per_step": learned_agg["cs_ms"] / args.steps,
+                   "intersections_per_step": learned_agg["inter"] // args.steps,
+                   "over_plain": plain_ms / learned_ms, "over_cost_model_batched": ms / learned_ms,
+                   "estimator": os.path.relpath(est_path, ROOT) if est_path.startswith(ROOT) else est_path,
+                   "learned_max_subset": args.learned_max or 6,
+                   "what": "asdm_run_batch_ex with the learned estimator: candidate spaces, learned greedy plans "
+                           "(one forward pass per planner step for the whole group), one persistent launch; "
+                           "planning is inside the timed region"}
     # end to end through the one-call C ABI (asdm_run_batch) from host buffers
     e2e_times = []
     h2d = packed.nbytes()
@@ -417,6 +452,7 @@ def main():
                                    "what": "one query per launch sequence (asdm_candidate_space, asdm_plan_create, "
                                            "asdm_run_plan)"},
                        batched_over_plain=plain_ms / ms,
+                       batched_learned=learned,
                        autotune={"chosen": tune_best, "table": tune_table}),
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",

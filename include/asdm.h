@@ -42,6 +42,7 @@ typedef struct asdm_graph asdm_graph;           /* device-resident data graph  *
 typedef struct asdm_cs asdm_cs;                 /* device candidate space      */
 typedef struct asdm_plan asdm_plan;             /* matching order + level info */
 typedef struct asdm_card asdm_card;             /* .card cardinality cache     */
+typedef struct asdm_estimator asdm_estimator;   /* learned cardinality model   */
 
 /* Returns a static, thread-local description of the last failure. */
 const char *asdm_last_error(void);
@@ -136,6 +137,10 @@ int asdm_cs_read(const asdm_cs *cs, uint32_t u, uint32_t *out, uint32_t capacity
  * *total receives the number of entries; ASDM_ERR_CAPACITY if it exceeds capacity. */
 int asdm_cs_read_edges(const asdm_cs *cs, uint32_t u, uint32_t u2, uint32_t *offsets,
                        uint32_t *vertices, uint64_t capacity, uint64_t *total);
+/* Candidate-edge entries of every directed query edge, in query-CSR order
+ * (sum over v in C(u) of |candidateEdge[u][v][u2]|; the reference's query
+ * edge weights, relation/candidate_space.cpp:507-524). */
+int asdm_cs_edge_totals(const asdm_cs *cs, uint64_t *totals);
 /* Algorithmic bytes and device milliseconds of the K1-K3 build (the
  * reference's "Filtering time", main.cpp:38). */
 int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms);
@@ -248,6 +253,21 @@ int asdm_run_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const ui
                    const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
                    const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
                    uint64_t *counts, int *status, asdm_run_stats *stats);
+/* Options of asdm_run_batch_ex. */
+typedef struct asdm_batch_opts {
+    double time_limit_s;            /* 0 = none (device time for the whole group)          */
+    uint64_t count_limit;           /* 0 = none; a query past it stops with ASDM_ERR_LIMIT  */
+    const asdm_card *const *cards;  /* per query cardinality cache for its plan, or NULL    */
+    asdm_estimator *estimator;      /* learned estimates for the planner, or NULL           */
+    uint32_t learned_max_subset;    /* largest prefix the estimator is asked about (0 = 6) */
+} asdm_batch_opts;
+/* asdm_run_batch with per-query count limits and plan caches (the learned
+ * estimator's predictions reach the planner this way); local_counts as in
+ * asdm_run_batch_local, or NULL for counts only. */
+int asdm_run_batch_ex(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                      const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                      const uint64_t *q_lab_base, const uint32_t *q_labels, const asdm_batch_opts *opts,
+                      uint64_t *counts, int *status, uint64_t *const *local_counts, asdm_run_stats *stats);
 /* The same, also producing each query's |Vg| x |Vq_i| local-count matrix
  * (the reference's LOCAL_COUNT output, matching/join.cpp:1035-1041, one
  * process per query there) into local_counts[i] (row-major, may be NULL to
@@ -261,11 +281,72 @@ int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, co
 
 /* ---- learned cardinality estimator ------------------------------------- */
 
+/* The three stages of the batched form as separate calls, for callers that
+ * plan between filtering and enumeration (the learned estimator does):
+ * candidate spaces of nq packed queries (layout as asdm_run_batch), built in
+ * groups; out[i] is NULL where status[i] != 0, nonempty[i] as in
+ * asdm_candidate_space.  Each out[i] is freed with asdm_cs_free. */
+int asdm_candidate_space_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
+                               const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,
+                               const uint64_t *q_lab_base, const uint32_t *q_labels, asdm_cs **out, int *nonempty,
+                               int *status);
+/* Counts every (cs[i], plans[i]) in one persistent launch; all candidate
+ * spaces on the same graph; opts->cards is ignored (plans are given). */
+int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans, const asdm_batch_opts *opts,
+                     uint64_t *counts, int *status, asdm_run_stats *stats);
+
+/* Partial-match counts of query-vertex prefixes inside a candidate space:
+ * prefix i is orders[i*|Vq| .. i*|Vq| + depths[i]) (distinct vertices, each
+ * after the first adjacent to an earlier one); counts[i] receives the number
+ * of injective assignments of those vertices to their candidate sets along
+ * candidate edges, i.e. the cardinality the reference's estimator samples
+ * (cardEstimateLabeled, plan/estimator.cpp:173-291).  All prefixes run in one
+ * batched launch; status[i] as in asdm_run_batch (ASDM_ERR_LIMIT past
+ * count_limit, 0 = none). */
+int asdm_prefix_counts(asdm_cs *cs, uint32_t nprefix, const uint32_t *orders, const uint32_t *depths,
+                       double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status);
+
 /* The estimator's tensor-core GEMM on its own, for testing: C[M][N] =
  * sum_k A[m][k] * B[n][k] with A, B given as bf16 bit patterns (host arrays)
  * and C in fp32.  No reference counterpart (the reference estimates by
  * sampling, plan/estimator.cpp:173-291). */
 int asdm_gemm_bf16(int M, int N, int K, const uint16_t *A, const uint16_t *B, float *C);
+
+/* A 3-layer message-passing network over (sub-)query graphs, hidden width
+ * 128, BF16 weights/activations with FP32 accumulation, predicting
+ * log(1 + cardinality); forward, backward and Adam on the device.  It stands
+ * in for the reference's sampling estimator (cardEstimateLabeled,
+ * plan/estimator.cpp:173-291) as a source of subset cardinalities for the
+ * planner; it changes plans, never counts.
+ * A batch: n_nodes nodes with `in_features` fp32 features each (x, row-major),
+ * a symmetric adjacency in CSR over the batch's nodes (adj_off[n_nodes+1],
+ * adj), and node_graph[v] in [0, n_graphs). */
+int asdm_est_create(uint32_t in_features, uint64_t seed, asdm_estimator **out);
+int asdm_est_train_step(asdm_estimator *e, int n_nodes, int n_graphs, const float *x, const uint32_t *adj_off,
+                        const uint32_t *adj, const uint32_t *node_graph, const float *target, float lr,
+                        float *loss);
+int asdm_est_predict(asdm_estimator *e, int n_nodes, int n_graphs, const float *x, const uint32_t *adj_off,
+                     const uint32_t *adj, const uint32_t *node_graph, float *out);
+/* fp32 parameter vector (for saving); count receives its length. */
+int asdm_est_params(asdm_estimator *e, float *out, uint64_t capacity, uint64_t *count);
+int asdm_est_set_params(asdm_estimator *e, const float *in, uint64_t count);
+void asdm_est_free(asdm_estimator *e);
+/* The estimator's input for sub-queries of a query with a built candidate
+ * space: subset i is the vertex set masks[i] (bit u = query vertex u, at most
+ * 64 vertices, connected).  Writes, per subset in order, its vertices in
+ * ascending order as nodes: x (ASDM_EST_FEATURES floats per node), the local
+ * adjacency in CSR over all nodes (adj_off, adj; adj_capacity entries), and
+ * node_graph[node] = i.  *n_nodes / *n_adj receive the totals (call with
+ * NULL outputs to size them). */
+#define ASDM_EST_FEATURES 44
+int asdm_est_features(const asdm_cs *cs, uint32_t nsub, const uint64_t *masks, float *x, uint32_t *adj_off,
+                      uint32_t *adj, uint64_t adj_capacity, uint32_t *node_graph, uint64_t *n_nodes, uint64_t *n_adj);
+/* A plan chosen with learned cardinalities: the planner's greedy search, with
+ * every prefix of 3..max_subset vertices (0 = 6) estimated by the model, all
+ * starts of all given queries searched in lockstep (one forward pass per
+ * step).  plans[i] is freed with asdm_plan_free. */
+int asdm_plan_create_learned(uint32_t nq, asdm_cs *const *cs, asdm_estimator *e, uint32_t max_subset,
+                             asdm_plan **plans);
 
 #ifdef __cplusplus
 }
