@@ -97,7 +97,11 @@ _run_plan = _sig("asdm_run_plan", C.c_int, [_vp, _vp, C.POINTER(RunOpts), C.POIN
 _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(RunOpts),
                                                   C.POINTER(RunStats)])
 class Tuning(C.Structure):
-    _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32)]
+    _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32), ("planner", C.c_uint32)]
+
+
+PLANNER_DP = 0
+PLANNER_GREEDY = 1
 
 
 _set_tuning = _sig("asdm_graph_set_tuning", C.c_int, [_vp, C.POINTER(Tuning)])
@@ -271,13 +275,15 @@ class DeviceGraph:
         self.n = g.n
         self.host = g
 
-    def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int):
-        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max))), "tuning")
+    def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None):
+        if planner is None:
+            planner = self.tuning()["planner"]
+        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner))), "tuning")
 
     def tuning(self):
         t = Tuning()
         _check(_get_tuning(self._h, C.byref(t)))
-        return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max}
+        return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max, "planner": t.planner}
 
     def stream(self) -> int:
         """cudaStream_t (as an int) the library uses for this graph."""
@@ -762,31 +768,45 @@ def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float
 
 
 def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
-             min_blocks=(1, 4, 5, 6), lane_leaf=(32, 96, 256)):
-    """Times the caller's batch under every kernel configuration and keeps the
-    fastest on `dg` (device time between CUDA events on the library's stream).
-    Returns (best, table)."""
+             min_blocks=(1, 4, 5, 6), lane_leaf=(32, 96, 256), planners=(PLANNER_DP, PLANNER_GREEDY),
+             run=None):
+    """Times the caller's batch under every kernel configuration (with the
+    graph's current planner), then every planner with the fastest kernel
+    configuration, and keeps the fastest on `dg` (device time between CUDA
+    events on the library's stream).  `run(dg, batch)` is the timed call
+    (default: run_batch_packed).  Returns (best, table)."""
     import torch
+    run = run or run_batch_packed
     stream = torch.cuda.ExternalStream(dg.stream())
     want = None
     table = []
+
+    def measure(mb, ll, pl):
+        nonlocal want
+        dg.set_tuning(mb, ll, pl)
+        run(dg, batch)  # warm
+        if want is None:
+            want = batch.counts.copy()
+        elif not np.array_equal(batch.counts, want):
+            raise AsdmError(ERR_INTERNAL, "tuning changed a count")
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(dg, batch)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "planner": pl, "ms": min(times)})
+
+    pl0 = dg.tuning()["planner"]
     for mb in min_blocks:
         for ll in lane_leaf:
-            dg.set_tuning(mb, ll)
-            run_batch_packed(dg, batch)  # warm
-            if want is None:
-                want = batch.counts.copy()
-            elif not np.array_equal(batch.counts, want):
-                raise AsdmError(ERR_INTERNAL, "tuning changed a count")
-            times = []
-            for _ in range(reps):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                run_batch_packed(dg, batch)
-                e1.record(stream)
-                e1.synchronize()
-                times.append(e0.elapsed_time(e1))
-            table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "ms": min(times)})
+            measure(mb, ll, pl0)
     best = min(table, key=lambda r: r["ms"])
-    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"])
+    for pl in planners:
+        if pl != pl0:
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], pl)
+    best = min(table, key=lambda r: r["ms"])
+    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"])
     return best, table

@@ -94,6 +94,8 @@ extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
     if (t->enum_min_blocks != 1 && (t->enum_min_blocks < 4 || t->enum_min_blocks > 6))
         return fail(ASDM_ERR_INVALID, "enum_min_blocks must be 1, 4, 5 or 6");
     if (t->lane_leaf_max > 4096) return fail(ASDM_ERR_INVALID, "lane_leaf_max must be <= 4096");
+    if (t->planner != ASDM_PLANNER_DP && t->planner != ASDM_PLANNER_GREEDY)
+        return fail(ASDM_ERR_INVALID, "planner must be ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY");
     g->tuning = *t;
     return ASDM_OK;
 }

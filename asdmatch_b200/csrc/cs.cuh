@@ -1,6 +1,7 @@
 // Candidate space of one query on the device (the product of K1-K3).
 #pragma once
 
+#include <functional>
 #include <memory>
 
 #include "device.cuh"
@@ -74,4 +75,13 @@ struct GreedyCand {
 void greedy_start(const asdm_cs &cs, uint32_t start, GreedyState &st);
 void greedy_candidates(const asdm_cs &cs, const GreedyState &st, std::vector<GreedyCand> &out);
 bool greedy_take(const asdm_cs &cs, GreedyState &st, const std::vector<GreedyCand> &cands);
+// Exhaustive search over connected prefixes for queries of at most
+// kDpMaxVertices vertices and kDpMaxSubsets connected vertex subsets; false
+// when the query is larger (the caller falls back to the greedy search).
+// known(S, c) supplies the cardinality of subset S where the caller has one.
+constexpr uint32_t kDpMaxVertices = 24;
+constexpr size_t kDpMaxSubsets = 1u << 12;
+bool connected_subsets(const QueryGraph &q, uint32_t max_size, size_t limit, std::vector<uint64_t> &out);
+bool plan_dp(const asdm_cs &cs, const std::function<bool(uint64_t, double &)> &known, std::vector<uint32_t> &order,
+             double &cost);
 }  // namespace asdm

@@ -95,6 +95,10 @@ struct EnumArgs {
     uint32_t nquery, maxn, maxnb;
     unsigned long long *qcounts;
     unsigned int *qflags;
+    // closed form of the last two levels (single-query kernel; QDesc for batches)
+    const unsigned long long *ps;
+    const uint32_t *rev_off, *rev_list;
+    uint32_t tail;
 };
 
 struct QDesc {
@@ -103,8 +107,19 @@ struct QDesc {
     const uint32_t *conf;
     unsigned long long *local;  // |Vg| x n (MODE_LOCAL batches)
     unsigned long long pairs, blk;
-    uint32_t n, nb, nc, pad;
+    uint32_t n, nb, nc, tail;
+    const unsigned long long *ps;
+    const uint32_t *rev_off, *rev_list;
 };
+
+// The last two levels of a COUNT-mode plan are counted in closed form when
+// each has exactly one backward edge (always so for tree-shaped queries):
+// kTailChain when the last level's edge comes from level n-2 (needs prefix
+// sums of the last level's list lengths along level n-2's driver edge, and
+// the reverse candidate edges last level -> level n-2), kTailLeaf when it
+// comes from an earlier level (the last level's list is then fixed by the
+// prefix).
+enum : uint32_t { kTailNone = 0, kTailChain = 1, kTailLeaf = 2 };
 
 __host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 32; }
 
@@ -172,12 +187,16 @@ struct Warp {
     unsigned long long *local;  // |Vg| x n local counts of the current query (MODE_LOCAL)
     unsigned long long count = 0, inter = 0, elems = 0;
     bool overflow = false;
+    const unsigned long long *ps;        // kTailChain: prefix sums over the driver edge of level n-2
+    const uint32_t *rev_off, *rev_list;  // kTailChain: candidate edges last level -> level n-2
+    uint32_t tail;                       // kTail* of the current query
 
     // w: this warp's shared-memory words, laid out for queries of up to maxn
     // levels and maxnb backward edges.
     __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln,
                     uint32_t levels, uint32_t maxn, uint32_t maxnb)
-        : a(args), L(l), B(b), CF(cf), lane(ln), n(levels), local(args.local) {
+        : a(args), L(l), B(b), CF(cf), lane(ln), n(levels), local(args.local), ps(args.ps), rev_off(args.rev_off),
+          rev_list(args.rev_list), tail(args.tail) {
         idx = w;
         vid = idx + maxn;
         buf = vid + maxn;
@@ -203,6 +222,149 @@ struct Warp {
         CF = d.conf;
         n = d.n;
         local = d.local;
+        ps = d.ps;
+        rev_off = d.rev_off;
+        rev_list = d.rev_list;
+        tail = d.tail;
+    }
+
+    __device__ __forceinline__ bool closed_at(uint32_t d) const {
+        return MODE == ASDM_MODE_COUNT && tail != kTailNone && d + 2 == n;
+    }
+
+    // |a ∩ b| of two ascending lists, warp-wide: each lane looks up entries
+    // of the shorter list in the longer one.
+    __device__ uint32_t isect_count(const uint32_t *x, uint32_t nx, const uint32_t *y, uint32_t ny) const {
+        const bool xs = nx <= ny;
+        const uint32_t *sl = xs ? x : y, *tl = xs ? y : x;
+        const uint32_t ns = xs ? nx : ny, nt = xs ? ny : nx;
+        uint32_t hits = 0;
+        for (uint32_t i = lane; i < ns; i += 32) {
+            const uint32_t v = sl[i];
+            const uint32_t q = lower_bound_u32(tl, nt, v);
+            hits += q < nt && tl[q] == v;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) hits += __shfl_xor_sync(kFull, hits, o);
+        return hits;
+    }
+
+    // The same for lists of candidate indices into two candidate sets of one
+    // label, compared by vertex id (cx[x[i]] against cy[y[j]]; both ascend).
+    __device__ uint32_t isect_count_vid(const uint32_t *x, uint32_t nx, const uint32_t *cx, const uint32_t *y,
+                                        uint32_t ny, const uint32_t *cy) const {
+        const bool xs = nx <= ny;
+        const uint32_t *sl = xs ? x : y, *tl = xs ? y : x, *cs = xs ? cx : cy, *ct = xs ? cy : cx;
+        const uint32_t ns = xs ? nx : ny, nt = xs ? ny : nx;
+        uint32_t hits = 0;
+        for (uint32_t i = lane; i < ns; i += 32) {
+            const uint32_t v = cs[sl[i]];
+            uint32_t lo = 0, hi = nt;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (ct[tl[mid]] < v) lo = mid + 1; else hi = mid;
+            }
+            hits += lo < nt && ct[tl[lo]] == v;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) hits += __shfl_xor_sync(kFull, hits, o);
+        return hits;
+    }
+
+    // The last two levels in closed form for driver positions [lo, hi) of
+    // level d = n-2 (prefix fixed down to level d-1; last-level conflict
+    // indices prepared in fidx).  Entries x of the driver range D that are
+    // conflicts at level d are taken out with their whole contribution.
+    //   kTailChain: sum over x in D of |list(x)| (prefix sums), minus, per
+    //     last-level conflict vertex y, the x in D adjacent to y (D intersected
+    //     with y's reverse candidate-edge list);
+    //   kTailLeaf: the last level's list LL is fixed: |D'| x (|LL| minus the
+    //     conflict vertices in LL), minus the x whose own vertex is in LL when
+    //     level d is itself a conflict of the last level.
+    __device__ void tail2(uint32_t d, uint32_t lo, uint32_t hi) {
+        const DLevel lv = L[d];
+        const uint32_t dslot = lv.back_first;
+        const uint32_t s0 = sstart[dslot];
+        const uint32_t *D = B[dslot].list + s0 + lo;
+        const uint32_t nd = hi - lo;
+        const DLevel lvL = L[n - 1];
+        const DBack bL = B[lvL.back_first];
+        // this lane's level-d conflict vertex, when it is an entry of D
+        uint32_t xc = kNone;
+        if (lane < lv.nconf) {
+            const uint32_t v = vid[CF[lv.conf_first + lane]];
+            const uint32_t y = lower_bound_u32(lv.cand, lv.ncand, v);
+            if (y < lv.ncand && lv.cand[y] == v) {
+                const uint32_t p = lower_bound_u32(D, nd, y);
+                if (p < nd && D[p] == y) xc = y;
+            }
+        }
+        unsigned long long sum = 0, touched = 2;
+        if (tail == kTailChain) {
+            sum = ps[s0 + hi] - ps[s0 + lo];
+            touched += 2;
+            for (uint32_t k = 0; k < lvL.nconf; ++k) {
+                const uint32_t y = fidx[k];
+                if (y >= kSelf) continue;  // not a candidate there (level d is adjacent, never itself)
+                const uint32_t r0 = rev_off[y], r1 = rev_off[y + 1];
+                sum -= isect_count(D, nd, rev_list + r0, r1 - r0);
+                touched += 2 + min(nd, r1 - r0);
+            }
+            unsigned long long back = 0;
+            if (xc != kNone) {
+                const uint32_t a0 = bL.off[xc], a1 = bL.off[xc + 1];
+                back = a1 - a0;
+                for (uint32_t k = 0; k < lvL.nconf; ++k) {
+                    const uint32_t y = fidx[k];
+                    if (y >= kSelf) continue;
+                    const uint32_t q = lower_bound_u32(bL.list + a0, a1 - a0, y);
+                    back -= (q < a1 - a0 && bL.list[a0 + q] == y) ? 1ull : 0ull;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) back += __shfl_xor_sync(kFull, back, o);
+            sum -= back;
+        } else {
+            const uint32_t ij = idx[bL.level];
+            const uint32_t a0 = bL.off[ij], a1 = bL.off[ij + 1];
+            const uint32_t *LL = bL.list + a0;
+            const uint32_t nl = a1 - a0;
+            uint32_t m = 0;
+            bool self = false;
+            if (lane < lvL.nconf) {
+                const uint32_t y = fidx[lane];
+                if (y == kSelf) {
+                    self = true;
+                } else if (y != kNone) {
+                    const uint32_t q = lower_bound_u32(LL, nl, y);
+                    m = q < nl && LL[q] == y;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(kFull, m, o);
+            self = __any_sync(kFull, self);
+            const uint32_t nexcl = __popc(__ballot_sync(kFull, xc != kNone));
+            sum = (unsigned long long)(nd - nexcl) * (unsigned long long)(nl - m);
+            if (self) {
+                // x whose own vertex lies in LL (excluded x not counted)
+                uint32_t hits = isect_count_vid(D, nd, lv.cand, LL, nl, lvL.cand);
+                bool xin = false;
+                if (xc != kNone) {
+                    const uint32_t v = lv.cand[xc];
+                    uint32_t l2 = 0, h2 = nl;
+                    while (l2 < h2) {
+                        const uint32_t mid = (l2 + h2) >> 1;
+                        if (lvL.cand[LL[mid]] < v) l2 = mid + 1; else h2 = mid;
+                    }
+                    xin = l2 < nl && lvL.cand[LL[l2]] == v;
+                }
+                hits -= __popc(__ballot_sync(kFull, xin));
+                sum -= hits;
+                touched += min(nd, nl);
+            }
+        }
+        add_count(sum);
+        elems += touched;
     }
 
     __device__ __forceinline__ bool lane_leaf_ok() const {
@@ -251,7 +413,8 @@ struct Warp {
             }
         }
         if (m > 1 && best > a.lane_leaf_max) return false;
-        touched += tot;
+        // a single list is not read: its length (two offsets) is the count
+        touched += m == 1 ? 2 : tot;
         unsigned long long c = 0;
         if (m == 1) {
             c = len[0];
@@ -336,7 +499,7 @@ struct Warp {
 
     // Loads the candidate-edge lists of level d's earlier neighbours into the
     // level's slots and picks the shortest as driver.  Returns its length.
-    __device__ uint32_t setup(uint32_t d) {
+    __device__ uint32_t setup(uint32_t d, bool whole = true) {
         const DLevel lv = L[d];
         uint32_t s_len = 0xFFFFFFFFu;
         if (lane < lv.nback) {
@@ -357,7 +520,9 @@ struct Warp {
         uint32_t tot = lane < lv.nback ? s_len : 0;
 #pragma unroll
         for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(kFull, tot, o);
-        elems += tot;
+        // a counted last level with one list reads only its two offsets; a
+        // level searched over part of its driver list is counted by the caller
+        if (whole) elems += (MODE == ASDM_MODE_COUNT && d + 1 == n && lv.nback == 1) ? 2 : tot;
         inter += lv.nback >= 2;
         if (lane == 0) {
             drv[d] = who;
@@ -645,8 +810,15 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
             }
             __syncwarp();
             ++d;
-            const uint32_t len = W.setup(d);
-            if (d == n - 1) {
+            const bool closed = W.closed_at(d);
+            const uint32_t len = W.setup(d, !closed);
+            if (closed) {
+                if (len) {
+                    W.prepare_lane_leaf(d);
+                    W.tail2(d, 0, len);
+                }
+                --d;
+            } else if (d == n - 1) {
                 if (len) W.leaf(d);
                 --d;
             } else if (len == 0) {
@@ -670,7 +842,22 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
 template <uint32_t MODE, bool MULTI>
 __device__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint32_t s, uint32_t lo, uint32_t hi,
                           uint32_t &iter, uint64_t deadline) {
-    W.setup(s);
+    if (W.closed_at(s)) {
+        W.setup(s, false);
+        if (hi > lo) {
+            W.prepare_lane_leaf(s);
+            W.tail2(s, lo, hi);
+        }
+        return true;
+    }
+    W.setup(s, false);
+    {
+        // list entries this range touches: the driver positions [lo, hi), one
+        // probe of every other list per driver entry, and the lists' offsets
+        const DLevel lv = W.L[s];
+        const bool by_length = MODE == ASDM_MODE_COUNT && s + 1 == W.n && lv.nback == 1;
+        W.elems += 2ull * lv.nback + (by_length ? 0ull : (unsigned long long)(hi - lo) * lv.nback);
+    }
     if (lane == 0) {
         W.dpos[s] = lo;
         W.dend[s] = hi;
@@ -809,7 +996,34 @@ __global__ void __launch_bounds__(kThreads, MINB) enum_batch_kernel(EnumArgs a) 
     const QDesc d0 = a.qd[0];
     Warp<MODE, true> W(a, d0.lv, d0.bk, d0.conf, wmem, lane, d0.n, a.maxn, a.maxnb);
     W.local = d0.local;
+    W.ps = d0.ps;
+    W.rev_off = d0.rev_off;
+    W.rev_list = d0.rev_list;
+    W.tail = d0.tail;
     warp_loop<MODE, true>(a, W, lane);
+}
+
+// Prefix sums for kTailChain plans: entry t of a segment (one plan's driver
+// edge of level n-2, in candidate-edge order) gets the length of the last
+// level's list of that entry; a scan over all segments follows.
+struct TailSeg {
+    const uint32_t *list;   // candidate-edge entries of level n-2's driver edge
+    const uint32_t *off2;   // offsets of the last level's lists, by candidate of level n-2
+    unsigned long long start, len;
+};
+
+__global__ void tail_lens(const TailSeg *__restrict__ seg, uint32_t nseg, unsigned long long total,
+                          uint32_t *__restrict__ lens) {
+    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nseg;  // the last segment starting at or before t
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (seg[mid].start <= t) lo = mid; else hi = mid;
+        }
+        const uint32_t x = seg[lo].list[t - seg[lo].start];
+        lens[t] = seg[lo].off2[x + 1] - seg[lo].off2[x];
+    }
 }
 
 __global__ void queue_init(unsigned long long *seq) {
@@ -833,6 +1047,91 @@ int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
 }
 
 }  // namespace
+
+// Closed form of the last two levels for a COUNT-mode plan (kTail*).
+uint32_t tail_mode(const asdm_plan &plan) {
+    const size_t n = plan.order.size();
+    if (n < 3 || plan.back[n - 2].size() != 1 || plan.back[n - 1].size() != 1) return kTailNone;
+    return plan.back[n - 1][0].first == n - 2 ? kTailChain : kTailLeaf;
+}
+
+// Tail data of every plan whose mode is given in `mode` (kTailChain plans get
+// prefix sums in one device array, *d_ps, which the caller frees; plans past
+// kTailSumCap entries fall back to kTailNone).
+constexpr unsigned long long kTailSumCap = 1ull << 29;
+struct TailData {
+    uint32_t mode = kTailNone;
+    const unsigned long long *ps = nullptr;
+    const uint32_t *rev_off = nullptr, *rev_list = nullptr;
+};
+int build_tails(const std::vector<const asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                std::vector<TailData> &out, unsigned long long **d_ps, cudaStream_t s) {
+    *d_ps = nullptr;
+    out.assign(cs.size(), TailData{});
+    std::vector<TailSeg> segs;
+    std::vector<size_t> seg_of;
+    unsigned long long total = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+        const asdm_cs &c = *cs[i];
+        const asdm_plan &p = *plans[i];
+        const uint32_t m = tail_mode(p);
+        if (m == kTailNone) continue;
+        const size_t n = p.order.size();
+        if (m == kTailLeaf) {
+            out[i].mode = m;
+            continue;
+        }
+        const uint32_t e1 = p.back[n - 2][0].second, e2 = p.back[n - 1][0].second;
+        const uint32_t ua = p.order[n - 2], ub = p.order[n - 1];
+        const int k = c.q.slot(ub, ua);
+        if (k < 0) continue;
+        const uint32_t er = c.q.off[ub] + (uint32_t)k;
+        const unsigned long long len = c.etotal[e1];
+        if (total + len > kTailSumCap) continue;  // element path for this plan
+        segs.push_back(TailSeg{c.d_elist + c.elist_base[e1], c.d_eoff + c.eoff_base[e2], total, len});
+        seg_of.push_back(i);
+        out[i].mode = m;
+        out[i].rev_off = c.d_eoff + c.eoff_base[er];
+        out[i].rev_list = c.d_elist + c.elist_base[er];
+        total += len;
+    }
+    if (segs.empty()) return ASDM_OK;
+    TailSeg *d_seg = nullptr;
+    uint32_t *d_lens = nullptr;
+    int rc = ASDM_OK;
+    do {
+        if ((rc = dalloc(d_ps, total + 1, s))) break;
+        if ((rc = dalloc(&d_seg, segs.size(), s))) break;
+        if ((rc = dalloc(&d_lens, std::max<unsigned long long>(total, 1), s))) break;
+        if (cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(TailSeg), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "tail segment upload failed");
+            break;
+        }
+        if (total) {
+            const unsigned grid = (unsigned)std::min<unsigned long long>((total + 255) / 256, 148ull * 32);
+            tail_lens<<<grid, 256, 0, s>>>(d_seg, (uint32_t)segs.size(), total, d_lens);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "tail length kernel failed");
+                break;
+            }
+        }
+        rc = scan_exclusive_u32(d_lens, reinterpret_cast<uint64_t *>(*d_ps), total, true, s);
+    } while (false);
+    // the copy above reads a host vector: wait before it goes out of scope
+    cudaStreamSynchronize(s);
+    dfree(d_lens, s);
+    dfree(d_seg, s);
+    if (rc != ASDM_OK) {
+        dfree(*d_ps, s);
+        *d_ps = nullptr;
+        for (auto &t : out) t = TailData{};
+        return rc;
+    }
+    for (size_t k = 0; k < segs.size(); ++k) out[seg_of[k]].ps = *d_ps + segs[k].start;
+    return ASDM_OK;
+}
 
 // Root tasks: blocks of consecutive (level-0, level-1) candidate pairs, about
 // 64K pairs per block count, between 1 and 256 pairs per block.
@@ -883,10 +1182,11 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     std::memcpy(hp.data() + n * sizeof(DLevel), bk.data(), nb * sizeof(DBack));
     std::memcpy(hp.data() + n * sizeof(DLevel) + nb * sizeof(DBack), cf.data(), nc * sizeof(uint32_t));
     uint8_t *d_plan = nullptr;
-    unsigned long long *d_ctr = nullptr, *d_local = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_local = nullptr, *d_ps = nullptr;
     uint32_t *d_rows = nullptr, *d_queue = nullptr;
     int rc = ASDM_OK;
     auto cleanup = [&]() {
+        dfree(d_ps, s);
         dfree(d_plan, s);
         dfree(d_ctr, s);
         dfree(d_local, s);
@@ -941,6 +1241,14 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         a.limit_ns = opt.time_limit_s > 0 ? (uint64_t)(opt.time_limit_s * 1e9) : 0;
         a.count_limit = opt.count_limit;
         a.lane_leaf_max = G->tuning.lane_leaf_max;
+        if (mode == ASDM_MODE_COUNT) {
+            std::vector<TailData> td;
+            if ((rc = build_tails({&cs}, {&plan}, td, &d_ps, s))) break;
+            a.tail = td[0].mode;
+            a.ps = td[0].ps;
+            a.rev_off = td[0].rev_off;
+            a.rev_list = td[0].rev_list;
+        }
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -1084,7 +1392,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     const uint64_t qd_at = append(nullptr, L * sizeof(QDesc));
     const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
     uint8_t *d_buf = nullptr;
-    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr;
     uint32_t *d_queue = nullptr;
     unsigned int *d_qflags = nullptr;
     int rc = ASDM_OK;
@@ -1105,6 +1413,22 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         if ((rc = dalloc(&d_buf, hp.size(), s)) || (rc = dalloc(&d_ctr, kCtrN, s)) || (rc = dalloc(&d_qcounts, L, s)) ||
             (rc = dalloc(&d_qflags, L, s)) || (rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s)))
             break;
+        if (!local_mode) {
+            std::vector<const asdm_cs *> tcs(L);
+            std::vector<const asdm_plan *> tpl(L);
+            for (uint32_t li = 0; li < L; ++li) {
+                tcs[li] = cs[live[li]];
+                tpl[li] = plans[live[li]];
+            }
+            std::vector<TailData> td;
+            if ((rc = build_tails(tcs, tpl, td, &d_ps, s))) break;
+            for (uint32_t li = 0; li < L; ++li) {
+                qd[li].tail = td[li].mode;
+                qd[li].ps = td[li].ps;
+                qd[li].rev_off = td[li].rev_off;
+                qd[li].rev_list = td[li].rev_list;
+            }
+        }
         for (uint32_t li = 0; li < L; ++li) {
             qd[li].lv = reinterpret_cast<const DLevel *>(d_buf + offs[li].lv);
             qd[li].bk = reinterpret_cast<const DBack *>(d_buf + offs[li].bk);
@@ -1214,6 +1538,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     } while (false);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
+    dfree(d_ps, s);
     dfree(d_buf, s);
     dfree(d_ctr, s);
     dfree(d_qcounts, s);

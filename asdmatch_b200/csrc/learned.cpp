@@ -133,11 +133,12 @@ int predict(asdm_estimator *e, const std::vector<const asdm_cs *> &qs, const std
 
 }  // namespace
 
+namespace {
+
 // Greedy order search for every start of every query, in lockstep; learned
 // estimates for prefixes of 3..kmax vertices.
-int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
-                       std::vector<asdm_plan> &plans) {
-    if (kmax == 0) kmax = 6;
+int greedy_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
+                         std::vector<asdm_plan> &plans) {
     struct Search {
         uint32_t query;
         GreedyState st;
@@ -207,6 +208,71 @@ int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uin
         if (!pick[i]) continue;  // not connected: the plan stays empty
         ASDM_TRY(build_plan(*css[i], pick[i]->st.order.data(), plans[i]));
         plans[i].cost = best[i];
+    }
+    return ASDM_OK;
+}
+
+}  // namespace
+
+// Learned plans for a group of queries: the exhaustive prefix search where a
+// query is small enough (every connected subset of 3..kmax vertices
+// estimated in one forward pass for the whole group), the lockstep greedy
+// search for the rest.
+int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
+                       std::vector<asdm_plan> &plans) {
+    if (kmax == 0) kmax = 6;
+    plans.assign(css.size(), asdm_plan{});
+    std::vector<uint32_t> dp_ids;
+    std::vector<asdm_cs *> rest;
+    std::vector<uint32_t> rest_ids;
+    std::vector<const asdm_cs *> rq;
+    std::vector<uint64_t> rm;
+    std::vector<std::pair<size_t, size_t>> range(css.size(), {0, 0});  // requests of query i
+    std::vector<uint64_t> subsets;
+    for (uint32_t i = 0; i < css.size(); ++i) {
+        const asdm_cs &cs = *css[i];
+        if (!cs.nonempty) continue;
+        const bool dp = cs.g->tuning.planner == ASDM_PLANNER_DP && cs.q.n <= kDpMaxVertices &&
+                        connected_subsets(cs.q, cs.q.n, kDpMaxSubsets, subsets);
+        if (!dp) {
+            rest.push_back(css[i]);
+            rest_ids.push_back(i);
+            continue;
+        }
+        dp_ids.push_back(i);
+        range[i].first = rm.size();
+        for (uint64_t S : subsets) {
+            const uint32_t k = (uint32_t)__builtin_popcountll(S);
+            if (k >= 3 && k <= kmax) {
+                rq.push_back(&cs);
+                rm.push_back(S);
+            }
+        }
+        range[i].second = rm.size();
+    }
+    std::vector<double> est;
+    if (!rm.empty()) ASDM_TRY(predict(e, rq, rm, est));
+    for (uint32_t i : dp_ids) {
+        std::unordered_map<uint64_t, double> known;
+        for (size_t r = range[i].first; r < range[i].second; ++r) known.emplace(rm[r], est[r]);
+        std::vector<uint32_t> order;
+        double cost = 0;
+        const bool ok = plan_dp(*css[i], [&](uint64_t S, double &c) {
+            auto it = known.find(S);
+            if (it == known.end()) return false;
+            c = it->second;
+            return true;
+        }, order, cost);
+        if (!ok) {  // not connected: the plan stays empty
+            continue;
+        }
+        ASDM_TRY(build_plan(*css[i], order.data(), plans[i]));
+        plans[i].cost = cost;
+    }
+    if (!rest.empty()) {
+        std::vector<asdm_plan> rp;
+        ASDM_TRY(greedy_batch_learned(rest, e, kmax, rp));
+        for (size_t k = 0; k < rest.size(); ++k) plans[rest_ids[k]] = std::move(rp[k]);
     }
     return ASDM_OK;
 }

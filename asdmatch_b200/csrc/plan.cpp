@@ -13,7 +13,10 @@
 // estimated work (partial matches expanded + 32-wide list chunks scanned).
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <memory>
+#include <unordered_map>
+#include <unordered_set>
 
 #include "cs.cuh"
 
@@ -112,6 +115,132 @@ void greedy_from(const asdm_cs &cs, const asdm_card *card, uint32_t start, std::
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Exhaustive order search over connected prefixes (dynamic programming over
+// vertex subsets, as the reference's optimalPlanDP does over bag subsets,
+// plan/subset_structure.cpp:146-233).  The cost of appending u to a prefix P
+// (|P| = l levels, N(P) partial matches, B backward edges whose shortest
+// average candidate list holds `drv` entries) follows what the enumeration
+// kernel does per partial match of P:
+//   inner level:  N(P) * (kOpen + drv * (1 + (B - 1) * kProbe))
+//   last level:   N(P) * kLeafOne               when B == 1 (the list length is the count)
+//                 N(P) * (kOpen + drv * (1 + (B - 1) * kProbe))   otherwise
+// N(S) is exact for one and two vertices (|C(u)|, the candidate-edge total),
+// the caller's figure where it has one (a .card entry, a learned estimate),
+// else the smallest over last vertices u of N(S - u) times the greedy's
+// extension factor.
+namespace {
+constexpr double kOpen = 4.0;     // opening a level for one partial match (list offsets, driver choice)
+constexpr double kProbe = 2.0;    // galloping into one more list, per driver entry
+constexpr double kLeafOne = 1.0;  // a one-list last level
+}  // namespace
+
+bool connected_subsets(const QueryGraph &q, uint32_t max_size, size_t limit, std::vector<uint64_t> &out) {
+    std::vector<uint64_t> nb(q.n, 0);
+    for (uint32_t u = 0; u < q.n; ++u)
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) nb[u] |= 1ull << q.nbr[e];
+    out.clear();
+    std::vector<uint64_t> level;
+    for (uint32_t u = 0; u < q.n; ++u) level.push_back(1ull << u);
+    for (uint32_t k = 1; !level.empty(); ++k) {
+        out.insert(out.end(), level.begin(), level.end());
+        if (out.size() > limit) return false;
+        if (k == max_size) break;
+        std::unordered_set<uint64_t> next;
+        for (uint64_t S : level) {
+            uint64_t ext = 0;
+            for (uint64_t r = S; r; r &= r - 1) ext |= nb[__builtin_ctzll(r)];
+            ext &= ~S;
+            for (; ext; ext &= ext - 1) {
+                next.insert(S | (ext & -ext));
+                if (out.size() + next.size() > limit) return false;
+            }
+        }
+        level.assign(next.begin(), next.end());
+        std::sort(level.begin(), level.end());
+    }
+    return true;
+}
+
+bool plan_dp(const asdm_cs &cs, const std::function<bool(uint64_t, double &)> &known, std::vector<uint32_t> &order,
+             double &cost) {
+    const QueryGraph &q = cs.q;
+    const uint32_t n = q.n;
+    if (n > kDpMaxVertices) return false;
+    std::vector<uint64_t> subsets;
+    if (!connected_subsets(q, n, kDpMaxSubsets, subsets)) return false;
+    const uint64_t full = n == 64 ? ~0ull : (1ull << n) - 1;
+    if (subsets.empty() || subsets.back() != full) return false;  // disconnected
+    std::vector<uint64_t> nb(n, 0);
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) nb[u] |= 1ull << q.nbr[e];
+    struct Entry { double N, f; int last; };
+    std::unordered_map<uint64_t, Entry> T;
+    T.reserve(subsets.size() * 2);
+    for (uint64_t S : subsets) {
+        const uint32_t k = (uint32_t)__builtin_popcountll(S);
+        Entry E{INFINITY, INFINITY, -1};
+        if (k == 1) {
+            E.N = (double)cs.ncand[__builtin_ctzll(S)];
+            E.f = 0.0;
+            E.last = (int)__builtin_ctzll(S);
+            double c;
+            if (known(S, c)) E.N = c;
+            T.emplace(S, E);
+            continue;
+        }
+        double derived = INFINITY;
+        for (uint64_t r = S; r; r &= r - 1) {
+            const uint32_t u = __builtin_ctzll(r);
+            const uint64_t P = S & ~(1ull << u);
+            if (!(nb[u] & P)) continue;
+            auto it = T.find(P);
+            if (it == T.end()) continue;  // P not connected
+            const Entry &EP = it->second;
+            // backward edges of u into P
+            double drv = INFINITY, lens[64];
+            uint32_t B = 0;
+            for (uint64_t b = nb[u] & P; b; b &= b - 1) {
+                const double a = avg_len(cs, __builtin_ctzll(b), u);
+                lens[B++] = a;
+                drv = std::min(drv, a);
+            }
+            double factor = drv;
+            bool skipped = false;
+            for (uint32_t i = 0; i < B; ++i) {
+                if (!skipped && lens[i] == drv) { skipped = true; continue; }
+                factor *= std::min(1.0, lens[i] / std::max(1.0, (double)cs.ncand[u]));
+            }
+            derived = std::min(derived, EP.N * factor);
+            const double step = (k == n && B == 1) ? EP.N * kLeafOne
+                                                   : EP.N * (kOpen + drv * (1.0 + (B - 1) * kProbe));
+            if (EP.f + step < E.f) {
+                E.f = EP.f + step;
+                E.last = (int)u;
+            }
+        }
+        if (k == 2) {
+            const uint32_t a = __builtin_ctzll(S), b = __builtin_ctzll(S & (S - 1));
+            E.N = (double)cs.etotal[q.off[a] + (uint32_t)q.slot(a, b)];
+        } else {
+            E.N = derived;
+        }
+        double c;
+        if (known(S, c)) E.N = c;
+        E.N = std::max(E.N, 1e-9);
+        T.emplace(S, E);
+    }
+    order.assign(n, 0);
+    uint64_t S = full;
+    for (uint32_t k = n; k > 0; --k) {
+        const Entry &E = T.at(S);
+        order[k - 1] = (uint32_t)E.last;
+        S &= ~(1ull << E.last);
+    }
+    cost = T.at(full).f;
+    return true;
+}
+
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card) {
     const QueryGraph &q = cs.q;
     const uint32_t n = q.n;
@@ -124,6 +253,12 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
             seen[p.order[k]] = 1;
         }
         p.cost = 0;
+    } else if (cs.g->tuning.planner == ASDM_PLANNER_DP &&
+               plan_dp(cs, [&](uint64_t S, double &c) {
+                   c = card_lookup_or(card, S, NAN);
+                   return !std::isnan(c);
+               }, p.order, p.cost)) {
+        // exhaustive search over connected prefixes
     } else {
         double best = INFINITY;
         for (uint32_t s = 0; s < n; ++s) {

@@ -383,6 +383,10 @@ def main():
     plain_ms, plain_agg = timed(plain_step, args.steps)
     learned = None
     if est is not None:
+        # the planner (exhaustive prefix search or greedy) for learned estimates, on the tuned kernel knobs
+        learned_tune, learned_table = A.autotune(
+            dg, packed, min_blocks=(tune_best["enum_min_blocks"],), lane_leaf=(tune_best["lane_leaf_max"],),
+            run=lambda d, b: A.run_batch_ex(d, b, estimator=est, learned_max_subset=args.learned_max))
         for _ in range(max(1, args.warmup // 2)):
             learned_step()
         learned_ms, learned_agg = timed(learned_step, args.steps)
@@ -393,9 +397,12 @@ def main():
                    "over_plain": plain_ms / learned_ms, "over_cost_model_batched": ms / learned_ms,
                    "estimator": os.path.relpath(est_path, ROOT) if est_path.startswith(ROOT) else est_path,
                    "learned_max_subset": args.learned_max or 6,
+                   "planner": "exhaustive prefix search" if learned_tune["planner"] == A.PLANNER_DP else "greedy",
+                   "planner_table": learned_table,
                    "what": "asdm_run_batch_ex with the learned estimator: candidate spaces, learned greedy plans "
                            "(one forward pass per planner step for the whole group), one persistent launch; "
                            "planning is inside the timed region"}
+        dg.set_tuning(tune_best["enum_min_blocks"], tune_best["lane_leaf_max"], tune_best["planner"])
     # end to end through the one-call C ABI (asdm_run_batch) from host buffers
     e2e_times = []
     h2d = packed.nbytes()
@@ -441,7 +448,8 @@ def main():
         "data": "synthetic (seeded generators; no dataset download)",
         "config": dict(cfg, l2="flushed (256 MB write) before every timed step",
                        form="batched: asdm_run_batch (one launch per CFL phase for the group, one persistent "
-                            "enumeration kernel over all (query, root task) pairs); planner: candidate-size cost model",
+                            "enumeration kernel over all (query, root task) pairs); planner: candidate-size cost model, "
+                            + ("exhaustive prefix search" if tune_best.get("planner", 0) == A.PLANNER_DP else "greedy"),
                        matches_per_step=agg["matches"] // steps,
                        matches_per_s=world * (agg["matches"] // steps) / (ms / 1e3),
                        intersections_per_step=agg["inter"] // steps,

@@ -112,7 +112,13 @@ int asdm_graph_free(asdm_graph *g);
 typedef struct asdm_tuning {
     uint32_t enum_min_blocks;
     uint32_t lane_leaf_max;
+    uint32_t planner;          /* ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY */
 } asdm_tuning;
+/* Order search: exhaustive over connected prefixes where the query is small
+ * enough (at most 24 vertices and 4096 connected vertex subsets), else
+ * greedy; or greedy always. */
+#define ASDM_PLANNER_DP 0
+#define ASDM_PLANNER_GREEDY 1
 int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t);
 int asdm_graph_get_tuning(const asdm_graph *g, asdm_tuning *t);
 

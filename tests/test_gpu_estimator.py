@@ -315,3 +315,37 @@ def test_batch_count_limit_statuses(golden, c0d_files, dg_c0d):
     b = A.BatchInput(qs)
     A.run_batch_ex(dg_c0d, b, cards=cards)
     assert b.counts.tolist() == [r["count"] for r in recs]
+
+
+def test_both_planners_give_the_golden_counts(golden, c0_files, c0d_files, dg_c0, dg_c0d, edge_files):
+    _, _, qs0, _ = c0_files
+    _, _, by_size = c0d_files
+    recs = golden["sets"]["c0d"]
+    qs = [by_size[r["size"]][0][r["index"]] for r in recs]
+    try:
+        for planner in (A.PLANNER_DP, A.PLANNER_GREEDY):
+            dg_c0d.set_tuning(1, 96, planner)
+            dg_c0.set_tuning(1, 96, planner)
+            assert dg_c0d.tuning()["planner"] == planner
+            counts, status = A.run_batch(dg_c0d, qs)
+            assert status.tolist() == [0] * len(qs)
+            assert counts.tolist() == [r["count"] for r in recs]
+            for r, q in list(zip(recs, qs))[::8]:
+                cs = A.CandidateSpace(dg_c0d, q)
+                p = A.Plan(cs)
+                o = p.order()
+                adj = E.query_adjacency(q)
+                assert sorted(o) == list(range(q.n))
+                assert all(any(w in adj[o[k]] for w in o[:k]) for k in range(1, q.n))
+                assert A.adaptive_share_join(cs, p).count == r["count"]
+                cs.close()
+            erecs = golden["sets"]["edge"]
+            counts, status = A.run_batch(dg_c0, [edge_files[r["name"]][0] for r in erecs])
+            assert counts.tolist() == [r["count"] for r in erecs]
+            counts, status = A.run_batch(dg_c0, qs0[:60])
+            assert counts.tolist() == [r["count"] for r in golden["sets"]["c0"][:60]]
+    finally:
+        dg_c0d.set_tuning(1, 96, A.PLANNER_DP)
+        dg_c0.set_tuning(1, 96, A.PLANNER_DP)
+    with pytest.raises(A.AsdmError):
+        dg_c0.set_tuning(1, 96, 7)
