@@ -1,22 +1,26 @@
 // K1-K3: the CFL candidate space on the device.
 //
 // Restates CandidateSpace::buildCandCFL (relation/candidate_space.cpp:550-721)
-// as the set computation it performs.  For every query vertex u a state word
-// per data vertex of u's label holds bit 31 = "passes the label, degree and
-// NLC filter" (K1, nlcValid at utility/utils.cpp:30-40) and bit b = "adjacent
-// to the storage of u's b-th query neighbour p" (K2).  The storage S(p) that
-// the reference scans for p is the top-down candidate set Ctd(p) plus data
-// vertex 0 whenever Ctd(p) is smaller than |V_l(p)|: candidateSet[p] is
-// resized to |V_l(p)| up front (:555-559), its zero-initialised tail is
-// iterated by the range-for loops (:588, :623, :661), and pruned entries stay
-// in it until the compaction at :692-703.  Hence
+// as the set computation it performs.  For every query vertex u, over the
+// data vertices of u's label (indexed by their rank inside the label), a
+// bitset F(u) holds "passes the label, degree and NLC filter" (K1, nlcValid
+// at utility/utils.cpp:30-40) and one bitset per query neighbour p of u holds
+// "adjacent to the storage of p" (K2).  The storage S(p) that the reference
+// scans for p is the top-down candidate set Ctd(p) plus data vertex 0
+// whenever Ctd(p) is smaller than |V_l(p)|: candidateSet[p] is resized to
+// |V_l(p)| up front (:555-559), its zero-initialised tail is iterated by the
+// range-for loops (:588, :623, :661), and pruned entries stay in it until the
+// compaction at :692-703.  Hence
 //     Ctd(root) = F(root),   Ctd(u) = F(u) ∩ ⋂_{p ∈ before(u)} N_l(u)(S(p)),
 //     C(u) = F(u) ∩ ⋂_{p ∈ N_q(u)} N_l(u)(S(p)),
 // computed wave by wave along the CFL BFS order (a vertex's wave is one more
-// than the latest wave among its earlier neighbours).  The marking is an
-// atomicOr of bit b, so the order of the scans inside a wave does not matter.
-// K3 compacts each C(u) in id order and builds the candidate edges
-// (buildCandidateEdge(false), :458-487) as CSR lists of indices into C(u2).
+// than the latest wave among its earlier neighbours).  Marking is an atomic
+// OR into a bitset, so the order of the scans inside a wave does not matter.
+// Compaction ANDs the required bitsets word by word and writes the surviving
+// vertices in id order.  K3 builds the candidate edges
+// (buildCandidateEdge(false), :458-487) as CSR lists of indices into C(u2),
+// looking a neighbour's index up in C(u2)'s membership bitset and per-word
+// prefix counts.
 #include <algorithm>
 #include <memory>
 #include <queue>
@@ -26,7 +30,6 @@
 namespace asdm {
 namespace {
 
-constexpr uint32_t kFBit = 0x80000000u;
 constexpr int kBlock = 256;
 constexpr uint32_t kLongRun = 32;
 
@@ -41,12 +44,16 @@ __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ pr
 }
 
 // ---- K1: label + degree + NLC filter --------------------------------------
-// One segment per (query, query vertex) of a batch.
+// One segment per (query, query vertex) of a group; a segment's items are
+// the ranks 0 .. |V_l(u)| - 1 of u's label, padded to a multiple of 32 so
+// that a warp's 32 items are one word of F(u).
 struct FilterArgs {
     DevGraph g;
-    uint32_t *st;
-    const uint64_t *seg;      // nseg + 1 prefix of |V_l(u)|
+    uint32_t *bits;           // bitsets of the group
+    const uint64_t *seg;      // nseg + 1 prefix of the padded item counts
+    const uint64_t *fword;    // word offset of F(u) in bits
     const uint32_t *lbase;    // vbl_off[l(u)]
+    const uint32_t *llen;     // |V_l(u)|
     const uint32_t *qdeg;     // deg(u)
     const uint32_t *qnlc;     // (label, count) pairs
     const uint32_t *qnlc_off; // nseg + 1
@@ -55,44 +62,46 @@ struct FilterArgs {
 };
 
 __global__ void __launch_bounds__(kBlock) k1_filter(FilterArgs a) {
-    const uint64_t *seg = a.seg;
-    const uint64_t total = seg[a.nq];
+    const uint64_t total = a.seg[a.nq];
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
-        const uint64_t item = base + lane;
+        const uint32_t u = find_segment(a.seg, a.nq, base);
+        const uint32_t i = (uint32_t)(base - a.seg[u]) + lane;
         bool pass = false;
-        uint32_t u = 0xFFFFFFFFu;
-        if (item < total) {
-            u = find_segment(seg, a.nq, item);
-            const uint32_t i = (uint32_t)(item - seg[u]);
-            const uint32_t v = a.g.vbl[a.lbase[u] + i];
-            pass = (a.g.off[v + 1] - a.g.off[v]) >= a.qdeg[u];
+        if (i < a.llen[u]) {
+            // degree and neighbour-label mask of the vertex, in label order
+            const uint2 info = a.g.rank_info[a.lbase[u] + i];
+            pass = info.x >= a.qdeg[u];
             for (uint32_t k = a.qnlc_off[u]; pass && k < a.qnlc_off[u + 1]; ++k) {
-                uint32_t b, e;
-                label_run(a.g, v, a.qnlc[2 * k], b, e);
-                pass = (e - b) >= a.qnlc[2 * k + 1];
+                const uint32_t l = a.qnlc[2 * k], c = a.qnlc[2 * k + 1];
+                pass = l < a.g.nlabels && ((info.y >> (l & 31u)) & 1u);
+                if (pass && (c > 1 || a.g.nlabels > 32)) {
+                    uint32_t b, e;
+                    label_run(a.g, a.g.vbl[a.lbase[u] + i], l, b, e);
+                    pass = (e - b) >= c;
+                }
             }
-            a.st[item] = pass ? kFBit : 0u;
         }
-        const uint32_t key = pass ? u : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        if (pass && (__ffs(peers) - 1) == (int)lane) atomicAdd(&a.fcount[u], (uint32_t)__popc(peers));
+        const uint32_t word = __ballot_sync(0xffffffffu, pass);
+        if (lane == 0) {
+            a.bits[a.fword[u] + (base - a.seg[u]) / 32] = word;
+            if (word) atomicAdd(&a.fcount[u], (uint32_t)__popc(word));
+        }
     }
 }
 
 // ---- K2: neighbour marking passes -------------------------------------------
 struct PassDesc {
     const uint32_t *src;  // storage S(p): vertex ids
-    uint32_t *st;         // state words of u (indexed by rank inside l(u))
+    uint32_t *mbits;      // u's bitset for p
     uint32_t label;       // l(u)
-    uint32_t mask;        // bit of p among u's query neighbours
+    uint32_t pad;
 };
 
-__device__ __forceinline__ void mark(const DevGraph &g, uint32_t *st, uint32_t k, uint32_t mask) {
-    const uint32_t i = g.pos_in_label[g.nbr[k]];
-    const uint32_t s = st[i];
-    if ((s & kFBit) && !(s & mask)) atomicOr(&st[i], mask);
+__device__ __forceinline__ void mark(const DevGraph &g, uint32_t *mb, uint32_t k) {
+    const uint32_t r = g.nbr_rank[k];
+    atomicOr(&mb[r >> 5], 1u << (r & 31u));  // result unused: a fire-and-forget reduction
 }
 
 __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__restrict__ passes,
@@ -104,15 +113,14 @@ __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__
     uint64_t scanned = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint64_t item = base + lane;
-        uint32_t b = 0, e = 0, mask = 0;
-        uint32_t *st = nullptr;
+        uint32_t b = 0, e = 0;
+        uint32_t *mb = nullptr;
         if (item < total) {
             const uint32_t p = find_segment(prefix, npass, item);
             const PassDesc d = passes[p];
             const uint32_t w = d.src[item - prefix[p]];
             label_run(g, w, d.label, b, e);
-            st = d.st;
-            mask = d.mask;
+            mb = d.mbits;
         }
         scanned += e - b;
         const bool coop = (e - b) > kLongRun;
@@ -121,40 +129,48 @@ __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
             const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            const uint32_t mm = __shfl_sync(0xffffffffu, mask, src);
-            uint32_t *ss = (uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)st, src);
-            for (uint32_t k = bb + lane; k < ee; k += 32) mark(g, ss, k, mm);
+            uint32_t *mm = (uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)mb, src);
+            for (uint32_t k = bb + lane; k < ee; k += 32) mark(g, mm, k);
         }
         if (!coop)
-            for (uint32_t k = b; k < e; ++k) mark(g, st, k, mask);
+            for (uint32_t k = b; k < e; ++k) mark(g, mb, k);
     }
     for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
     if (lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
 }
 
-// ---- K3a: order-preserving compaction of state words into vertex lists ----
-constexpr int kItems = 8;
-constexpr int kTile = kBlock * kItems;
+// ---- K3a: compaction of bitsets into vertex lists, word by word ------------
+constexpr int kItems = 8;               // words per thread
+constexpr int kTile = kBlock * kItems;  // words per tile
 
 struct CompDesc {
-    const uint32_t *st;
-    uint32_t *out;        // vertex ids, capacity len
-    uint32_t len;         // |V_l(u)|
-    uint32_t need;        // required bits
-    uint32_t lbase;       // vbl_off[l(u)]
-    uint32_t phantom;     // append data vertex 0 when fewer than len survive
+    const uint32_t *bits;   // F(u); the bitset of u's query-neighbour slot b at bits + (1 + b) * words
+    uint32_t words;         // ceil(|V_l(u)| / 32)
+    uint32_t need;          // slots whose bitsets are required
+    uint32_t len;           // |V_l(u)|
+    uint32_t lbase;         // vbl_off[l(u)]
+    uint32_t phantom;       // append data vertex 0 when fewer than len survive
+    uint32_t pad;
+    uint32_t *cbits;        // or null: membership bitset of the result
+    uint32_t *cpre;         //          and the result's size before each word
 };
+
+__device__ __forceinline__ uint32_t comp_word(const CompDesc &d, uint32_t w) {
+    uint32_t x = d.bits[w];
+    for (uint32_t m = d.need; m && x; m &= m - 1) x &= d.bits[(uint64_t)__ffs(m) * d.words + w];
+    return x;
+}
 
 __global__ void __launch_bounds__(kBlock) k3_count(const CompDesc *__restrict__ segs, const uint64_t *__restrict__ tile_first,
                                                    uint32_t nseg, uint32_t *__restrict__ tile_cnt) {
     const uint32_t t = blockIdx.x;
     const uint32_t sidx = find_segment(tile_first, nseg, t);
     const CompDesc d = segs[sidx];
-    const uint64_t first = (uint64_t)(t - tile_first[sidx]) * kTile;
+    const uint32_t first = (uint32_t)(t - tile_first[sidx]) * kTile;
     uint32_t c = 0;
-    for (uint32_t k = threadIdx.x; k < kTile; k += kBlock) {
-        const uint64_t i = first + k;
-        if (i < d.len && (d.st[i] & d.need) == d.need) ++c;
+    for (uint32_t k = threadIdx.x; k < (uint32_t)kTile; k += kBlock) {
+        const uint32_t w = first + k;
+        if (w < d.words) c += __popc(comp_word(d, w));
     }
     __shared__ uint32_t wsum[kBlock / 32];
     for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -167,29 +183,33 @@ __global__ void __launch_bounds__(kBlock) k3_count(const CompDesc *__restrict__ 
     }
 }
 
+// Segment sidx writes to out + tile_pos[tile_first[sidx]] + sidx (one spare
+// slot per segment for the phantom vertex).
 __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ segs, const uint64_t *__restrict__ tile_first,
                                                    uint32_t nseg, const uint64_t *__restrict__ tile_pos,
-                                                   const uint32_t *__restrict__ vbl, uint32_t *__restrict__ seg_count) {
+                                                   const uint32_t *__restrict__ vbl, uint32_t *__restrict__ out,
+                                                   uint32_t *__restrict__ seg_count) {
     const uint32_t t = blockIdx.x;
     const uint32_t sidx = find_segment(tile_first, nseg, t);
     const CompDesc d = segs[sidx];
-    const uint64_t first = (uint64_t)(t - tile_first[sidx]) * kTile;
-    const uint64_t my = first + (uint64_t)threadIdx.x * kItems;
-    uint32_t flags = 0, c = 0;
+    const uint32_t first = (uint32_t)(t - tile_first[sidx]) * kTile;
+    const uint32_t my = first + threadIdx.x * kItems;
+    uint32_t x[kItems];
+    uint32_t c = 0;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const uint64_t i = my + k;
-        if (i < d.len && (d.st[i] & d.need) == d.need) { flags |= 1u << k; ++c; }
+        x[k] = (my + k < d.words) ? comp_word(d, my + k) : 0u;
+        c += __popc(x[k]);
     }
     // block exclusive scan of c
     __shared__ uint32_t wsum[kBlock / 32];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = c;
+    uint32_t v = c;
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
+        uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
     }
-    if (lane == 31) wsum[warp] = x;
+    if (lane == 31) wsum[warp] = v;
     __syncthreads();
     if (warp == 0) {
         uint32_t w = lane < kBlock / 32 ? wsum[lane] : 0;
@@ -200,36 +220,40 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
         if (lane < kBlock / 32) wsum[lane] = w;
     }
     __syncthreads();
-    uint64_t pos = (tile_pos[t] - tile_pos[tile_first[sidx]]) + (warp ? wsum[warp - 1] : 0) + x - c;
+    const uint64_t seg_first = tile_pos[tile_first[sidx]];
+    uint32_t *o = out + seg_first + sidx;
+    uint32_t pos = (uint32_t)(tile_pos[t] - seg_first) + (warp ? wsum[warp - 1] : 0) + v - c;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k)
-        if (flags & (1u << k)) d.out[pos++] = vbl[d.lbase + (uint32_t)(my + k)];
+    for (int k = 0; k < kItems; ++k) {
+        const uint32_t w = my + k;
+        if (w >= d.words) break;
+        if (d.cbits) {
+            d.cbits[w] = x[k];
+            d.cpre[w] = pos;
+        }
+        for (uint32_t y = x[k]; y; y &= y - 1) o[pos++] = vbl[d.lbase + 32 * w + (uint32_t)(__ffs(y) - 1)];
+    }
     // the last tile of a segment records the segment size
     if (threadIdx.x == 0 && t + 1 == tile_first[sidx + 1]) {
-        uint32_t size = (uint32_t)(tile_pos[t + 1] - tile_pos[tile_first[sidx]]);
-        if (d.phantom && size < d.len) d.out[size++] = 0;  // the reference's zero-filled storage tail
+        uint32_t size = (uint32_t)(tile_pos[t + 1] - seg_first);
+        if (d.phantom && size < d.len) o[size++] = 0;  // the reference's zero-filled storage tail
         seg_count[sidx] = size;
     }
 }
 
 // ---- K3b: candidate edges ---------------------------------------------------
 struct EdgeDesc {
-    const uint32_t *cand_u;  // C(u)
-    const uint32_t *map_u2;  // rank in l(u2) -> index in C(u2) or kNone
+    const uint32_t *cand_u;   // C(u)
+    const uint32_t *cbits;    // membership of C(u2) by rank in l(u2)
+    const uint32_t *cpre;     // |C(u2)| before each word
     uint32_t ncand_u;
     uint32_t label_u2;
 };
 
-__global__ void __launch_bounds__(kBlock) k3_scatter_map(const uint32_t *const *__restrict__ cands,
-                                                         const uint64_t *__restrict__ cprefix, uint32_t nseg,
-                                                         uint32_t *const *__restrict__ maps,
-                                                         const uint32_t *__restrict__ pos_in_label) {
-    const uint64_t total = cprefix[nseg];
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t u = find_segment(cprefix, nseg, i);
-        const uint32_t j = (uint32_t)(i - cprefix[u]);
-        maps[u][pos_in_label[cands[u][j]]] = j;
-    }
+// Index in C(u2) of the vertex of rank r in l(u2), or kNone.
+__device__ __forceinline__ uint32_t cand_index(const uint32_t *cb, const uint32_t *cp, uint32_t r) {
+    const uint32_t w = cb[r >> 5], bit = 1u << (r & 31u);
+    return (w & bit) ? cp[r >> 5] + (uint32_t)__popc(w & (bit - 1u)) : kNone;
 }
 
 template <bool kFill>
@@ -244,13 +268,14 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint64_t item = base + lane;
         uint32_t b = 0, e = 0;
-        const uint32_t *map = nullptr;
+        const uint32_t *cb = nullptr, *cp = nullptr;
         if (item < total) {
             const uint32_t ei = find_segment(item_base, nedges, item);
             const EdgeDesc d = edges[ei];
             const uint32_t i = (uint32_t)(item - item_base[ei]);
             if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
-            map = d.map_u2;
+            cb = d.cbits;
+            cp = d.cpre;
         }
         scanned += e - b;
         const bool coop = (e - b) > kLongRun;
@@ -261,13 +286,13 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
             const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            const uint32_t *mm = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)map, src);
+            const uint32_t *mb = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)cb, src);
+            const uint32_t *mp = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)cp, src);
             uint64_t o = __shfl_sync(0xffffffffu, out, src);
             uint32_t c = 0;
             for (uint32_t k0 = bb; k0 < ee; k0 += 32) {
                 const uint32_t k = k0 + lane;
-                uint32_t idx = kNone;
-                if (k < ee) idx = mm[g.pos_in_label[g.nbr[k]]];
+                const uint32_t idx = k < ee ? cand_index(mb, mp, g.nbr_rank[k]) : kNone;
                 const uint32_t hit = __ballot_sync(0xffffffffu, idx != kNone);
                 if (kFill && idx != kNone) elist[o + __popc(hit & ((1u << lane) - 1))] = idx;
                 o += __popc(hit);
@@ -277,7 +302,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
         }
         if (!coop) {
             for (uint32_t k = b; k < e; ++k) {
-                const uint32_t idx = map[g.pos_in_label[g.nbr[k]]];
+                const uint32_t idx = cand_index(cb, cp, g.nbr_rank[k]);
                 if (idx != kNone) {
                     if (kFill) elist[out++] = idx;
                     ++mine;
@@ -309,38 +334,65 @@ unsigned grid_for(uint64_t items, int num_sms) {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)num_sms * 32));
 }
 
-// Runs one compaction over the given segments; returns per-segment sizes.
-int compact(asdm_graph *G, const std::vector<CompDesc> &segs, std::vector<uint32_t> &sizes) {
+// One compaction over the given segments into one new device buffer (*out,
+// the caller frees it): segment i's vertices at *out + start[i], size[i] of
+// them (plus, where asked, the phantom vertex).
+int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, std::vector<uint64_t> &start,
+            std::vector<uint32_t> &sizes) {
     cudaStream_t s = G->stream;
     const uint32_t nseg = (uint32_t)segs.size();
+    *out = nullptr;
     sizes.assign(nseg, 0);
+    start.assign(nseg, 0);
     if (nseg == 0) return ASDM_OK;
     std::vector<uint64_t> tile_first(nseg + 1, 0);
-    for (uint32_t i = 0; i < nseg; ++i) tile_first[i + 1] = tile_first[i] + (segs[i].len + kTile - 1) / kTile;
+    for (uint32_t i = 0; i < nseg; ++i) tile_first[i + 1] = tile_first[i] + (segs[i].words + kTile - 1) / kTile;
     const uint64_t ntiles = tile_first[nseg];
-    if (ntiles == 0) return ASDM_OK;
     CompDesc *d_segs = nullptr;
     uint64_t *d_tf = nullptr, *d_pos = nullptr;
     uint32_t *d_cnt = nullptr, *d_sc = nullptr;
-    ASDM_TRY(dalloc(&d_segs, nseg, s));
-    ASDM_TRY(dalloc(&d_tf, nseg + 1, s));
-    ASDM_TRY(dalloc(&d_cnt, ntiles, s));
-    ASDM_TRY(dalloc(&d_pos, ntiles + 1, s));
-    ASDM_TRY(dalloc(&d_sc, nseg, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_segs, segs.data(), nseg * sizeof(CompDesc), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_tf, tile_first.data(), (nseg + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemsetAsync(d_sc, 0, nseg * sizeof(uint32_t), s));
-    k3_count<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_cnt);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
-    ASDM_TRY(scan_exclusive_u32(d_cnt, d_pos, ntiles, true, s));
-    k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, d_sc);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
-    ASDM_CUDA(cudaMemcpyAsync(sizes.data(), d_sc, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    ASDM_CUDA(cudaStreamSynchronize(s));
+    int rc = ASDM_OK;
+    std::vector<uint64_t> pos(ntiles + 1, 0);
+    do {
+        if (ntiles == 0) {
+            if ((rc = dalloc(out, nseg, s))) break;
+            for (uint32_t i = 0; i < nseg; ++i) start[i] = i;
+            break;
+        }
+        if ((rc = dalloc(&d_segs, nseg, s)) || (rc = dalloc(&d_tf, nseg + 1, s)) || (rc = dalloc(&d_cnt, ntiles, s)) ||
+            (rc = dalloc(&d_pos, ntiles + 1, s)) || (rc = dalloc(&d_sc, nseg, s)))
+            break;
+        if (cudaMemcpyAsync(d_segs, segs.data(), nseg * sizeof(CompDesc), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(d_tf, tile_first.data(), (nseg + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemsetAsync(d_sc, 0, nseg * sizeof(uint32_t), s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "compaction upload failed");
+            break;
+        }
+        k3_count<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_cnt);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "compaction count failed"); break; }
+        if ((rc = scan_exclusive_u32(d_cnt, d_pos, ntiles, true, s))) break;
+        if (cudaMemcpyAsync(pos.data(), d_pos, (ntiles + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "compaction readback failed");
+            break;
+        }
+        if ((rc = dalloc(out, pos[ntiles] + nseg, s))) break;
+        k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, *out, d_sc);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "compaction write failed"); break; }
+        if (cudaMemcpyAsync(sizes.data(), d_sc, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "compaction size readback failed");
+            break;
+        }
+        for (uint32_t i = 0; i < nseg; ++i) start[i] = pos[tile_first[i]] + i;
+    } while (false);
     dfree(d_segs, s); dfree(d_tf, s); dfree(d_cnt, s); dfree(d_pos, s); dfree(d_sc, s);
-    return ASDM_OK;
+    if (rc != ASDM_OK) dfree(*out, s);
+    return rc;
 }
 
 int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::vector<uint64_t> &lens,
@@ -360,6 +412,8 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, d_elems);
     ::asdm::count_launch();
     ASDM_CUDA(cudaGetLastError());
+    // the host vectors above are read by the copies: wait before they go out of scope
+    ASDM_CUDA(cudaStreamSynchronize(s));
     dfree(d_p, s);
     dfree(d_prefix, s);
     return ASDM_OK;
@@ -376,6 +430,9 @@ struct Scratch {
         int rc = dalloc(p, n, s);
         if (rc == ASDM_OK) ptrs.push_back((void *)*p);
         return rc;
+    }
+    void keep(void *p) {
+        if (p) ptrs.push_back(p);
     }
     template <typename T>
     int upload(T **p, const std::vector<T> &h) {
@@ -427,15 +484,18 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             }
         }
     }
-    // segment tables
-    std::vector<uint64_t> seg(nseg + 1, 0);
-    std::vector<uint32_t> lbase(nseg), qdeg(nseg), qnlc, qnlc_off(nseg + 1, 0);
+    // segment tables: padded item ranges for K1, bitset layout [F | slot 0 | slot 1 | ...]
+    std::vector<uint64_t> seg(nseg + 1, 0), fword(nseg + 1, 0);
+    std::vector<uint32_t> lbase(nseg), llen(nseg), qdeg(nseg), words(nseg), qnlc, qnlc_off(nseg + 1, 0);
     for (const QPlan &qp : P) {
         const QueryGraph &q = qp.cs->q;
         for (uint32_t u = 0; u < q.n; ++u) {
             const uint32_t sg = qp.seg0 + u;
-            seg[sg + 1] = seg[sg] + qp.lsize[u];
+            words[sg] = (qp.lsize[u] + 31) / 32;
+            seg[sg + 1] = seg[sg] + 32ull * words[sg];
+            fword[sg + 1] = fword[sg] + (uint64_t)(q.deg(u) + 1) * words[sg];
             lbase[sg] = qp.lbase[u];
+            llen[sg] = qp.lsize[u];
             qdeg[sg] = q.deg(u);
             for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                 const uint32_t l = q.lab[q.nbr[e]];
@@ -445,13 +505,16 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             qnlc_off[sg + 1] = (uint32_t)(qnlc.size() / 2);
         }
     }
-    uint32_t *st = nullptr, *d_fcount = nullptr, *d_lbase = nullptr, *d_qdeg = nullptr, *d_qnlc = nullptr,
-             *d_qnlc_off = nullptr;
-    uint64_t *d_seg = nullptr;
+    uint32_t *bits = nullptr, *d_fcount = nullptr, *d_lbase = nullptr, *d_llen = nullptr, *d_qdeg = nullptr,
+             *d_qnlc = nullptr, *d_qnlc_off = nullptr;
+    uint64_t *d_seg = nullptr, *d_fword = nullptr;
     unsigned long long *d_elems = nullptr;
-    ASDM_TRY(scr.alloc(&st, seg[nseg]));
+    ASDM_TRY(scr.alloc(&bits, fword[nseg]));
+    ASDM_CUDA(cudaMemsetAsync(bits, 0, std::max<uint64_t>(fword[nseg], 1) * sizeof(uint32_t), s));
     ASDM_TRY(scr.upload(&d_seg, seg));
+    ASDM_TRY(scr.upload(&d_fword, fword));
     ASDM_TRY(scr.upload(&d_lbase, lbase));
+    ASDM_TRY(scr.upload(&d_llen, llen));
     ASDM_TRY(scr.upload(&d_qdeg, qdeg));
     if (qnlc.empty()) qnlc.push_back(0);
     ASDM_TRY(scr.upload(&d_qnlc, qnlc));
@@ -461,7 +524,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     ASDM_CUDA(cudaMemsetAsync(d_fcount, 0, nseg * sizeof(uint32_t), s));
     ASDM_CUDA(cudaMemsetAsync(d_elems, 0, 2 * sizeof(unsigned long long), s));
     if (seg[nseg]) {
-        FilterArgs fa{g, st, d_seg, d_lbase, d_qdeg, d_qnlc, d_qnlc_off, nseg, d_fcount};
+        FilterArgs fa{g, bits, d_seg, d_fword, d_lbase, d_llen, d_qdeg, d_qnlc, d_qnlc_off, nseg, d_fcount};
         k1_filter<<<grid_for(seg[nseg], G->num_sms), kBlock, 0, s>>>(fa);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
@@ -527,13 +590,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             maxwave = std::max(maxwave, qp.wave[u]);
         }
     }
-    // storage S(u) = Ctd(u) (+ vertex 0), capacity |V_l(u)| + 1 per segment
-    std::vector<uint64_t> sbase(nseg + 1, 0);
-    for (const QPlan &qp : P)
-        for (uint32_t u = 0; u < qp.cs->q.n; ++u) sbase[qp.seg0 + u + 1] = sbase[qp.seg0 + u] + qp.lsize[u] + 1;
-    uint32_t *sbuf = nullptr;
-    ASDM_TRY(scr.alloc(&sbuf, sbase[nseg]));
+    // storage S(u) = Ctd(u) (+ vertex 0), one buffer per wave
+    std::vector<const uint32_t *> sptr(nseg, nullptr);
     std::vector<uint64_t> slen(nseg, 0);
+    uint64_t bit_words_read = 0;
     for (uint32_t w = 0; w <= maxwave; ++w) {
         std::vector<PassDesc> passes;
         std::vector<uint64_t> lens;
@@ -545,23 +605,31 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             for (uint32_t u : qp.order) {
                 if (qp.wave[u] != w) continue;
                 const uint32_t su = qp.seg0 + u;
-                uint32_t need = kFBit;
+                uint32_t need = 0;
                 for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                     const uint32_t p = q.nbr[e];
                     if (qp.rank[p] >= qp.rank[u]) continue;
-                    const uint32_t bit = 1u << (e - q.off[u]);
-                    need |= bit;
-                    passes.push_back(PassDesc{sbuf + sbase[qp.seg0 + p], st + seg[su], q.lab[u], bit});
+                    const uint32_t slot = e - q.off[u];
+                    need |= 1u << slot;
+                    passes.push_back(PassDesc{sptr[qp.seg0 + p], bits + fword[su] + (1ull + slot) * words[su], q.lab[u], 0});
                     lens.push_back(slen[qp.seg0 + p]);
                 }
-                segs.push_back(CompDesc{st + seg[su], sbuf + sbase[su], qp.lsize[u], need, qp.lbase[u], 1});
+                segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr,
+                                        nullptr});
                 seg_ids.push_back(su);
+                bit_words_read += (uint64_t)(1 + __builtin_popcount(need)) * words[su];
             }
         }
         ASDM_TRY(run_passes(G, passes, lens, d_elems));
+        uint32_t *sbuf = nullptr;
+        std::vector<uint64_t> start;
         std::vector<uint32_t> sizes;
-        ASDM_TRY(compact(G, segs, sizes));
-        for (size_t i = 0; i < seg_ids.size(); ++i) slen[seg_ids[i]] = sizes[i];
+        ASDM_TRY(compact(G, segs, &sbuf, start, sizes));
+        scr.keep(sbuf);
+        for (size_t i = 0; i < seg_ids.size(); ++i) {
+            sptr[seg_ids[i]] = sbuf + start[i];
+            slen[seg_ids[i]] = sizes[i];
+        }
     }
     // remaining passes (neighbours later in the BFS order), all queries at once
     {
@@ -574,17 +642,22 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                 for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                     const uint32_t p = q.nbr[e];
                     if (qp.rank[p] < qp.rank[u]) continue;
-                    passes.push_back(PassDesc{sbuf + sbase[qp.seg0 + p], st + seg[qp.seg0 + u], q.lab[u],
-                                              1u << (e - q.off[u])});
+                    const uint32_t su = qp.seg0 + u, slot = e - q.off[u];
+                    passes.push_back(PassDesc{sptr[qp.seg0 + p], bits + fword[su] + (1ull + slot) * words[su], q.lab[u], 0});
                     lens.push_back(slen[qp.seg0 + p]);
                 }
         }
         ASDM_TRY(run_passes(G, passes, lens, d_elems));
     }
-    // final candidate sets into the group's arena
+    // final candidate sets into the group's arena, with the membership
+    // bitsets and per-word prefix counts that K3 looks indices up in
     auto arena = std::make_shared<CsArena>();
     arena->stream = s;
-    ASDM_TRY(dalloc(&arena->d_cand, seg[nseg], s));
+    std::vector<uint64_t> mword(nseg + 1, 0);
+    for (uint32_t i = 0; i < nseg; ++i) mword[i + 1] = mword[i] + words[i];
+    uint32_t *cbits = nullptr, *cpre = nullptr;
+    ASDM_TRY(scr.alloc(&cbits, mword[nseg]));
+    ASDM_TRY(scr.alloc(&cpre, mword[nseg]));
     {
         std::vector<CompDesc> segs;
         std::vector<uint32_t> seg_ids;
@@ -594,53 +667,33 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             for (uint32_t u = 0; u < q.n; ++u) {
                 const uint32_t all = q.deg(u) ? ((q.deg(u) == 32 ? 0xFFFFFFFFu : (1u << q.deg(u)) - 1u)) : 0u;
                 const uint32_t su = qp.seg0 + u;
-                segs.push_back(CompDesc{st + seg[su], arena->d_cand + seg[su], qp.lsize[u], kFBit | all, qp.lbase[u], 0});
+                segs.push_back(CompDesc{bits + fword[su], words[su], all, qp.lsize[u], qp.lbase[u], 0, 0,
+                                        cbits + mword[su], cpre + mword[su]});
                 seg_ids.push_back(su);
+                bit_words_read += (uint64_t)(1 + q.deg(u)) * words[su];
             }
         }
+        std::vector<uint64_t> start;
         std::vector<uint32_t> sizes;
-        ASDM_TRY(compact(G, segs, sizes));
+        ASDM_TRY(compact(G, segs, &arena->d_cand, start, sizes));
         std::vector<uint32_t> ncand(nseg, 0);
-        for (size_t i = 0; i < seg_ids.size(); ++i) ncand[seg_ids[i]] = sizes[i];
+        std::vector<uint64_t> cbase(nseg, 0);
+        for (size_t i = 0; i < seg_ids.size(); ++i) {
+            ncand[seg_ids[i]] = sizes[i];
+            cbase[seg_ids[i]] = start[i];
+        }
+        if (!arena->d_cand) ASDM_TRY(dalloc(&arena->d_cand, 1, s));
         for (QPlan &qp : P) {
             if (qp.empty) continue;
             asdm_cs &cs = *qp.cs;
             bool ok = true;
             for (uint32_t u = 0; u < cs.q.n; ++u) {
                 cs.ncand[u] = ncand[qp.seg0 + u];
-                cs.cand_base[u] = seg[qp.seg0 + u];
+                cs.cand_base[u] = cbase[qp.seg0 + u];
                 ok &= cs.ncand[u] > 0;
             }
-            cs.cand_base[cs.q.n] = seg[qp.seg0 + cs.q.n];
+            cs.cand_base[cs.q.n] = cs.cand_base[cs.q.n - 1] + cs.ncand[cs.q.n - 1];
             qp.empty = !ok;
-        }
-    }
-    // candidate edges: rank-in-label -> candidate index maps (reuse st)
-    ASDM_CUDA(cudaMemsetAsync(st, 0xFF, seg[nseg] * sizeof(uint32_t), s));
-    {
-        std::vector<const uint32_t *> cands;
-        std::vector<uint32_t *> maps;
-        std::vector<uint64_t> cpre{0};
-        for (const QPlan &qp : P) {
-            if (qp.empty) continue;
-            for (uint32_t u = 0; u < qp.cs->q.n; ++u) {
-                const uint32_t su = qp.seg0 + u;
-                cands.push_back(arena->d_cand + seg[su]);
-                maps.push_back(st + seg[su]);
-                cpre.push_back(cpre.back() + qp.cs->ncand[u]);
-            }
-        }
-        if (cpre.back()) {
-            const uint32_t **d_cands = nullptr;
-            uint32_t **d_maps = nullptr;
-            uint64_t *d_cpre = nullptr;
-            ASDM_TRY(scr.upload(&d_cands, cands));
-            ASDM_TRY(scr.upload(&d_maps, maps));
-            ASDM_TRY(scr.upload(&d_cpre, cpre));
-            k3_scatter_map<<<grid_for(cpre.back(), G->num_sms), kBlock, 0, s>>>(d_cands, d_cpre, (uint32_t)cands.size(),
-                                                                               d_maps, g.pos_in_label);
-            ::asdm::count_launch();
-            ASDM_CUDA(cudaGetLastError());
         }
     }
     std::vector<EdgeDesc> edges;
@@ -655,7 +708,9 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         for (uint32_t u = 0; u < q.n; ++u)
             for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                 const uint32_t u2 = q.nbr[e];
-                edges.push_back(EdgeDesc{arena->d_cand + seg[qp.seg0 + u], st + seg[qp.seg0 + u2], cs.ncand[u], q.lab[u2]});
+                const uint32_t s2 = qp.seg0 + u2;
+                edges.push_back(EdgeDesc{arena->d_cand + cs.cand_base[u], cbits + mword[s2], cpre + mword[s2],
+                                         cs.ncand[u], q.lab[u2]});
                 item_base.push_back(item_base.back() + cs.ncand[u] + 1);
             }
     }
@@ -702,8 +757,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
-    // K2 scans + K3 scans (count and fill read the same runs) + K1 state words
-    const uint64_t bytes = 4ull * (elems[0] + 2 * elems[1]) + 4ull * seg[nseg];
+    // K1 reads 8 bytes per vertex of each query vertex's label; K2 and K3
+    // read one rank per scanned neighbour (K3 twice: count and fill);
+    // compaction reads the bitsets it ANDs
+    const uint64_t bytes = 8ull * seg[nseg] + 4ull * (elems[0] + 2 * elems[1]) + 4ull * bit_words_read;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         QPlan &qp = P[qi];
         asdm_cs &cs = *qp.cs;

@@ -39,6 +39,8 @@ struct DevGraph {
     const uint32_t *run_off = nullptr;       // n + 1
     const uint32_t *run_lab = nullptr;       // nruns
     const uint32_t *run_start = nullptr;     // nruns
+    const uint32_t *nbr_rank = nullptr;      // m2: pos_in_label of nbr[k]
+    const uint2 *rank_info = nullptr;        // n, in vbl order: {degree, bit (l mod 32) per neighbour label l}
 };
 
 // [b, e) edge range of label l in w's adjacency (empty if w has no such neighbour).

@@ -89,6 +89,21 @@ __global__ void write_runs(DevGraph g, const uint64_t *__restrict__ run_pos, uin
     }
 }
 
+__global__ void nbr_ranks(DevGraph g, uint32_t *__restrict__ rank) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < g.m2; k += (uint64_t)gridDim.x * blockDim.x)
+        rank[k] = g.pos_in_label[g.nbr[k]];
+}
+
+// Per vertex, stored at its place in the vertices-by-label order: degree and
+// a mask with bit (l mod 32) set for every label l among its neighbours.
+__global__ void rank_infos(DevGraph g, uint2 *__restrict__ info) {
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t mask = 0;
+        for (uint32_t r = g.run_off[v]; r < g.run_off[v + 1]; ++r) mask |= 1u << (g.run_lab[r] & 31u);
+        info[g.vbl_off[g.lab[v]] + g.pos_in_label[v]] = make_uint2(g.off[v + 1] - g.off[v], mask);
+    }
+}
+
 __global__ void narrow_u64(const uint64_t *__restrict__ in, uint32_t *__restrict__ out, uint64_t n) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         out[i] = (uint32_t)in[i];
@@ -131,7 +146,7 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     }
     g->max_deg = max_deg;
     // one backing allocation for the fixed-size arrays
-    const uint64_t fixed = (uint64_t)(n + 1) + m2 + n + n + (nlabels + 1) + n + (n + 1);
+    const uint64_t fixed = (uint64_t)(n + 1) + m2 + n + n + (nlabels + 1) + n + (n + 1) + m2 + 1 + 2ull * n;
     ASDM_CUDA(cudaMalloc((void **)&g->buf, fixed * sizeof(uint32_t)));
     uint32_t *p = g->buf;
     uint32_t *d_off = p; p += n + 1;
@@ -141,6 +156,9 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     uint32_t *d_vbl_off = p; p += nlabels + 1;
     uint32_t *d_vbl = p; p += n;
     uint32_t *d_run_off = p; p += n + 1;
+    uint32_t *d_nbr_rank = p; p += m2;
+    if ((p - g->buf) & 1) ++p;  // 8-byte alignment for the uint2 array
+    uint2 *d_rank_info = reinterpret_cast<uint2 *>(p);
     ASDM_CUDA(cudaMemcpyAsync(d_off, offsets, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     if (m2) ASDM_CUDA(cudaMemcpyAsync(d_nbr, nbrs, m2 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     ASDM_CUDA(cudaMemcpyAsync(d_lab, labels, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
@@ -194,6 +212,15 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     d.run_lab = d_run_lab;
     d.run_start = d_run_start;
     d.nruns = nruns;
+    if (m2) {
+        nbr_ranks<<<(unsigned)std::min<uint64_t>((m2 + 255) / 256, (uint64_t)g->num_sms * 32), 256, 0, s>>>(d, d_nbr_rank);
+        ::asdm::count_launch();
+    }
+    rank_infos<<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)g->num_sms * 32), 256, 0, s>>>(d, d_rank_info);
+    ::asdm::count_launch();
+    ASDM_CUDA(cudaGetLastError());
+    d.nbr_rank = d_nbr_rank;
+    d.rank_info = d_rank_info;
     dfree(runs, s); dfree(bad, s); dfree(run_pos, s);
     ASDM_CUDA(cudaStreamSynchronize(s));
     // the run arrays live in their own allocation; remember it for free()
