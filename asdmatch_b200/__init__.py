@@ -97,7 +97,8 @@ _run_plan = _sig("asdm_run_plan", C.c_int, [_vp, _vp, C.POINTER(RunOpts), C.POIN
 _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(RunOpts),
                                                   C.POINTER(RunStats)])
 class Tuning(C.Structure):
-    _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32), ("planner", C.c_uint32)]
+    _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32), ("planner", C.c_uint32),
+                ("root_block_min", C.c_uint32)]
 
 
 PLANNER_DP = 0
@@ -147,6 +148,9 @@ _est_features = _sig("asdm_est_features", C.c_int, [_vp, C.c_uint32, _u64p, C.PO
                                                     C.c_uint64, _u32p, _u64p, _u64p])
 _plan_learned = _sig("asdm_plan_create_learned", C.c_int, [C.c_uint32, C.POINTER(_vp), _vp, C.c_uint32,
                                                            C.POINTER(_vp)])
+_run_planned_profile = _sig("asdm_run_planned_profile", C.c_int,
+                            [C.c_uint32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(BatchOpts), _u64p,
+                             C.POINTER(C.c_int), C.POINTER(RunStats), _u64p])
 _launches = _sig("asdm_kernel_launches", C.c_uint64, [])
 _g_stream = _sig("asdm_graph_stream", C.c_int, [_vp, C.POINTER(_vp)])
 _cs_stats = _sig("asdm_cs_stats", C.c_int, [_vp, _u64p, C.POINTER(C.c_double)])
@@ -275,15 +279,18 @@ class DeviceGraph:
         self.n = g.n
         self.host = g
 
-    def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None):
-        if planner is None:
-            planner = self.tuning()["planner"]
-        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner))), "tuning")
+    def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None,
+                   root_block_min: Optional[int] = None):
+        cur = self.tuning()
+        planner = cur["planner"] if planner is None else planner
+        root_block_min = cur["root_block_min"] if root_block_min is None else root_block_min
+        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner, root_block_min))), "tuning")
 
     def tuning(self):
         t = Tuning()
         _check(_get_tuning(self._h, C.byref(t)))
-        return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max, "planner": t.planner}
+        return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max, "planner": t.planner,
+                "root_block_min": t.root_block_min}
 
     def stream(self) -> int:
         """cudaStream_t (as an int) the library uses for this graph."""
@@ -707,6 +714,24 @@ def plans_learned(css: Sequence[CandidateSpace], est: "Estimator", max_subset: i
     return plans
 
 
+def run_planned_profile(css: Sequence[CandidateSpace], plans: Sequence[Optional["Plan"]], time_limit_s: float = 0.0):
+    """run_planned, also returning per query the SM cycles warps spent on it: (counts, status, stats, cycles)."""
+    nq = len(css)
+    ch = (_vp * max(1, nq))(*[c._h for c in css])
+    ph = (_vp * max(1, nq))(*[(p._h if p is not None else _vp()) for p in plans])
+    opts = BatchOpts()
+    opts.time_limit_s = time_limit_s
+    counts = np.zeros(max(1, nq), np.uint64)
+    status = np.zeros(max(1, nq), np.int32)
+    cycles = np.zeros(max(1, nq), np.uint64)
+    st = RunStats()
+    rc = _run_planned_profile(nq, ch, ph, C.byref(opts), _ptr(counts, _u64p), status.ctypes.data_as(C.POINTER(C.c_int)),
+                              C.byref(st), _ptr(cycles, _u64p))
+    if rc == ERR_CUDA:
+        _check(rc, "planned batch")
+    return counts[:nq], status[:nq], st, cycles[:nq]
+
+
 class Estimator:
     """The learned cardinality estimator: a 3-layer message-passing network on
     the device (BF16 tcgen05 GEMMs, FP32 accumulation), predicting
@@ -769,11 +794,12 @@ def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float
 
 def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
              min_blocks=(1, 4, 5, 6), lane_leaf=(32, 96, 256), planners=(PLANNER_DP, PLANNER_GREEDY),
-             run=None):
+             root_blocks=(1, 4, 16), run=None):
     """Times the caller's batch under every kernel configuration (with the
-    graph's current planner), then every planner with the fastest kernel
-    configuration, and keeps the fastest on `dg` (device time between CUDA
-    events on the library's stream).  `run(dg, batch)` is the timed call
+    graph's current planner and root-block size), then every planner, then
+    every smallest root-block size with the fastest settings so far, and keeps
+    the fastest on `dg` (device time between CUDA events on the library's
+    stream).  `run(dg, batch)` is the timed call
     (default: run_batch_packed).  Returns (best, table)."""
     import torch
     run = run or run_batch_packed
@@ -781,9 +807,9 @@ def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
     want = None
     table = []
 
-    def measure(mb, ll, pl):
+    def measure(mb, ll, pl, rb):
         nonlocal want
-        dg.set_tuning(mb, ll, pl)
+        dg.set_tuning(mb, ll, pl, rb)
         run(dg, batch)  # warm
         if want is None:
             want = batch.counts.copy()
@@ -797,16 +823,21 @@ def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
-        table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "planner": pl, "ms": min(times)})
+        table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "planner": pl, "root_block_min": rb,
+                      "ms": min(times)})
 
-    pl0 = dg.tuning()["planner"]
+    pl0, rb0 = dg.tuning()["planner"], dg.tuning()["root_block_min"]
     for mb in min_blocks:
         for ll in lane_leaf:
-            measure(mb, ll, pl0)
+            measure(mb, ll, pl0, rb0)
     best = min(table, key=lambda r: r["ms"])
     for pl in planners:
         if pl != pl0:
-            measure(best["enum_min_blocks"], best["lane_leaf_max"], pl)
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], pl, rb0)
     best = min(table, key=lambda r: r["ms"])
-    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"])
+    for rb in root_blocks:
+        if rb != rb0:
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], rb)
+    best = min(table, key=lambda r: r["ms"])
+    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], best["root_block_min"])
     return best, table

@@ -94,6 +94,7 @@ extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
     if (t->enum_min_blocks != 1 && (t->enum_min_blocks < 4 || t->enum_min_blocks > 6))
         return fail(ASDM_ERR_INVALID, "enum_min_blocks must be 1, 4, 5 or 6");
     if (t->lane_leaf_max > 4096) return fail(ASDM_ERR_INVALID, "lane_leaf_max must be <= 4096");
+    if (t->root_block_min < 1 || t->root_block_min > 256) return fail(ASDM_ERR_INVALID, "root_block_min must be 1..256");
     if (t->planner != ASDM_PLANNER_DP && t->planner != ASDM_PLANNER_GREEDY)
         return fail(ASDM_ERR_INVALID, "planner must be ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY");
     g->tuning = *t;
@@ -186,7 +187,7 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
 int build_prefix_plan(const asdm_cs &cs, const uint32_t *order, uint32_t depth, asdm_plan &p);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out);
+                    uint64_t *const *local_out, uint64_t *cycles = nullptr);
 int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
                        std::vector<asdm_plan> &plans);
 }  // namespace asdm
@@ -437,8 +438,9 @@ extern "C" int asdm_candidate_space_batch(asdm_graph *g, uint32_t nq, const uint
 }
 
 // One persistent launch over candidate spaces and plans the caller built.
-extern "C" int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans,
-                                const asdm_batch_opts *opts, uint64_t *counts, int *status, asdm_run_stats *stats) {
+extern "C" int asdm_run_planned_profile(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans,
+                                        const asdm_batch_opts *opts, uint64_t *counts, int *status,
+                                        asdm_run_stats *stats, uint64_t *cycles) {
     clear_error();
     if (stats) *stats = asdm_run_stats{};
     if (nq && (!cs || !plans || !counts || !status)) return fail(ASDM_ERR_INVALID, "null argument");
@@ -472,12 +474,22 @@ extern "C" int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan
     std::vector<int> st(run_ids.size());
     const double tl = opts ? opts->time_limit_s : 0.0;
     const uint64_t cl = opts ? opts->count_limit : 0;
-    const int rc = run_batch_count(g, run_cs, run_plans, tl, cl, c.data(), st.data(), stats, nullptr);
+    std::vector<uint64_t> cy(cycles ? run_ids.size() : 0);
+    const int rc = run_batch_count(g, run_cs, run_plans, tl, cl, c.data(), st.data(), stats, nullptr,
+                                   cycles ? cy.data() : nullptr);
+    if (cycles)
+        for (uint32_t i = 0; i < nq; ++i) cycles[i] = 0;
     for (size_t k = 0; k < run_ids.size(); ++k) {
         counts[run_ids[k]] = c[k];
         status[run_ids[k]] = st[k];
+        if (cycles) cycles[run_ids[k]] = cy[k];
         if (st[k] != ASDM_OK && worst == ASDM_OK) worst = st[k];
     }
     if (rc != ASDM_OK && (worst == ASDM_OK || rc == ASDM_ERR_CUDA)) worst = rc;
     return worst;
+}
+
+extern "C" int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans,
+                                const asdm_batch_opts *opts, uint64_t *counts, int *status, asdm_run_stats *stats) {
+    return asdm_run_planned_profile(nq, cs, plans, opts, counts, status, stats, nullptr);
 }

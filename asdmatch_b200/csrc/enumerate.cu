@@ -99,6 +99,7 @@ struct EnumArgs {
     const unsigned long long *ps;
     const uint32_t *rev_off, *rev_list;
     uint32_t tail;
+    unsigned long long *qcycles;  // batches, optional: SM cycles warps spent on each query
 };
 
 struct QDesc {
@@ -121,13 +122,18 @@ struct QDesc {
 // prefix).
 enum : uint32_t { kTailNone = 0, kTailChain = 1, kTailLeaf = 2 };
 
-__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 32; }
+__host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 96; }
 
 // The last level is evaluated one survivor per lane (instead of one warp per
 // survivor) when it has at most this many earlier neighbours and its shortest
 // list is at most kLaneLeafMax long.
 constexpr uint32_t kLaneLeafLists = 4;
 constexpr uint32_t kSelf = 0xFFFFFFFEu;
+constexpr uint32_t kSelfD = 0xFFFFFFFDu;   // the conflict is the lane's own level-d vertex
+// Lane-parallel closed form at level n-3: at most this many conflict levels
+// per tail level, and this many list entries of intersection work per lane.
+constexpr uint32_t kLaneTailConf = 4;
+constexpr uint32_t kLaneTailWork = 64;
 
 __host__ __device__ inline uint32_t plan_words(uint32_t n, uint32_t nb, uint32_t nc) {
     return (uint32_t)((n * sizeof(DLevel) + nb * sizeof(DBack)) / 4) + ((nc + 3) & ~3u);
@@ -180,7 +186,7 @@ struct Warp {
     const DLevel *L;
     const DBack *B;
     const uint32_t *CF;
-    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur, *fidx;
+    uint32_t *idx, *vid, *buf, *cnt, *pos, *dpos, *dend, *drv, *sstart, *slen, *scur, *fidx, *fta, *ftz;
     uint32_t lane;
     uint32_t n;            // levels of the current query
     uint32_t q = 0;        // current query (batches)
@@ -209,6 +215,8 @@ struct Warp {
         slen = sstart + maxnb;
         scur = slen + maxnb;
         fidx = scur + maxnb;
+        fta = fidx + 32;
+        ftz = fta + 32;
     }
 
     // Switches to query qq of a batch (its plan is read from global memory).
@@ -269,6 +277,179 @@ struct Warp {
 #pragma unroll
         for (int o = 16; o; o >>= 1) hits += __shfl_xor_sync(kFull, hits, o);
         return hits;
+    }
+
+    __device__ __forceinline__ bool lane_tail_ok(uint32_t d) const {
+        return MODE == ASDM_MODE_COUNT && tail != kTailNone && d + 3 == n && L[d + 1].nconf <= kLaneTailConf &&
+               L[d + 2].nconf <= kLaneTailConf;
+    }
+
+    // For a node at level d-1 whose level-d entries get lane-parallel tails:
+    // the indices of the prefix's conflict vertices in C(u_{d+1}) (fta) and in
+    // C(u_{d+2}) (ftz); kSelfD where the conflict level is d itself, kSelf
+    // where it is level d+1 (the last level's conflict with level n-2).
+    __device__ void prepare_lane_tail(uint32_t d) {
+        const DLevel La = L[d + 1], Lz = L[d + 2];
+        if (lane < La.nconf) {
+            const uint32_t c = CF[La.conf_first + lane];
+            uint32_t y = kSelfD;
+            if (c < d) {
+                const uint32_t v = vid[c];
+                y = lower_bound_u32(La.cand, La.ncand, v);
+                if (y >= La.ncand || La.cand[y] != v) y = kNone;
+            }
+            fta[lane] = y;
+        }
+        if (lane < Lz.nconf) {
+            const uint32_t c = CF[Lz.conf_first + lane];
+            uint32_t y = c == d + 1 ? kSelf : kSelfD;
+            if (c < d) {
+                const uint32_t v = vid[c];
+                y = lower_bound_u32(Lz.cand, Lz.ncand, v);
+                if (y >= Lz.ncand || Lz.cand[y] != v) y = kNone;
+            }
+            ftz[lane] = y;
+        }
+        __syncwarp();
+    }
+
+    // |x ∩ y| of two ascending lists by one lane: the shorter list's entries
+    // looked up in the longer one.
+    __device__ __forceinline__ static uint32_t lane_isect(const uint32_t *x, uint32_t nx, const uint32_t *y, uint32_t ny) {
+        if (nx > ny) {
+            const uint32_t *t = x; x = y; y = t;
+            const uint32_t tn = nx; nx = ny; ny = tn;
+        }
+        uint32_t hits = 0, cur = 0;
+        for (uint32_t i = 0; i < nx && cur < ny; ++i) {
+            cur = gallop_lb(y, cur, ny, x[i]);
+            hits += cur < ny && y[cur] == x[i];
+        }
+        return hits;
+    }
+
+    // The same by vertex id for candidate-index lists of two candidate sets of one label.
+    __device__ __forceinline__ static uint32_t lane_isect_vid(const uint32_t *x, uint32_t nx, const uint32_t *cx,
+                                                              const uint32_t *y, uint32_t ny, const uint32_t *cy) {
+        uint32_t hits = 0, i = 0, j = 0;
+        while (i < nx && j < ny) {
+            const uint32_t a = cx[x[i]], b = cy[y[j]];
+            hits += a == b;
+            i += a <= b;
+            j += b <= a;
+        }
+        return hits;
+    }
+
+    // The closed form of the last two levels for one level-d entry x (d =
+    // n-3), by this lane alone; false (x left to the warp-wide path) when an
+    // intersection would be long.  Same arithmetic as tail2 with the whole
+    // driver list of level d+1.
+    __device__ bool lane_tail(uint32_t d, uint32_t x, unsigned long long &out, unsigned long long &touched) {
+        const uint32_t a = d + 1;
+        const DLevel La = L[a], Lz = L[a + 1];
+        const DBack ba = B[La.back_first], bz = B[Lz.back_first];
+        const uint32_t ija = ba.level == d ? x : idx[ba.level];
+        const uint32_t s0 = ba.off[ija], nd = ba.off[ija + 1] - s0;
+        const uint32_t *D = ba.list + s0;
+        const uint32_t vx = L[d].cand[x];
+        // conflict indices, resolving the ones that are x's own vertex
+        uint32_t ya[kLaneTailConf], yz[kLaneTailConf];
+        bool self = false;
+#pragma unroll
+        for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+            ya[k] = kNone;
+            yz[k] = kNone;
+            if (k < La.nconf) {
+                uint32_t y = fta[k];
+                if (y == kSelfD) {
+                    y = lower_bound_u32(La.cand, La.ncand, vx);
+                    if (y >= La.ncand || La.cand[y] != vx) y = kNone;
+                }
+                ya[k] = y;
+            }
+            if (k < Lz.nconf) {
+                uint32_t y = ftz[k];
+                if (y == kSelfD) {
+                    y = lower_bound_u32(Lz.cand, Lz.ncand, vx);
+                    if (y >= Lz.ncand || Lz.cand[y] != vx) y = kNone;
+                } else if (y == kSelf) {
+                    self = true;
+                    y = kNone;
+                }
+                yz[k] = y;
+            }
+        }
+        // entries of D that are level-(d+1) conflicts
+        uint32_t xe[kLaneTailConf];
+        uint32_t nexcl = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+            xe[k] = kNone;
+            if (ya[k] != kNone) {
+                const uint32_t p = lower_bound_u32(D, nd, ya[k]);
+                if (p < nd && D[p] == ya[k]) { xe[k] = ya[k]; ++nexcl; }
+            }
+        }
+        unsigned long long sum;
+        uint32_t work = 0;
+        touched += 4;
+        if (tail == kTailChain) {
+            sum = ps[s0 + nd] - ps[s0];
+#pragma unroll
+            for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                if (yz[k] == kNone) continue;
+                const uint32_t r0 = rev_off[yz[k]], nr = rev_off[yz[k] + 1] - r0;
+                work += min(nd, nr);
+                if (work > kLaneTailWork) return false;
+                sum -= lane_isect(D, nd, rev_list + r0, nr);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                if (xe[k] == kNone) continue;
+                const uint32_t a0 = bz.off[xe[k]], a1 = bz.off[xe[k] + 1];
+                unsigned long long c = a1 - a0;
+#pragma unroll
+                for (uint32_t j = 0; j < kLaneTailConf; ++j) {
+                    if (yz[j] == kNone) continue;
+                    const uint32_t q = lower_bound_u32(bz.list + a0, a1 - a0, yz[j]);
+                    c -= (q < a1 - a0 && bz.list[a0 + q] == yz[j]) ? 1ull : 0ull;
+                }
+                sum -= c;
+            }
+        } else {
+            const uint32_t ijz = bz.level == d ? x : idx[bz.level];
+            const uint32_t a0 = bz.off[ijz], nl = bz.off[ijz + 1] - a0;
+            const uint32_t *LL = bz.list + a0;
+            uint32_t m = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                if (yz[k] == kNone) continue;
+                const uint32_t q = lower_bound_u32(LL, nl, yz[k]);
+                m += q < nl && LL[q] == yz[k];
+            }
+            sum = (unsigned long long)(nd - nexcl) * (unsigned long long)(nl - m);
+            if (self) {
+                work += nd + nl;
+                if (work > kLaneTailWork) return false;
+                uint32_t hits = lane_isect_vid(D, nd, La.cand, LL, nl, Lz.cand);
+#pragma unroll
+                for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                    if (xe[k] == kNone) continue;
+                    const uint32_t v = La.cand[xe[k]];
+                    uint32_t l2 = 0, h2 = nl;
+                    while (l2 < h2) {
+                        const uint32_t mid = (l2 + h2) >> 1;
+                        if (Lz.cand[LL[mid]] < v) l2 = mid + 1; else h2 = mid;
+                    }
+                    hits -= (l2 < nl && Lz.cand[LL[l2]] == v) ? 1u : 0u;
+                }
+                sum -= hits;
+            }
+        }
+        touched += work;
+        out = sum;
+        return true;
     }
 
     // The last two levels in closed form for driver positions [lo, hi) of
@@ -672,6 +853,19 @@ struct Warp {
             }
             add_count(c);
             elems += touched;
+        } else if (d + 3 == n && lane_tail_ok(d)) {
+            // the last two levels of every entry lane-parallel; entries whose
+            // intersections are long stay buffered for the warp-wide tail
+            unsigned long long c = 0, touched = 0;
+            const bool done = ok && lane_tail(d, x, c, touched);
+            ok = ok && !done;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                c += __shfl_xor_sync(kFull, c, o);
+                touched += __shfl_xor_sync(kFull, touched, o);
+            }
+            add_count(c);
+            elems += touched;
         }
         const uint32_t mask = __ballot_sync(kFull, ok);
         if (ok) buf[32 * d + __popc(mask & ((1u << lane) - 1))] = x;
@@ -825,6 +1019,8 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
                 --d;
             } else if (d + 2 == n && W.lane_leaf_ok()) {
                 W.prepare_lane_leaf(d);
+            } else if (W.lane_tail_ok(d)) {
+                W.prepare_lane_tail(d);
             }
             continue;
         }
@@ -868,6 +1064,7 @@ __device__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
         return true;
     }
     if (s + 2 == W.n && W.lane_leaf_ok()) W.prepare_lane_leaf(s);
+    else if (W.lane_tail_ok(s)) W.prepare_lane_tail(s);
     return dfs(a, W, lane, s, iter, deadline);
 }
 
@@ -893,6 +1090,7 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
             }
             b = __shfl_sync(kFull, b, 0);
             if (b < nblocks) {
+                const long long c0 = clock64();
                 unsigned long long K = a.blk, P = a.pairs;
                 if (MULTI) {
                     const uint32_t qq = warp_find_row64(a.task_pre, a.nquery, b, lane);
@@ -935,7 +1133,10 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                         ++i0;
                     }
                 }
-                if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+                if (lane == 0) {
+                    if (MULTI && a.qcycles) atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
+                    atomicAdd(&a.ctr[kCtrActive], ~0ull);
+                }
                 continue;
             }
             roots_left = false;
@@ -952,8 +1153,12 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
         }
         W.release(qpos);
         __syncwarp();
+        const long long c0 = clock64();
         stop = !run_range(a, W, lane, s, lo, hi, iter, deadline);
-        if (lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
+        if (lane == 0) {
+            if (MULTI && a.qcycles) atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
+            atomicAdd(&a.ctr[kCtrActive], ~0ull);
+        }
     }
     // flush per-warp totals
     W.flush_count();
@@ -1133,16 +1338,18 @@ int build_tails(const std::vector<const asdm_cs *> &cs, const std::vector<const 
     return ASDM_OK;
 }
 
+unsigned long long root_pairs(const asdm_cs &cs, const asdm_plan &plan) {
+    return plan.order.size() == 1 ? cs.ncand[plan.order[0]] : cs.etotal[plan.back[1][0].second];
+}
+
 // Root tasks: blocks of consecutive (level-0, level-1) candidate pairs, about
 // 64K pairs per block count, between 1 and 256 pairs per block.
+// `min_blk` raises the block size (a batch's whole launch needs only a few
+// dozen tasks per resident warp; work donation splits heavy ranges).
 void root_blocks(const asdm_cs &cs, const asdm_plan &plan, unsigned long long &pairs, unsigned long long &blk,
-                 unsigned long long &nblocks) {
-    if (plan.order.size() == 1) {
-        pairs = cs.ncand[plan.order[0]];
-    } else {
-        pairs = cs.etotal[plan.back[1][0].second];
-    }
-    blk = std::min<unsigned long long>(256, std::max<unsigned long long>(1, pairs / 65536));
+                 unsigned long long &nblocks, unsigned long long min_blk = 1) {
+    pairs = root_pairs(cs, plan);
+    blk = std::min<unsigned long long>(256, std::max<unsigned long long>(min_blk, pairs / 65536));
     nblocks = (pairs + blk - 1) / blk;
 }
 
@@ -1332,13 +1539,14 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
 // counts[i] / status[i] receive each query's result.
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out) {
+                    uint64_t *const *local_out, uint64_t *cycles) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
     std::vector<uint32_t> live;  // queries with a non-empty candidate space
     for (uint32_t i = 0; i < Q; ++i) {
         counts[i] = 0;
         status[i] = ASDM_OK;
+        if (cycles) cycles[i] = 0;
         if (cs[i]->nonempty) live.push_back(i);
     }
     if (agg) *agg = asdm_run_stats{};
@@ -1351,6 +1559,9 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     std::vector<QDesc> qd(L);
     std::vector<unsigned long long> task_pre(L + 1, 0);
     uint32_t maxn = 1, maxnb = 1;
+    // smallest root block (a tuning knob: larger blocks cost less per pair,
+    // smaller ones balance heavy subtrees better)
+    const unsigned long long min_blk = std::max<uint32_t>(1, G->tuning.root_block_min);
     auto append = [&](const void *src, size_t bytes) {
         const uint64_t at = (hp.size() + 15) & ~15ull;
         hp.resize(at + bytes);
@@ -1384,7 +1595,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         qd[li].nb = (uint32_t)bk.size();
         qd[li].nc = (uint32_t)cf.size();
         unsigned long long nt = 0;
-        root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt);
+        root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt, min_blk);
         task_pre[li + 1] = task_pre[li] + nt;
         maxn = std::max(maxn, n);
         maxnb = std::max(maxnb, (uint32_t)bk.size());
@@ -1392,7 +1603,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     const uint64_t qd_at = append(nullptr, L * sizeof(QDesc));
     const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
     uint8_t *d_buf = nullptr;
-    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr;
+    unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr, *d_cyc = nullptr;
     uint32_t *d_queue = nullptr;
     unsigned int *d_qflags = nullptr;
     int rc = ASDM_OK;
@@ -1457,6 +1668,14 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         a.maxnb = maxnb;
         a.qcounts = d_qcounts;
         a.qflags = d_qflags;
+        if (cycles) {
+            if ((rc = dalloc(&d_cyc, L, s))) break;
+            if (cudaMemsetAsync(d_cyc, 0, L * sizeof(unsigned long long), s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "cycle counter reset failed");
+                break;
+            }
+            a.qcycles = d_cyc;
+        }
         a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
         a.count_limit = count_limit;
         const uint32_t smem = 4u * kWarps * warp_words(maxn, maxnb);
@@ -1508,6 +1727,16 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
+        if (cycles) {
+            std::vector<unsigned long long> cy(L);
+            if (cudaMemcpyAsync(cy.data(), d_cyc, L * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "cycle readback failed");
+                break;
+            }
+            for (uint32_t li = 0; li < L; ++li) cycles[live[li]] = cy[li];
+        }
         const uint32_t gflags = (uint32_t)ctr[kCtrFlags];
         for (uint32_t li = 0; li < L; ++li) {
             const uint32_t i = live[li];
@@ -1539,6 +1768,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     dfree(d_ps, s);
+    dfree(d_cyc, s);
     dfree(d_buf, s);
     dfree(d_ctr, s);
     dfree(d_qcounts, s);

@@ -402,7 +402,8 @@ def main():
                    "what": "asdm_run_batch_ex with the learned estimator: candidate spaces, learned greedy plans "
                            "(one forward pass per planner step for the whole group), one persistent launch; "
                            "planning is inside the timed region"}
-        dg.set_tuning(tune_best["enum_min_blocks"], tune_best["lane_leaf_max"], tune_best["planner"])
+        dg.set_tuning(tune_best["enum_min_blocks"], tune_best["lane_leaf_max"], tune_best["planner"],
+                      tune_best["root_block_min"])
     # end to end through the one-call C ABI (asdm_run_batch) from host buffers
     e2e_times = []
     h2d = packed.nbytes()

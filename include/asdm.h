@@ -113,6 +113,7 @@ typedef struct asdm_tuning {
     uint32_t enum_min_blocks;
     uint32_t lane_leaf_max;
     uint32_t planner;          /* ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY */
+    uint32_t root_block_min;   /* batches: fewest (level-0, level-1) pairs per root task, 1..256 */
 } asdm_tuning;
 /* Order search: exhaustive over connected prefixes where the query is small
  * enough (at most 24 vertices and 4096 connected vertex subsets), else
@@ -300,6 +301,12 @@ int asdm_candidate_space_batch(asdm_graph *g, uint32_t nq, const uint32_t *q_siz
  * spaces on the same graph; opts->cards is ignored (plans are given). */
 int asdm_run_planned(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans, const asdm_batch_opts *opts,
                      uint64_t *counts, int *status, asdm_run_stats *stats);
+/* The same, also returning per query the SM clock cycles that warps spent
+ * on its tasks (summed over warps): where a batch's enumeration time goes.
+ * No reference counterpart. */
+int asdm_run_planned_profile(uint32_t nq, asdm_cs *const *cs, const asdm_plan *const *plans,
+                             const asdm_batch_opts *opts, uint64_t *counts, int *status, asdm_run_stats *stats,
+                             uint64_t *cycles);
 
 /* Partial-match counts of query-vertex prefixes inside a candidate space:
  * prefix i is orders[i*|Vq| .. i*|Vq| + depths[i]) (distinct vertices, each
