@@ -75,6 +75,8 @@ _hg_info = _sig("asdm_host_graph_info", C.c_int, [_vp, _u32p, _u64p, _u32p])
 _hg_csr = _sig("asdm_host_graph_csr", C.c_int, [_vp, C.POINTER(_u32p), C.POINTER(_u32p), C.POINTER(_u32p)])
 _hg_write = _sig("asdm_host_graph_write", C.c_int, [_vp, C.c_char_p])
 _hg_free = _sig("asdm_host_graph_free", None, [_vp])
+_hg_write_bin = _sig("asdm_host_graph_write_binary", C.c_int, [_vp, C.c_char_p])
+_hg_load_bin = _sig("asdm_host_graph_load_binary", C.c_int, [C.c_char_p, C.POINTER(_vp)])
 _gen_cl = _sig("asdm_gen_chung_lu", C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_uint32, C.c_double, C.c_uint64,
                                               C.POINTER(_vp)])
 _gen_clc = _sig("asdm_gen_chung_lu_capped", C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_uint32, C.c_double,
@@ -247,6 +249,17 @@ class HostGraph:
 
     def write(self, path: str):
         _check(_hg_write(self._h, path.encode()), path)
+
+    def write_binary(self, path: str):
+        """The reference's binary graph cache (Graph::writeToStream)."""
+        _check(_hg_write_bin(self._h, path.encode()), path)
+
+    @classmethod
+    def load_binary(cls, path: str) -> "HostGraph":
+        """Graph::readFromStream (relation/graph.cpp:293-314)."""
+        h = _vp()
+        _check(_hg_load_bin(path.encode(), C.byref(h)), path)
+        return cls(h.value)
 
     def degree(self, v: int) -> int:
         return int(self.offsets[v + 1] - self.offsets[v])

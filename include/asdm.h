@@ -71,6 +71,11 @@ int asdm_host_graph_csr(const asdm_host_graph *g, const uint32_t **offsets, cons
                         const uint32_t **labels);
 /* Writes the graph in 't/v/e' text (Graph::writeToTextFile, relation/graph.h:157). */
 int asdm_host_graph_write(const asdm_host_graph *g, const char *path);
+/* The reference's binary graph cache (Graph::writeToStream / readFromStream,
+ * relation/graph.cpp:293-332): byte-identical to what the reference writes
+ * for the same graph; the reader keeps CSR and labels. */
+int asdm_host_graph_write_binary(const asdm_host_graph *g, const char *path);
+int asdm_host_graph_load_binary(const char *path, asdm_host_graph **out);
 void asdm_host_graph_free(asdm_host_graph *g);
 
 /* Seeded Chung-Lu power-law graph: weights (i+i0)^(-1/(gamma-1)) with i0 set so

@@ -18,7 +18,9 @@
 //                   reference's CandidateSpace::writeToStream listing
 //                   (relation/candidate_space.cpp:489-505);
 //        -e <file>  (COLLECT_RESULT builds) the embedding set, sorted, in the
-//                   reference's storeMatches format (matching/join.cpp:1099-1107).
+//                   reference's storeMatches format (matching/join.cpp:1099-1107);
+//        -b <file>  the data graph in the reference's binary cache format
+//                   (Graph::writeToStream, relation/graph.cpp:316-332), then exit.
 // Build variants select the reference's compile-time modes (config/config.h:38-40):
 //   ref_count : ALL_LEVEL                          (exact counts)
 //   ref_local : ALL_LEVEL + LOCAL_COUNT            (+ |Vg|x|Vq| CSV via -c)
@@ -60,6 +62,13 @@ int main(int argc, char **argv) {
     const size_t budget = (size_t)1024 * memKB;
 
     Graph q, g;
+    const std::string binOut = option_after(argc, argv, "-b");
+    if (!binOut.empty()) {
+        g.loadGraphFromTextFile(dpath);
+        std::ofstream os(binOut, std::ios::binary);
+        g.writeToStream(os);
+        return 0;
+    }
     q.loadGraphFromTextFile(qpath);
     g.loadGraphFromTextFile(dpath);
     CandidateSpace cs(q, g);
