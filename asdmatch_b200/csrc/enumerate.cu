@@ -1559,9 +1559,11 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     std::vector<QDesc> qd(L);
     std::vector<unsigned long long> task_pre(L + 1, 0);
     uint32_t maxn = 1, maxnb = 1;
-    // smallest root block (a tuning knob: larger blocks cost less per pair,
-    // smaller ones balance heavy subtrees better)
-    const unsigned long long min_blk = std::max<uint32_t>(1, G->tuning.root_block_min);
+    // Root blocks of "light" plans (at most 4 levels with a closed-form tail:
+    // every pair then costs O(1)) hold at least root_block_min pairs, which
+    // saves per-task overhead; other plans keep fine blocks, which balance
+    // heavy subtrees.
+    const unsigned long long light_blk = std::max<uint32_t>(1, G->tuning.root_block_min);
     auto append = [&](const void *src, size_t bytes) {
         const uint64_t at = (hp.size() + 15) & ~15ull;
         hp.resize(at + bytes);
@@ -1595,7 +1597,8 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         qd[li].nb = (uint32_t)bk.size();
         qd[li].nc = (uint32_t)cf.size();
         unsigned long long nt = 0;
-        root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt, min_blk);
+        const bool light = local_out == nullptr && n <= 4 && tail_mode(plan) != kTailNone;
+        root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt, light ? light_blk : 1);
         task_pre[li + 1] = task_pre[li] + nt;
         maxn = std::max(maxn, n);
         maxnb = std::max(maxnb, (uint32_t)bk.size());

@@ -118,7 +118,8 @@ typedef struct asdm_tuning {
     uint32_t enum_min_blocks;
     uint32_t lane_leaf_max;
     uint32_t planner;          /* ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY */
-    uint32_t root_block_min;   /* batches: fewest (level-0, level-1) pairs per root task, 1..256 */
+    uint32_t root_block_min;   /* batches: fewest (level-0, level-1) pairs per root task of plans of at
+                                  most 4 levels with a closed-form tail, 1..256 (default 64) */
 } asdm_tuning;
 /* Order search: exhaustive over connected prefixes where the query is small
  * enough (at most 24 vertices and 4096 connected vertex subsets), else

@@ -239,13 +239,12 @@ def test_every_tuning_gives_the_same_counts(golden, c0d_files, dg_c0d):
     # four kernel configurations, then the other planner, then two more root-block sizes
     assert len(table) == 7 and best in table
     assert {r["planner"] for r in table} == {A.PLANNER_DP, A.PLANNER_GREEDY}
-    assert {r["root_block_min"] for r in table} == {1, 4, 16}
-    dg_c0d.set_tuning(1, 96, A.PLANNER_DP, 1)
-    for rb in (4, 256):
+    assert {r["root_block_min"] for r in table} == {16, 64, 256}
+    for rb in (1, 4, 256):
         dg_c0d.set_tuning(1, 96, A.PLANNER_DP, rb)
         A.run_batch_packed(dg_c0d, b)
         assert b.counts.tolist() == want, rb
-    dg_c0d.set_tuning(1, 96, A.PLANNER_DP, 1)
+    dg_c0d.set_tuning(1, 96, A.PLANNER_DP, 64)
 
 
 def test_batched_local_counts_match_golden_csv(golden, c0_files, c0d_files, dg_c0, dg_c0d, edge_files):
