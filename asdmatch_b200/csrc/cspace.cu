@@ -32,6 +32,9 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr uint32_t kLongRun = 32;
+// K3b pads candidate-edge lists to their label-run lengths up to this many
+// entries in total (4 GiB), and counts first beyond it.
+constexpr uint64_t kPaddedEdgeCap = 1ull << 30;
 
 __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ prefix, uint32_t nseg, uint64_t item) {
     // last s with prefix[s] <= item (prefix has nseg + 1 entries, non-decreasing)
@@ -61,32 +64,48 @@ struct FilterArgs {
     uint32_t *fcount;         // |F(u)|
 };
 
+// A warp takes a run of up to kK1Words words (32 items each) inside one
+// segment, so the segment lookup and the query vertex's parameters are read
+// once per run.
+constexpr uint32_t kK1Words = 32;
+
 __global__ void __launch_bounds__(kBlock) k1_filter(FilterArgs a) {
-    const uint64_t total = a.seg[a.nq];
+    const uint64_t total_words = a.seg[a.nq] / 32;
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
-        const uint32_t u = find_segment(a.seg, a.nq, base);
-        const uint32_t i = (uint32_t)(base - a.seg[u]) + lane;
-        bool pass = false;
-        if (i < a.llen[u]) {
-            // degree and neighbour-label mask of the vertex, in label order
-            const uint2 info = a.g.rank_info[a.lbase[u] + i];
-            pass = info.x >= a.qdeg[u];
-            for (uint32_t k = a.qnlc_off[u]; pass && k < a.qnlc_off[u + 1]; ++k) {
-                const uint32_t l = a.qnlc[2 * k], c = a.qnlc[2 * k + 1];
-                pass = l < a.g.nlabels && ((info.y >> (l & 31u)) & 1u);
-                if (pass && (c > 1 || a.g.nlabels > 32)) {
-                    uint32_t b, e;
-                    label_run(a.g, a.g.vbl[a.lbase[u] + i], l, b, e);
-                    pass = (e - b) >= c;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const uint64_t nruns = (total_words + kK1Words - 1) / kK1Words;
+    for (uint64_t run = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); run < nruns; run += nwarps) {
+        uint64_t w = run * kK1Words;
+        const uint64_t w_end = min(total_words, w + kK1Words);
+        while (w < w_end) {
+            const uint32_t u = find_segment(a.seg, a.nq, w * 32);
+            const uint64_t seg_w0 = a.seg[u] / 32, seg_w1 = a.seg[u + 1] / 32;
+            const uint64_t stop = min(w_end, seg_w1);
+            const uint32_t len = a.llen[u], lbase = a.lbase[u], qdeg = a.qdeg[u];
+            const uint32_t k0 = a.qnlc_off[u], k1 = a.qnlc_off[u + 1];
+            uint32_t total = 0;
+            for (; w < stop; ++w) {
+                const uint32_t i = (uint32_t)(w - seg_w0) * 32 + lane;
+                bool pass = false;
+                if (i < len) {
+                    // degree and neighbour-label mask of the vertex, in label order
+                    const uint2 info = a.g.rank_info[lbase + i];
+                    pass = info.x >= qdeg;
+                    for (uint32_t k = k0; pass && k < k1; ++k) {
+                        const uint32_t l = a.qnlc[2 * k], c = a.qnlc[2 * k + 1];
+                        pass = l < a.g.nlabels && ((info.y >> (l & 31u)) & 1u);
+                        if (pass && (c > 1 || a.g.nlabels > 32)) {
+                            uint32_t b, e;
+                            label_run(a.g, a.g.vbl[lbase + i], l, b, e);
+                            pass = (e - b) >= c;
+                        }
+                    }
                 }
+                const uint32_t word = __ballot_sync(0xffffffffu, pass);
+                if (lane == 0) a.bits[a.fword[u] + (w - seg_w0)] = word;
+                total += __popc(word);
             }
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, pass);
-        if (lane == 0) {
-            a.bits[a.fword[u] + (base - a.seg[u]) / 32] = word;
-            if (word) atomicAdd(&a.fcount[u], (uint32_t)__popc(word));
+            if (lane == 0 && total) atomicAdd(&a.fcount[u], total);
         }
     }
 }
@@ -309,11 +328,52 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
                 }
             }
         }
-        if (!kFill && item < total) cnt[item] = mine;
+        if (cnt && item < total) cnt[item] = mine;
     }
-    if (!kFill) {
+    if (elems) {
         for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
         if (lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
+    }
+}
+
+// Upper bound of every item's list: the length of the candidate's label run.
+__global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *__restrict__ edges,
+                                                   const uint64_t *__restrict__ item_base, uint32_t nedges,
+                                                   uint32_t *__restrict__ ub) {
+    const uint64_t total = item_base[nedges];
+    for (uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; item < total;
+         item += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t ei = find_segment(item_base, nedges, item);
+        const EdgeDesc d = edges[ei];
+        const uint32_t i = (uint32_t)(item - item_base[ei]);
+        uint32_t b = 0, e = 0;
+        if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
+        ub[item] = e - b;
+    }
+}
+
+// Dense copy of the padded lists: a lane per item copies a short list, the
+// warp together copies every list longer than 32 entries.
+__global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ upos, const uint32_t *__restrict__ cnt,
+                                                  const uint64_t *__restrict__ wpos, uint64_t nitems,
+                                                  const uint32_t *__restrict__ padded, uint32_t *__restrict__ elist) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < nitems;
+         base += nwarps * 32) {
+        const uint64_t my = base + lane;
+        const uint32_t c = my < nitems ? cnt[my] : 0u;
+        const uint64_t from = my < nitems ? upos[my] : 0, to = my < nitems ? wpos[my] : 0;
+        if (c <= kLongRun)
+            for (uint32_t k = 0; k < c; ++k) elist[to + k] = padded[from + k];
+        uint32_t todo = __ballot_sync(0xffffffffu, c > kLongRun);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
+            const uint64_t f = __shfl_sync(0xffffffffu, from, src), t = __shfl_sync(0xffffffffu, to, src);
+            for (uint32_t k = lane; k < cc; k += 32) elist[t + k] = padded[f + k];
+        }
     }
 }
 
@@ -525,7 +585,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     ASDM_CUDA(cudaMemsetAsync(d_elems, 0, 2 * sizeof(unsigned long long), s));
     if (seg[nseg]) {
         FilterArgs fa{g, bits, d_seg, d_fword, d_lbase, d_llen, d_qdeg, d_qnlc, d_qnlc_off, nseg, d_fcount};
-        k1_filter<<<grid_for(seg[nseg], G->num_sms), kBlock, 0, s>>>(fa);
+        k1_filter<<<grid_for(seg[nseg] / kK1Words, G->num_sms), kBlock, 0, s>>>(fa);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
     }
@@ -730,16 +790,46 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         ASDM_TRY(dalloc(&arena->d_eoff, nitems, s));
         ASDM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), s));
         const unsigned egrid = grid_for(nitems, G->num_sms);
-        k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, nullptr, nullptr, d_elems + 1);
+        // One scan of the neighbour runs: fill into lists padded to their
+        // label-run lengths (counting on the way), then pack densely; the
+        // exact two-scan form (count, then fill) where the padded lists would
+        // be too large.
+        uint64_t bound = 0;
+        uint64_t *d_upos = nullptr;
+        ASDM_TRY(scr.alloc(&d_upos, nitems + 1));
+        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
-        ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
-        ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
+        ASDM_CUDA(cudaMemcpyAsync(&bound, d_upos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         ASDM_CUDA(cudaStreamSynchronize(s));
-        ASDM_TRY(dalloc(&arena->d_elist, total, s));
-        k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, arena->d_elist, nullptr);
-        ::asdm::count_launch();
-        ASDM_CUDA(cudaGetLastError());
+        if (bound <= kPaddedEdgeCap) {
+            uint32_t *padded = nullptr;
+            ASDM_TRY(scr.alloc(&padded, bound));
+            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, d_upos, padded, d_elems + 1);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+            ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
+            ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+            ASDM_CUDA(cudaStreamSynchronize(s));
+            ASDM_TRY(dalloc(&arena->d_elist, total, s));
+            k3_pack<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_upos, arena->d_eoff, d_wpos, nitems,
+                                                                           padded, arena->d_elist);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+        } else {
+            k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, nullptr, nullptr,
+                                                    d_elems + 1);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+            ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
+            ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+            ASDM_CUDA(cudaStreamSynchronize(s));
+            ASDM_TRY(dalloc(&arena->d_elist, total, s));
+            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, arena->d_elist, nullptr);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+        }
         k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, arena->d_eoff, d_estart, d_bad);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
@@ -758,9 +848,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     // K1 reads 8 bytes per vertex of each query vertex's label; K2 and K3
-    // read one rank per scanned neighbour (K3 twice: count and fill);
-    // compaction reads the bitsets it ANDs
-    const uint64_t bytes = 8ull * seg[nseg] + 4ull * (elems[0] + 2 * elems[1]) + 4ull * bit_words_read;
+    // read one rank per scanned neighbour; compaction reads the bitsets it ANDs
+    const uint64_t bytes = 8ull * seg[nseg] + 4ull * (elems[0] + elems[1]) + 4ull * bit_words_read;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         QPlan &qp = P[qi];
         asdm_cs &cs = *qp.cs;
