@@ -46,6 +46,44 @@ __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ pr
     return lo;
 }
 
+// ---- Visiting order: items grouped by the data vertex they read ------------
+// A K2 work item reads one storage vertex's label runs and adjacency.  Items
+// of a group arrive in per-query order, so popular vertices would be fetched
+// from HBM once per query and pass; grouping the items by vertex id block
+// (kBucketShift) keeps a block's adjacency in L2 while its items run.  The
+// order inside a block does not matter: marking is an atomic OR.
+constexpr uint32_t kBucketShift = 12;
+
+__global__ void bucket_count(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ cnt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys[i] : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        if (valid && (uint32_t)(__ffs(peers) - 1) == lane) atomicAdd(&cnt[key], (unsigned long long)__popc(peers));
+    }
+}
+
+// cursor: exclusive prefix of the counts; order[cursor[key]++] = item
+__global__ void bucket_scatter(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ cursor,
+                               uint32_t *__restrict__ order) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool valid = i < n;
+        const uint32_t key = valid ? keys[i] : 0xFFFFFFFFu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+        unsigned long long at = 0;
+        if (valid && leader == lane) at = atomicAdd(&cursor[key], (unsigned long long)__popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (valid) order[at + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)i;
+    }
+}
+
 // ---- K1: label + degree + NLC filter --------------------------------------
 // One segment per (query, query vertex) of a group; a segment's items are
 // the ranks 0 .. |V_l(u)| - 1 of u's label, padded to a multiple of 32 so
@@ -123,18 +161,31 @@ __device__ __forceinline__ void mark(const DevGraph &g, uint32_t *mb, uint32_t k
     atomicOr(&mb[r >> 5], 1u << (r & 31u));  // result unused: a fire-and-forget reduction
 }
 
+// Bucket keys of the pass items (storage vertex >> kBucketShift).
+__global__ void k2_keys(const PassDesc *__restrict__ passes, const uint64_t *__restrict__ prefix, uint32_t npass,
+                        uint32_t *__restrict__ keys) {
+    const uint64_t total = prefix[npass];
+    for (uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; item < total;
+         item += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = find_segment(prefix, npass, item);
+        keys[item] = passes[p].src[item - prefix[p]] >> kBucketShift;
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__restrict__ passes,
                                                   const uint64_t *__restrict__ prefix, uint32_t npass,
+                                                  const uint32_t *__restrict__ order,
                                                   unsigned long long *__restrict__ elems) {
     const uint64_t total = prefix[npass];
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint64_t scanned = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
-        const uint64_t item = base + lane;
+        const uint64_t pos = base + lane;
+        const uint64_t item = (order && pos < total) ? order[pos] : pos;
         uint32_t b = 0, e = 0;
         uint32_t *mb = nullptr;
-        if (item < total) {
+        if (pos < total) {
             const uint32_t p = find_segment(prefix, npass, item);
             const PassDesc d = passes[p];
             const uint32_t w = d.src[item - prefix[p]];
@@ -278,6 +329,7 @@ __device__ __forceinline__ uint32_t cand_index(const uint32_t *cb, const uint32_
 template <bool kFill>
 __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
+                                                   const uint32_t *__restrict__ order,
                                                    uint32_t *__restrict__ cnt, const uint64_t *__restrict__ wpos,
                                                    uint32_t *__restrict__ elist, unsigned long long *__restrict__ elems) {
     const uint64_t total = item_base[nedges];
@@ -285,10 +337,11 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint64_t scanned = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
-        const uint64_t item = base + lane;
+        const uint64_t pos = base + lane;
+        const uint64_t item = (order && pos < total) ? order[pos] : pos;
         uint32_t b = 0, e = 0;
         const uint32_t *cb = nullptr, *cp = nullptr;
-        if (item < total) {
+        if (pos < total) {
             const uint32_t ei = find_segment(item_base, nedges, item);
             const EdgeDesc d = edges[ei];
             const uint32_t i = (uint32_t)(item - item_base[ei]);
@@ -299,7 +352,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
         scanned += e - b;
         const bool coop = (e - b) > kLongRun;
         uint32_t mine = 0;
-        uint64_t out = kFill && item < total ? wpos[item] : 0;
+        uint64_t out = kFill && pos < total ? wpos[item] : 0;
         uint32_t todo = __ballot_sync(0xffffffffu, coop);
         while (todo) {
             const int src = __ffs(todo) - 1;
@@ -328,7 +381,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
                 }
             }
         }
-        if (cnt && item < total) cnt[item] = mine;
+        if (cnt && pos < total) cnt[item] = mine;
     }
     if (elems) {
         for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
@@ -339,10 +392,11 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
 // Upper bound of every item's list: the length of the candidate's label run.
 __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
-                                                   uint32_t *__restrict__ ub) {
+                                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ub) {
     const uint64_t total = item_base[nedges];
-    for (uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; item < total;
-         item += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t pos = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+         pos += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t item = order ? order[pos] : pos;
         const uint32_t ei = find_segment(item_base, nedges, item);
         const EdgeDesc d = edges[ei];
         const uint32_t i = (uint32_t)(item - item_base[ei]);
@@ -455,6 +509,37 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
     return rc;
 }
 
+// Positions of n items grouped by their keys (vertex blocks) into *order (the
+// caller frees it); *order stays null when n does not fit 32-bit positions
+// or is too small to matter.
+int bucket_order(asdm_graph *G, const uint32_t *d_keys, uint64_t n, uint64_t nb, uint32_t **order) {
+    cudaStream_t s = G->stream;
+    *order = nullptr;
+    if (n < (1u << 16) || n >= 0xFFFFFFFFull) return ASDM_OK;
+    unsigned long long *cnt = nullptr;
+    uint64_t *cur = nullptr;
+    int rc = ASDM_OK;
+    do {
+        if ((rc = dalloc(&cnt, nb, s)) || (rc = dalloc(&cur, nb + 1, s)) || (rc = dalloc(order, n, s))) break;
+        if (cudaMemsetAsync(cnt, 0, nb * sizeof(unsigned long long), s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "bucket reset failed");
+            break;
+        }
+        bucket_count<<<grid_for(n, G->num_sms), kBlock, 0, s>>>(d_keys, n, cnt);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "bucket count failed"); break; }
+        if ((rc = scan_exclusive_u64(reinterpret_cast<const uint64_t *>(cnt), cur, nb, true, s))) break;
+        bucket_scatter<<<grid_for(n, G->num_sms), kBlock, 0, s>>>(d_keys, n, reinterpret_cast<unsigned long long *>(cur),
+                                                                   *order);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "bucket scatter failed"); break; }
+    } while (false);
+    dfree(cnt, s);
+    dfree(cur, s);
+    if (rc != ASDM_OK) dfree(*order, s);
+    return rc;
+}
+
 int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::vector<uint64_t> &lens,
                unsigned long long *d_elems) {
     cudaStream_t s = G->stream;
@@ -469,14 +554,30 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     ASDM_TRY(dalloc(&d_prefix, np + 1, s));
     ASDM_CUDA(cudaMemcpyAsync(d_p, passes.data(), np * sizeof(PassDesc), cudaMemcpyHostToDevice, s));
     ASDM_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), (np + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, d_elems);
-    ::asdm::count_launch();
-    ASDM_CUDA(cudaGetLastError());
+    uint32_t *keys = nullptr, *order = nullptr;
+    int rc = ASDM_OK;
+    if (prefix[np] >= (1u << 16) && prefix[np] < 0xFFFFFFFFull) {
+        rc = dalloc(&keys, prefix[np], s);
+        if (rc == ASDM_OK) {
+            k2_keys<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(d_p, d_prefix, np, keys);
+            ::asdm::count_launch();
+            rc = cudaGetLastError() == cudaSuccess
+                     ? bucket_order(G, keys, prefix[np], ((uint64_t)G->d.n >> kBucketShift) + 1, &order)
+                                                   : fail(ASDM_ERR_CUDA, "pass key kernel failed");
+        }
+    }
+    if (rc == ASDM_OK) {
+        k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, order, d_elems);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
+    }
     // the host vectors above are read by the copies: wait before they go out of scope
-    ASDM_CUDA(cudaStreamSynchronize(s));
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == ASDM_OK) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
+    dfree(keys, s);
+    dfree(order, s);
     dfree(d_p, s);
     dfree(d_prefix, s);
-    return ASDM_OK;
+    return rc;
 }
 
 struct Scratch {
@@ -796,8 +897,12 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         // be too large.
         uint64_t bound = 0;
         uint64_t *d_upos = nullptr;
+        // K3 keeps edge-major order: a warp's lanes take consecutive candidates
+        // of one edge, whose ascending ids put their adjacency runs side by
+        // side in the CSR (grouping by vertex block across edges measured slower)
+        const uint32_t *order = nullptr;
         ASDM_TRY(scr.alloc(&d_upos, nitems + 1));
-        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff);
+        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
         ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
@@ -806,7 +911,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         if (bound <= kPaddedEdgeCap) {
             uint32_t *padded = nullptr;
             ASDM_TRY(scr.alloc(&padded, bound));
-            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, d_upos, padded, d_elems + 1);
+            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, d_upos, padded,
+                                                    d_elems + 1);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
             ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
@@ -818,7 +924,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         } else {
-            k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, nullptr, nullptr,
+            k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, nullptr, nullptr,
                                                     d_elems + 1);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
@@ -826,7 +932,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
             ASDM_CUDA(cudaStreamSynchronize(s));
             ASDM_TRY(dalloc(&arena->d_elist, total, s));
-            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, arena->d_elist, nullptr);
+            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, nullptr, d_wpos, arena->d_elist,
+                                                    nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         }
