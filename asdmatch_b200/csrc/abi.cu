@@ -290,6 +290,8 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
             stats->list_bytes += gs.list_bytes;
             stats->tasks += gs.tasks;
             stats->kernel_ms += gs.kernel_ms;
+            stats->tails_lane += gs.tails_lane;
+            stats->tails_warp += gs.tails_warp;
             for (asdm_cs *gc : group) {
                 stats->build_ms += gc->build_ms;
                 stats->build_bytes += gc->build_bytes;

@@ -33,6 +33,9 @@
 namespace asdm {
 
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
+bool tree_countable(const QueryGraph &q);
+int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
+                std::vector<char> &done);
 
 namespace {
 
@@ -44,7 +47,8 @@ enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4, kFlagI
 constexpr uint32_t kStopFlags = kFlagOverflow | kFlagTimeout | kFlagInternal | kFlagLimit;
 enum : int {
     kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5,
-    kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrN = 16
+    kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrTailLane = 11,
+    kCtrTailWarp = 12, kCtrN = 16
 };
 // Work-donation ring (a bounded multi-producer multi-consumer queue with a
 // sequence number per slot): a record is [query, level s, lo, hi, idx[0..s-1]].
@@ -100,6 +104,7 @@ struct EnumArgs {
     const uint32_t *rev_off, *rev_list;
     uint32_t tail;
     unsigned long long *qcycles;  // batches, optional: SM cycles warps spent on each query
+    const uint32_t *xmap_a, *xmap_z;
 };
 
 struct QDesc {
@@ -111,6 +116,9 @@ struct QDesc {
     uint32_t n, nb, nc, tail;
     const unsigned long long *ps;
     const uint32_t *rev_off, *rev_list;
+    // lane tails at level d = n-3: index in C(u_{n-2}) / C(u_{n-1}) of each
+    // candidate of level d, where level d is a conflict of that level (or null)
+    const uint32_t *xmap_a, *xmap_z;
 };
 
 // The last two levels of a COUNT-mode plan are counted in closed form when
@@ -191,18 +199,19 @@ struct Warp {
     uint32_t n;            // levels of the current query
     uint32_t q = 0;        // current query (batches)
     unsigned long long *local;  // |Vg| x n local counts of the current query (MODE_LOCAL)
-    unsigned long long count = 0, inter = 0, elems = 0;
+    unsigned long long count = 0, inter = 0, elems = 0, tails_lane = 0, tails_warp = 0;
     bool overflow = false;
     const unsigned long long *ps;        // kTailChain: prefix sums over the driver edge of level n-2
     const uint32_t *rev_off, *rev_list;  // kTailChain: candidate edges last level -> level n-2
     uint32_t tail;                       // kTail* of the current query
+    const uint32_t *xmap_a, *xmap_z;     // cross indices for lane tails (or null)
 
     // w: this warp's shared-memory words, laid out for queries of up to maxn
     // levels and maxnb backward edges.
     __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln,
                     uint32_t levels, uint32_t maxn, uint32_t maxnb)
         : a(args), L(l), B(b), CF(cf), lane(ln), n(levels), local(args.local), ps(args.ps), rev_off(args.rev_off),
-          rev_list(args.rev_list), tail(args.tail) {
+          rev_list(args.rev_list), tail(args.tail), xmap_a(args.xmap_a), xmap_z(args.xmap_z) {
         idx = w;
         vid = idx + maxn;
         buf = vid + maxn;
@@ -234,6 +243,8 @@ struct Warp {
         rev_off = d.rev_off;
         rev_list = d.rev_list;
         tail = d.tail;
+        xmap_a = d.xmap_a;
+        xmap_z = d.xmap_z;
     }
 
     __device__ __forceinline__ bool closed_at(uint32_t d) const {
@@ -363,16 +374,24 @@ struct Warp {
             if (k < La.nconf) {
                 uint32_t y = fta[k];
                 if (y == kSelfD) {
-                    y = lower_bound_u32(La.cand, La.ncand, vx);
-                    if (y >= La.ncand || La.cand[y] != vx) y = kNone;
+                    if (xmap_a) {
+                        y = xmap_a[x];
+                    } else {
+                        y = lower_bound_u32(La.cand, La.ncand, vx);
+                        if (y >= La.ncand || La.cand[y] != vx) y = kNone;
+                    }
                 }
                 ya[k] = y;
             }
             if (k < Lz.nconf) {
                 uint32_t y = ftz[k];
                 if (y == kSelfD) {
-                    y = lower_bound_u32(Lz.cand, Lz.ncand, vx);
-                    if (y >= Lz.ncand || Lz.cand[y] != vx) y = kNone;
+                    if (xmap_z) {
+                        y = xmap_z[x];
+                    } else {
+                        y = lower_bound_u32(Lz.cand, Lz.ncand, vx);
+                        if (y >= Lz.ncand || Lz.cand[y] != vx) y = kNone;
+                    }
                 } else if (y == kSelf) {
                     self = true;
                     y = kNone;
@@ -463,6 +482,7 @@ struct Warp {
     //     conflict vertices in LL), minus the x whose own vertex is in LL when
     //     level d is itself a conflict of the last level.
     __device__ void tail2(uint32_t d, uint32_t lo, uint32_t hi) {
+        ++tails_warp;
         const DLevel lv = L[d];
         const uint32_t dslot = lv.back_first;
         const uint32_t s0 = sstart[dslot];
@@ -859,6 +879,7 @@ struct Warp {
             unsigned long long c = 0, touched = 0;
             const bool done = ok && lane_tail(d, x, c, touched);
             ok = ok && !done;
+            tails_lane += __popc(__ballot_sync(kFull, done));
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
                 c += __shfl_xor_sync(kFull, c, o);
@@ -1165,6 +1186,8 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
     if (lane == 0) {
         atomicAdd(&a.ctr[kCtrInter], W.inter);
         atomicAdd(&a.ctr[kCtrElems], W.elems);
+        atomicAdd(&a.ctr[kCtrTailLane], W.tails_lane);
+        atomicAdd(&a.ctr[kCtrTailWarp], W.tails_warp);
     }
 }
 
@@ -1205,6 +1228,8 @@ __global__ void __launch_bounds__(kThreads, MINB) enum_batch_kernel(EnumArgs a) 
     W.rev_off = d0.rev_off;
     W.rev_list = d0.rev_list;
     W.tail = d0.tail;
+    W.xmap_a = d0.xmap_a;
+    W.xmap_z = d0.xmap_z;
     warp_loop<MODE, true>(a, W, lane);
 }
 
@@ -1228,6 +1253,33 @@ __global__ void tail_lens(const TailSeg *__restrict__ seg, uint32_t nseg, unsign
         }
         const uint32_t x = seg[lo].list[t - seg[lo].start];
         lens[t] = seg[lo].off2[x + 1] - seg[lo].off2[x];
+    }
+}
+
+// Cross indices: for candidate i of one query vertex, its index in the
+// candidate set of another query vertex of the same label (or kNone).
+struct XSeg {
+    const uint32_t *from;   // candidate set the map is indexed by
+    const uint32_t *to;     // candidate set the indices point into
+    uint32_t *out;
+    uint32_t nto;
+    uint32_t pad;
+    unsigned long long start, len;
+};
+
+__global__ void cross_index(const XSeg *__restrict__ seg, uint32_t nseg, unsigned long long total) {
+    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (seg[mid].start <= t) lo = mid; else hi = mid;
+        }
+        const XSeg sg = seg[lo];
+        const unsigned long long i = t - sg.start;
+        const uint32_t v = sg.from[i];
+        const uint32_t j = lower_bound_u32(sg.to, sg.nto, v);
+        sg.out[i] = (j < sg.nto && sg.to[j] == v) ? j : kNone;
     }
 }
 
@@ -1268,7 +1320,63 @@ struct TailData {
     uint32_t mode = kTailNone;
     const unsigned long long *ps = nullptr;
     const uint32_t *rev_off = nullptr, *rev_list = nullptr;
+    const uint32_t *xmap_a = nullptr, *xmap_z = nullptr;
 };
+
+// Cross-index maps for the lane tails of every plan whose level n-3 is a
+// conflict level of level n-2 or n-1 (one device array, *d_x, caller frees).
+int build_xmaps(const std::vector<const asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                std::vector<TailData> &td, uint32_t **d_x, cudaStream_t s) {
+    *d_x = nullptr;
+    std::vector<XSeg> segs;
+    std::vector<std::pair<size_t, int>> owner;  // (plan, 0 = a / 1 = z)
+    unsigned long long total = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+        if (td[i].mode == kTailNone) continue;
+        const asdm_plan &p = *plans[i];
+        const size_t n = p.order.size();
+        if (n < 4) continue;
+        const uint32_t d = (uint32_t)n - 3;
+        const asdm_cs &c = *cs[i];
+        const uint32_t ud = p.order[d];
+        for (int which = 0; which < 2; ++which) {
+            const uint32_t t = (uint32_t)n - 2 + which;
+            if (std::find(p.conf[t].begin(), p.conf[t].end(), d) == p.conf[t].end()) continue;
+            const uint32_t ut = p.order[t];
+            XSeg sg{c.d_cand + c.cand_base[ud], c.d_cand + c.cand_base[ut], nullptr, c.ncand[ut], 0, total,
+                    c.ncand[ud]};
+            segs.push_back(sg);
+            owner.emplace_back(i, which);
+            total += c.ncand[ud];
+        }
+    }
+    if (segs.empty()) return ASDM_OK;
+    ASDM_TRY(dalloc(d_x, total, s));
+    for (auto &sg : segs) sg.out = *d_x + sg.start;
+    XSeg *d_seg = nullptr;
+    int rc = dalloc(&d_seg, segs.size(), s);
+    if (rc == ASDM_OK &&
+        cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(XSeg), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        rc = fail(ASDM_ERR_CUDA, "cross-index upload failed");
+    if (rc == ASDM_OK && total) {
+        const unsigned grid = (unsigned)std::min<unsigned long long>((total + 255) / 256, 148ull * 32);
+        cross_index<<<grid, 256, 0, s>>>(d_seg, (uint32_t)segs.size(), total);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "cross-index kernel failed");
+    }
+    cudaStreamSynchronize(s);  // the upload reads a host vector
+    dfree(d_seg, s);
+    if (rc != ASDM_OK) {
+        dfree(*d_x, s);
+        return rc;
+    }
+    for (size_t k = 0; k < segs.size(); ++k) {
+        if (owner[k].second == 0) td[owner[k].first].xmap_a = segs[k].out;
+        else td[owner[k].first].xmap_z = segs[k].out;
+    }
+    return ASDM_OK;
+}
+
 int build_tails(const std::vector<const asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                 std::vector<TailData> &out, unsigned long long **d_ps, cudaStream_t s) {
     *d_ps = nullptr;
@@ -1363,6 +1471,30 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     if (opt.local_counts && (mode & ASDM_MODE_LOCAL))
         std::fill(opt.local_counts, opt.local_counts + (uint64_t)G->d.n * n, 0ull);
     if (!cs.nonempty) return ASDM_OK;
+    if (mode == ASDM_MODE_COUNT && plan.order.size() == n && tree_countable(q)) {
+        // conflict-free tree: the tree program counts it (the enumeration
+        // below only when the program overflows)
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, s);
+        std::vector<uint64_t> tc;
+        std::vector<char> done;
+        const int trc = tree_counts(G, {&cs}, tc, done);
+        cudaEventRecord(t1, s);
+        cudaEventSynchronize(t1);
+        float tms = 0.f;
+        cudaEventElapsedTime(&tms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (trc != ASDM_OK) return trc;
+        if (done[0]) {
+            st.count = tc[0];
+            st.kernel_ms = tms;
+            if (opt.count_limit && st.count > opt.count_limit) return fail(ASDM_ERR_LIMIT, "count limit reached");
+            return ASDM_OK;
+        }
+    }
     // device plan
     std::vector<DLevel> lv(n);
     std::vector<DBack> bk;
@@ -1390,10 +1522,11 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     std::memcpy(hp.data() + n * sizeof(DLevel) + nb * sizeof(DBack), cf.data(), nc * sizeof(uint32_t));
     uint8_t *d_plan = nullptr;
     unsigned long long *d_ctr = nullptr, *d_local = nullptr, *d_ps = nullptr;
-    uint32_t *d_rows = nullptr, *d_queue = nullptr;
+    uint32_t *d_rows = nullptr, *d_queue = nullptr, *d_xmap = nullptr;
     int rc = ASDM_OK;
     auto cleanup = [&]() {
         dfree(d_ps, s);
+        dfree(d_xmap, s);
         dfree(d_plan, s);
         dfree(d_ctr, s);
         dfree(d_local, s);
@@ -1451,10 +1584,13 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         if (mode == ASDM_MODE_COUNT) {
             std::vector<TailData> td;
             if ((rc = build_tails({&cs}, {&plan}, td, &d_ps, s))) break;
+            if ((rc = build_xmaps({&cs}, {&plan}, td, &d_xmap, s))) break;
             a.tail = td[0].mode;
             a.ps = td[0].ps;
             a.rev_off = td[0].rev_off;
             a.rev_list = td[0].rev_list;
+            a.xmap_a = td[0].xmap_a;
+            a.xmap_z = td[0].xmap_z;
         }
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         cudaEventCreate(&e0);
@@ -1483,6 +1619,8 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         st.kernel_ms = ms;
+        st.tails_lane = ctr[kCtrTailLane];
+        st.tails_warp = ctr[kCtrTailWarp];
         st.count = ctr[kCtrCount];
         st.intersections = ctr[kCtrInter];
         st.list_bytes = 4ull * ctr[kCtrElems];
@@ -1551,6 +1689,48 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     }
     if (agg) *agg = asdm_run_stats{};
     if (live.empty()) return ASDM_OK;
+    // COUNT mode: conflict-free tree queries are counted by the tree program
+    // (full plans only; prefix plans count partial matches)
+    float tree_ms = 0.f;
+    if (!local_out) {
+        std::vector<asdm_cs *> tcs;
+        std::vector<uint32_t> tid;
+        for (uint32_t i : live)
+            if (plans[i]->order.size() == cs[i]->q.n && tree_countable(cs[i]->q)) {
+                tcs.push_back(cs[i]);
+                tid.push_back(i);
+            }
+        if (!tcs.empty()) {
+            cudaEvent_t t0, t1;
+            cudaEventCreate(&t0);
+            cudaEventCreate(&t1);
+            cudaEventRecord(t0, s);
+            std::vector<uint64_t> tc;
+            std::vector<char> done;
+            const int trc = tree_counts(G, tcs, tc, done);
+            cudaEventRecord(t1, s);
+            cudaEventSynchronize(t1);
+            cudaEventElapsedTime(&tree_ms, t0, t1);
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            if (trc != ASDM_OK) return trc;
+            std::vector<char> settled(Q, 0);
+            for (size_t k = 0; k < tid.size(); ++k)
+                if (done[k]) {
+                    const uint32_t i = tid[k];
+                    settled[i] = 1;
+                    counts[i] = tc[k];
+                    if (count_limit && tc[k] > count_limit) status[i] = ASDM_ERR_LIMIT;
+                    if (agg) agg->count += tc[k];
+                }
+            std::vector<uint32_t> rest;
+            for (uint32_t i : live)
+                if (!settled[i]) rest.push_back(i);
+            live.swap(rest);
+            if (agg) agg->kernel_ms += tree_ms;
+            if (live.empty()) return ASDM_OK;
+        }
+    }
     const uint32_t L = (uint32_t)live.size();
     // host images of all plans, then one upload
     std::vector<uint8_t> hp;
@@ -1607,7 +1787,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
     uint8_t *d_buf = nullptr;
     unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr, *d_cyc = nullptr;
-    uint32_t *d_queue = nullptr;
+    uint32_t *d_queue = nullptr, *d_xmap = nullptr;
     unsigned int *d_qflags = nullptr;
     int rc = ASDM_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1636,11 +1816,14 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             }
             std::vector<TailData> td;
             if ((rc = build_tails(tcs, tpl, td, &d_ps, s))) break;
+            if ((rc = build_xmaps(tcs, tpl, td, &d_xmap, s))) break;
             for (uint32_t li = 0; li < L; ++li) {
                 qd[li].tail = td[li].mode;
                 qd[li].ps = td[li].ps;
                 qd[li].rev_off = td[li].rev_off;
                 qd[li].rev_list = td[li].rev_list;
+                qd[li].xmap_a = td[li].xmap_a;
+                qd[li].xmap_z = td[li].xmap_z;
             }
         }
         for (uint32_t li = 0; li < L; ++li) {
@@ -1750,11 +1933,13 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             else if (qf[li] & kFlagLimit) status[i] = ASDM_ERR_LIMIT;
         }
         if (agg) {
-            agg->count = ctr[kCtrCount];
+            agg->count += ctr[kCtrCount];
             agg->intersections = ctr[kCtrInter];
             agg->list_bytes = 4ull * ctr[kCtrElems];
             agg->tasks = task_pre[L];
-            agg->kernel_ms = ms;
+            agg->kernel_ms += ms;
+            agg->tails_lane = ctr[kCtrTailLane];
+            agg->tails_warp = ctr[kCtrTailWarp];
         }
         if (gflags & kFlagInternal) rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
         else if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
@@ -1771,6 +1956,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     dfree(d_ps, s);
+    dfree(d_xmap, s);
     dfree(d_cyc, s);
     dfree(d_buf, s);
     dfree(d_ctr, s);

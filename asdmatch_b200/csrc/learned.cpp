@@ -112,6 +112,14 @@ void subset_features(const asdm_cs &cs, uint64_t mask, uint32_t graph, FeatBatch
 // Learned log(1 + cardinality) -> cardinality.
 double from_log(float y) { return std::expm1((double)std::min(std::max(y, 0.f), 60.f)); }
 
+// A subset has at most prod |C(u)| partial matches.
+bool in_range(const asdm_cs &cs, uint64_t mask, double card) {
+    if (!std::isfinite(card) || card < 0) return false;
+    double log_bound = 0;
+    for (uint64_t r = mask; r; r &= r - 1) log_bound += std::log(std::max(1.0, (double)cs.ncand[__builtin_ctzll(r)]));
+    return std::log1p(card) <= log_bound + 1e-9;
+}
+
 // Predictions for a list of (query, subset) requests, in chunks that bound
 // the estimator's device workspace.
 int predict(asdm_estimator *e, const std::vector<const asdm_cs *> &qs, const std::vector<uint64_t> &masks,
@@ -189,7 +197,8 @@ int greedy_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, u
             const asdm_cs &cs = *css[x.query];
             if (!x.alive || k >= cs.q.n) continue;
             for (size_t c = 0; c < x.cands.size(); ++c)
-                if (x.req[c] >= 0) x.cands[c].Nu = est[(size_t)x.req[c]];
+                if (x.req[c] >= 0 && in_range(cs, x.st.mask | (1ull << x.cands[c].u), est[(size_t)x.req[c]]))
+                    x.cands[c].Nu = est[(size_t)x.req[c]];
             x.alive = greedy_take(cs, x.st, x.cands);
         }
     }
@@ -253,8 +262,12 @@ int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uin
     std::vector<double> est;
     if (!rm.empty()) ASDM_TRY(predict(e, rq, rm, est));
     for (uint32_t i : dp_ids) {
+        // a prediction outside the possible range (more partial matches than
+        // the product of the subset's candidate-set sizes, or not finite) is
+        // dropped: the planner's own estimate stands in for it
         std::unordered_map<uint64_t, double> known;
-        for (size_t r = range[i].first; r < range[i].second; ++r) known.emplace(rm[r], est[r]);
+        for (size_t r = range[i].first; r < range[i].second; ++r)
+            if (in_range(*css[i], rm[r], est[r])) known.emplace(rm[r], est[r]);
         std::vector<uint32_t> order;
         double cost = 0;
         const bool ok = plan_dp(*css[i], [&](uint64_t S, double &c) {

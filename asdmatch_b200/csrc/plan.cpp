@@ -129,10 +129,16 @@ void greedy_from(const asdm_cs &cs, const asdm_card *card, uint32_t start, std::
 // the caller's figure where it has one (a .card entry, a learned estimate),
 // else the smallest over last vertices u of N(S - u) times the greedy's
 // extension factor.
+// When levels n-2 and n-1 each have one backward edge, the enumeration
+// counts both in closed form per level-(n-3) partial match (COUNT mode):
+//   last two steps:  N(P) * kTail
+// Since the vertex left after a prefix of n-1 vertices is fixed, the last
+// step is folded into the cost of that prefix.
 namespace {
 constexpr double kOpen = 4.0;     // opening a level for one partial match (list offsets, driver choice)
 constexpr double kProbe = 2.0;    // galloping into one more list, per driver entry
 constexpr double kLeafOne = 1.0;  // a one-list last level
+constexpr double kTail = 1.0;     // the closed form of the last two levels, per level-(n-3) partial match
 }  // namespace
 
 bool connected_subsets(const QueryGraph &q, uint32_t max_size, size_t limit, std::vector<uint64_t> &out) {
@@ -212,8 +218,23 @@ bool plan_dp(const asdm_cs &cs, const std::function<bool(uint64_t, double &)> &k
                 factor *= std::min(1.0, lens[i] / std::max(1.0, (double)cs.ncand[u]));
             }
             derived = std::min(derived, EP.N * factor);
-            const double step = (k == n && B == 1) ? EP.N * kLeafOne
-                                                   : EP.N * (kOpen + drv * (1.0 + (B - 1) * kProbe));
+            double step = (k == n && B == 1) ? EP.N * kLeafOne : EP.N * (kOpen + drv * (1.0 + (B - 1) * kProbe));
+            if (k == n) {
+                step = 0.0;  // charged with the prefix of n-1 vertices
+            } else if (n >= 3 && k + 1 == n) {
+                // u is level n-2; z, the remaining vertex, is the last level
+                const uint32_t z = __builtin_ctzll(full & ~S);
+                const uint64_t zb = nb[z] & S;
+                const uint32_t Bz = (uint32_t)__builtin_popcountll(zb);
+                if (B == 1 && Bz == 1) {
+                    step = EP.N * kTail;
+                } else {
+                    double dz = INFINITY;
+                    for (uint64_t b = zb; b; b &= b - 1) dz = std::min(dz, avg_len(cs, __builtin_ctzll(b), z));
+                    const double Ns = std::max(EP.N * factor, 1e-9);
+                    step += Ns * (Bz == 1 ? kLeafOne : kOpen + dz * (1.0 + (Bz - 1) * kProbe));
+                }
+            }
             if (EP.f + step < E.f) {
                 E.f = EP.f + step;
                 E.last = (int)u;

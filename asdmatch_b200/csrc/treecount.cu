@@ -1,0 +1,280 @@
+// Exact counts of tree-shaped queries without enumeration.
+//
+// Within the candidate space, a map of the query vertices to candidates that
+// sends every query edge to a candidate edge is an embedding unless two
+// distinct query vertices land on the same data vertex.  Two vertices of
+// different labels never do (their candidate sets are disjoint), nor do two
+// adjacent vertices (the data graph has no self loops).  So when no two
+// non-adjacent query vertices share a label, the count of embeddings equals
+// the count of such maps, and for a tree query that count is a bottom-up
+// dynamic program over the candidate-edge lists:
+//     w_u(i) = prod over children c of u of  sum over j in list_{u->c}(i) of  w_c(j)
+//     count  = sum over i of w_root(i)
+// (the reference reaches the same number by enumeration: adaptiveShareJoin
+// with ALL_LEVEL, matching/adaptive.cpp:1179-2279).  Arithmetic is uint64
+// with overflow detection; a query whose program overflows anywhere is left
+// to the enumeration kernels, which report ASDM_ERR_OVERFLOW if its count
+// itself exceeds 2^64 - 1.
+#include <algorithm>
+
+#include "cs.cuh"
+
+namespace asdm {
+namespace {
+
+// One (query, query vertex) of a height level of the programs.
+struct TreeSeg {
+    unsigned long long *w;       // weights of u's candidates (output)
+    uint32_t ncand;              // |C(u)|
+    uint32_t child_first;        // children in the TreeChild array
+    uint32_t nchild;
+    uint32_t query;              // index into counts / flags
+    uint32_t root;               // 1: add the weights into the query's count
+    uint32_t pad;
+    unsigned long long start;    // first item of this segment in the launch
+};
+
+struct TreeChild {
+    const uint32_t *off;              // candidate-edge offsets of (u -> c), by candidate of u
+    const uint32_t *list;             // entries: indices into C(c)
+    const unsigned long long *w;      // weights of c's candidates
+};
+
+// One thread per candidate of the level's query vertices; a list longer than
+// 32 entries is summed by the whole warp.
+__global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsigned long long total,
+                           const TreeChild *__restrict__ kids, unsigned long long *__restrict__ counts,
+                           unsigned int *__restrict__ overflow) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total;
+         base += stride) {
+        const unsigned long long t = base + lane;
+        const bool valid = t < total;
+        TreeSeg sg{};
+        uint32_t i = 0;
+        if (valid) {
+            uint32_t lo = 0, hi = nseg;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (segs[mid].start <= t) lo = mid; else hi = mid;
+            }
+            sg = segs[lo];
+            i = (uint32_t)(t - sg.start);
+        }
+        unsigned long long acc = 1;
+        bool over = false;
+        // children are visited in lock step: k-th child of every lane's segment
+        uint32_t maxk = valid ? sg.nchild : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+        for (uint32_t k = 0; k < maxk; ++k) {
+            const bool mine = valid && k < sg.nchild;
+            uint32_t b = 0, e = 0;
+            const unsigned long long *w = nullptr;
+            const uint32_t *list = nullptr;
+            if (mine) {
+                const TreeChild ch = kids[sg.child_first + k];
+                b = ch.off[i];
+                e = ch.off[i + 1];
+                w = ch.w;
+                list = ch.list;
+            }
+            unsigned long long sum = 0;
+            const bool coop = mine && (e - b) > 32;
+            uint32_t todo = __ballot_sync(0xffffffffu, coop);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+                const unsigned long long *ww =
+                    (const unsigned long long *)__shfl_sync(0xffffffffu, (unsigned long long)w, src);
+                const uint32_t *ll = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)list, src);
+                unsigned long long part = 0;
+                bool pover = false;
+                for (uint32_t x = bb + lane; x < ee; x += 32) {
+                    const unsigned long long v = ww[ll[x]];
+                    pover |= part + v < part;
+                    part += v;
+                }
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    const unsigned long long y = __shfl_xor_sync(0xffffffffu, part, o);
+                    pover |= part + y < part;
+                    part += y;
+                }
+                pover = __any_sync(0xffffffffu, pover);
+                if ((int)lane == src) {
+                    sum = part;
+                    over |= pover;
+                }
+            }
+            if (mine && !coop)
+                for (uint32_t x = b; x < e; ++x) {
+                    const unsigned long long v = w[list[x]];
+                    over |= sum + v < sum;
+                    sum += v;
+                }
+            if (mine) {
+                over |= __umul64hi(acc, sum) != 0;
+                acc *= sum;
+            }
+        }
+        if (!valid) continue;
+        if (over) {
+            atomicOr(&overflow[sg.query], 1u);
+            acc = 0;
+        }
+        sg.w[i] = acc;
+        if (sg.root && acc) {
+            const unsigned long long old = atomicAdd(&counts[sg.query], acc);
+            if (old + acc < old) atomicOr(&overflow[sg.query], 1u);
+        }
+    }
+}
+
+}  // namespace
+
+// A query the program counts exactly: connected tree, no two non-adjacent
+// vertices with one label.
+bool tree_countable(const QueryGraph &q) {
+    if (q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) return false;
+    for (uint32_t u = 0; u < q.n; ++u)
+        for (uint32_t w = u + 1; w < q.n; ++w)
+            if (q.lab[u] == q.lab[w] && q.slot(u, w) < 0) return false;
+    return true;
+}
+
+// Counts every countable query of `cs` (non-empty candidate spaces on graph
+// G); done[i] = 1 and counts[i] set for the queries it settled.
+int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
+                std::vector<char> &done) {
+    cudaStream_t s = G->stream;
+    const uint32_t Q = (uint32_t)cs.size();
+    counts.assign(Q, 0);
+    done.assign(Q, 0);
+    // rooted trees, vertices grouped by height
+    struct Item { uint32_t q, u, parent; };
+    std::vector<std::vector<Item>> by_height;
+    std::vector<uint64_t> qwb(Q, 0);  // per query: first weight
+    uint64_t wtotal = 0;
+    std::vector<uint32_t> take;
+    for (uint32_t qi = 0; qi < Q; ++qi) {
+        const asdm_cs &c = *cs[qi];
+        if (!c.nonempty || !tree_countable(c.q)) continue;
+        const QueryGraph &q = c.q;
+        // root at vertex 0; BFS gives parents, heights from the leaves up
+        std::vector<uint32_t> order{0}, par(q.n, kNone), height(q.n, 0);
+        std::vector<char> seen(q.n, 0);
+        seen[0] = 1;
+        for (size_t k = 0; k < order.size(); ++k)
+            for (uint32_t e = q.off[order[k]]; e < q.off[order[k] + 1]; ++e) {
+                const uint32_t w = q.nbr[e];
+                if (!seen[w]) { seen[w] = 1; par[w] = order[k]; order.push_back(w); }
+            }
+        if (order.size() != q.n) continue;
+        for (size_t k = order.size(); k-- > 1;) height[par[order[k]]] = std::max(height[par[order[k]]], height[order[k]] + 1);
+        qwb[qi] = wtotal;
+        for (uint32_t u = 0; u < q.n; ++u) wtotal += c.ncand[u];
+        for (uint32_t u = 0; u < q.n; ++u) {
+            if (by_height.size() <= height[u]) by_height.resize(height[u] + 1);
+            by_height[height[u]].push_back(Item{qi, u, par[u]});
+        }
+        take.push_back(qi);
+    }
+    if (take.empty()) return ASDM_OK;
+    auto wptr_off = [&](uint32_t qi, uint32_t u) {
+        uint64_t o = qwb[qi];
+        for (uint32_t v = 0; v < u; ++v) o += cs[qi]->ncand[v];
+        return o;
+    };
+    unsigned long long *w = nullptr, *d_counts = nullptr;
+    unsigned int *d_over = nullptr;
+    TreeSeg *d_segs = nullptr;
+    TreeChild *d_kids = nullptr;
+    int rc = ASDM_OK;
+    do {
+        if ((rc = dalloc(&w, wtotal, s)) || (rc = dalloc(&d_counts, Q, s)) || (rc = dalloc(&d_over, Q, s))) break;
+        if (cudaMemsetAsync(d_counts, 0, Q * sizeof(unsigned long long), s) != cudaSuccess ||
+            cudaMemsetAsync(d_over, 0, Q * sizeof(unsigned int), s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "tree-count reset failed");
+            break;
+        }
+        // every level's segments and children, uploaded once
+        std::vector<TreeSeg> segs;
+        std::vector<TreeChild> kids;
+        std::vector<size_t> lvl_first{0};
+        std::vector<unsigned long long> lvl_total;
+        for (size_t h = 0; h < by_height.size(); ++h) {
+            unsigned long long total = 0;
+            for (const Item &it : by_height[h]) {
+                const asdm_cs &c = *cs[it.q];
+                const QueryGraph &q = c.q;
+                TreeSeg sg{};
+                sg.w = w + wptr_off(it.q, it.u);
+                sg.ncand = c.ncand[it.u];
+                sg.child_first = (uint32_t)kids.size();
+                sg.query = it.q;
+                sg.root = it.parent == kNone ? 1u : 0u;
+                sg.start = total;
+                for (uint32_t e = q.off[it.u]; e < q.off[it.u + 1]; ++e) {
+                    const uint32_t ch = q.nbr[e];
+                    if (ch == it.parent) continue;
+                    kids.push_back(TreeChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                             w + wptr_off(it.q, ch)});
+                }
+                sg.nchild = (uint32_t)kids.size() - sg.child_first;
+                total += sg.ncand;
+                segs.push_back(sg);
+            }
+            lvl_first.push_back(segs.size());
+            lvl_total.push_back(total);
+        }
+        if (kids.empty()) kids.push_back(TreeChild{nullptr, nullptr, nullptr});
+        if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s))) break;
+        if (cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(TreeSeg), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(d_kids, kids.data(), kids.size() * sizeof(TreeChild), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "tree-count upload failed");
+            break;
+        }
+        for (size_t h = 0; h < by_height.size() && rc == ASDM_OK; ++h) {
+            const unsigned long long total = lvl_total[h];
+            if (total == 0) continue;
+            const unsigned grid =
+                (unsigned)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)G->num_sms * 32);
+            tree_level<<<grid, 256, 0, s>>>(d_segs + lvl_first[h], (uint32_t)(lvl_first[h + 1] - lvl_first[h]),
+                                            total, d_kids, d_counts, d_over);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "tree-count kernel failed");
+        }
+        if (rc != ASDM_OK) break;
+        std::vector<unsigned long long> hc(Q);
+        std::vector<unsigned int> ho(Q);
+        if (cudaMemcpyAsync(hc.data(), d_counts, Q * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(ho.data(), d_over, Q * sizeof(unsigned int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "tree-count readback failed");
+            break;
+        }
+        for (uint32_t qi : take)
+            if (!ho[qi]) {
+                counts[qi] = hc[qi];
+                done[qi] = 1;
+            }
+    } while (false);
+    dfree(d_segs, s);
+    dfree(d_kids, s);
+    dfree(w, s);
+    dfree(d_counts, s);
+    dfree(d_over, s);
+    if (rc != ASDM_OK) {
+        done.assign(Q, 0);
+        cudaStreamSynchronize(s);
+    }
+    return rc;
+}
+
+}  // namespace asdm

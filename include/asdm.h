@@ -223,6 +223,8 @@ typedef struct asdm_run_stats {
     double kernel_ms;        /* device time of the enumeration kernels          */
     double build_ms;         /* device time of the candidate-space build (K1-K3) */
     uint64_t build_bytes;    /* algorithmic bytes of that build                  */
+    uint64_t tails_lane;     /* last-two-level closed forms evaluated one per lane */
+    uint64_t tails_warp;     /* ... and warp-wide (long intersections)             */
 } asdm_run_stats;
 
 /* Exact enumeration of one query over its candidate space.  Replaces
