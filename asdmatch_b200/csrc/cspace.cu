@@ -476,8 +476,8 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
         if ((rc = dalloc(&d_segs, nseg, s)) || (rc = dalloc(&d_tf, nseg + 1, s)) || (rc = dalloc(&d_cnt, ntiles, s)) ||
             (rc = dalloc(&d_pos, ntiles + 1, s)) || (rc = dalloc(&d_sc, nseg, s)))
             break;
-        if (cudaMemcpyAsync(d_segs, segs.data(), nseg * sizeof(CompDesc), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-            cudaMemcpyAsync(d_tf, tile_first.data(), (nseg + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s) !=
+        if (upload_async(G, d_segs, segs.data(), nseg * sizeof(CompDesc)) != cudaSuccess ||
+            upload_async(G, d_tf, tile_first.data(), (nseg + 1) * sizeof(uint64_t)) !=
                 cudaSuccess ||
             cudaMemsetAsync(d_sc, 0, nseg * sizeof(uint32_t), s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "compaction upload failed");
@@ -552,8 +552,8 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     uint64_t *d_prefix = nullptr;
     ASDM_TRY(dalloc(&d_p, np, s));
     ASDM_TRY(dalloc(&d_prefix, np + 1, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_p, passes.data(), np * sizeof(PassDesc), cudaMemcpyHostToDevice, s));
-    ASDM_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), (np + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    ASDM_CUDA(upload_async(G, d_p, passes.data(), np * sizeof(PassDesc)));
+    ASDM_CUDA(upload_async(G, d_prefix, prefix.data(), (np + 1) * sizeof(uint64_t)));
     uint32_t *keys = nullptr, *order = nullptr;
     int rc = ASDM_OK;
     if (prefix[np] >= (1u << 16) && prefix[np] < 0xFFFFFFFFull) {
@@ -571,8 +571,6 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
         ::asdm::count_launch();
         if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
     }
-    // the host vectors above are read by the copies: wait before they go out of scope
-    if (cudaStreamSynchronize(s) != cudaSuccess && rc == ASDM_OK) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
     dfree(keys, s);
     dfree(order, s);
     dfree(d_p, s);
@@ -582,6 +580,7 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
 
 struct Scratch {
     cudaStream_t s;
+    asdm_graph *G;
     std::vector<void *> ptrs;
     ~Scratch() {
         for (void *p : ptrs) cudaFreeAsync(p, s);
@@ -598,7 +597,7 @@ struct Scratch {
     template <typename T>
     int upload(T **p, const std::vector<T> &h) {
         ASDM_TRY(alloc(p, h.size()));
-        if (!h.empty()) ASDM_CUDA(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+        if (!h.empty()) ASDM_CUDA(upload_async(G, *p, h.data(), h.size() * sizeof(T)));
         return ASDM_OK;
     }
 };
@@ -621,7 +620,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     asdm_graph *G = group[0]->g;
     const DevGraph &g = G->d;
     cudaStream_t s = G->stream;
-    Scratch scr{s, {}};
+    Scratch scr{s, G, {}};
+    // descriptor uploads go through the graph's pinned stage, reused per build
+    ASDM_CUDA(cudaStreamSynchronize(s));
+    G->stage.reset();
     cudaEvent_t ev0, ev1;
     ASDM_CUDA(cudaEventCreate(&ev0));
     ASDM_CUDA(cudaEventCreate(&ev1));

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "internal.h"
@@ -118,6 +119,33 @@ void count_launch();
 
 }  // namespace asdm
 
+// Pinned host memory for descriptor uploads: a copy from pageable memory
+// first waits for the stream, a copy from pinned memory does not.  Memory
+// handed out stays valid until the next reset().
+struct PinnedStage {
+    std::vector<std::pair<uint8_t *, size_t>> chunks;
+    size_t cur = 0, off = 0;
+    void reset() { cur = 0; off = 0; }
+    void *put(const void *src, size_t bytes) {
+        const size_t need = (bytes + 63) & ~size_t(63);
+        while (cur < chunks.size() && off + need > chunks[cur].second) { ++cur; off = 0; }
+        if (cur == chunks.size()) {
+            uint8_t *p = nullptr;
+            const size_t sz = std::max<size_t>(need, 4u << 20);
+            if (cudaMallocHost((void **)&p, sz) != cudaSuccess) return nullptr;
+            chunks.emplace_back(p, sz);
+            off = 0;
+        }
+        uint8_t *dst = chunks[cur].first + off;
+        if (bytes) std::memcpy(dst, src, bytes);
+        off += need;
+        return dst;
+    }
+    ~PinnedStage() {
+        for (auto &c : chunks) cudaFreeHost(c.first);
+    }
+};
+
 struct asdm_graph {
     asdm_tuning tuning{1, 96, ASDM_PLANNER_DP, 64};             // enumeration kernel knobs (asdm_graph_set_tuning)
     int device = 0;
@@ -127,4 +155,15 @@ struct asdm_graph {
     uint32_t *buf = nullptr;               // one allocation backing every DevGraph array
     std::vector<uint32_t> h_vbl_off;       // host copy of the label offsets
     uint32_t max_deg = 0;
+    PinnedStage stage;                     // descriptor uploads of the candidate-space build
 };
+
+namespace asdm {
+// Host-to-device copy on the graph's stream through its pinned stage (a plain
+// copy when pinned memory is not available).
+inline cudaError_t upload_async(asdm_graph *G, void *dst, const void *src, size_t bytes) {
+    if (!bytes) return cudaSuccess;
+    const void *p = G->stage.put(src, bytes);
+    return cudaMemcpyAsync(dst, p ? p : src, bytes, cudaMemcpyHostToDevice, G->stream);
+}
+}  // namespace asdm

@@ -105,6 +105,7 @@ struct EnumArgs {
     uint32_t tail;
     unsigned long long *qcycles;  // batches, optional: SM cycles warps spent on each query
     const uint32_t *xmap_a, *xmap_z;
+    unsigned long long *lw;       // LOCAL mode: leaf weights (see Warp::lw)
 };
 
 struct QDesc {
@@ -119,6 +120,7 @@ struct QDesc {
     // lane tails at level d = n-3: index in C(u_{n-2}) / C(u_{n-1}) of each
     // candidate of level d, where level d is a conflict of that level (or null)
     const uint32_t *xmap_a, *xmap_z;
+    unsigned long long *lw;  // LOCAL mode: leaf weights (or null)
 };
 
 // The last two levels of a COUNT-mode plan are counted in closed form when
@@ -205,13 +207,17 @@ struct Warp {
     const uint32_t *rev_off, *rev_list;  // kTailChain: candidate edges last level -> level n-2
     uint32_t tail;                       // kTail* of the current query
     const uint32_t *xmap_a, *xmap_z;     // cross indices for lane tails (or null)
+    // LOCAL mode with a one-list last level: per candidate of the list's
+    // source level, how many prefixes counted that candidate's whole list;
+    // a pass after the kernel adds them to the last level's local counts
+    unsigned long long *lw;
 
     // w: this warp's shared-memory words, laid out for queries of up to maxn
     // levels and maxnb backward edges.
     __device__ Warp(const EnumArgs &args, const DLevel *l, const DBack *b, const uint32_t *cf, uint32_t *w, uint32_t ln,
                     uint32_t levels, uint32_t maxn, uint32_t maxnb)
         : a(args), L(l), B(b), CF(cf), lane(ln), n(levels), local(args.local), ps(args.ps), rev_off(args.rev_off),
-          rev_list(args.rev_list), tail(args.tail), xmap_a(args.xmap_a), xmap_z(args.xmap_z) {
+          rev_list(args.rev_list), tail(args.tail), xmap_a(args.xmap_a), xmap_z(args.xmap_z), lw(args.lw) {
         idx = w;
         vid = idx + maxn;
         buf = vid + maxn;
@@ -245,6 +251,7 @@ struct Warp {
         tail = d.tail;
         xmap_a = d.xmap_a;
         xmap_z = d.xmap_z;
+        lw = d.lw;
     }
 
     __device__ __forceinline__ bool closed_at(uint32_t d) const {
@@ -952,6 +959,24 @@ struct Warp {
                 }
                 total -= __popc(__ballot_sync(kFull, present));
             }
+        } else if (MODE == ASDM_MODE_LOCAL && lw && lv.nback == 1 && lo == 0 && hi == slen[dslot]) {
+            // the whole list of one candidate: one weight for the pass after
+            // the kernel, minus the same-label earlier vertices lying in it
+            total = hi - lo;
+            bool present = false;
+            uint32_t v = 0;
+            if (lane < lv.nconf) {
+                v = vid[CF[lv.conf_first + lane]];
+                const uint32_t y = lower_bound_u32(lv.cand, lv.ncand, v);
+                if (y < lv.ncand && lv.cand[y] == v) {
+                    const uint32_t q = lower_bound_u32(dl, hi, y);
+                    present = q < hi && dl[q] == y;
+                }
+            }
+            if (present) atomicAdd(&local[(unsigned long long)v * n + lv.u], ~0ull);  // -1
+            total -= __popc(__ballot_sync(kFull, present));
+            if (lane == 0) atomicAdd(&lw[idx[B[dslot].level]], 1ull);
+            if (total && lane < d) atomicAdd(&local[(unsigned long long)vid[lane] * n + L[lane].u], total);
         } else {
             for (uint32_t p0 = lo; p0 < hi; p0 += 32) {
                 const uint32_t p = p0 + lane;
@@ -1230,6 +1255,7 @@ __global__ void __launch_bounds__(kThreads, MINB) enum_batch_kernel(EnumArgs a) 
     W.tail = d0.tail;
     W.xmap_a = d0.xmap_a;
     W.xmap_z = d0.xmap_z;
+    W.lw = d0.lw;
     warp_loop<MODE, true>(a, W, lane);
 }
 
@@ -1254,6 +1280,98 @@ __global__ void tail_lens(const TailSeg *__restrict__ seg, uint32_t nseg, unsign
         const uint32_t x = seg[lo].list[t - seg[lo].start];
         lens[t] = seg[lo].off2[x + 1] - seg[lo].off2[x];
     }
+}
+
+// LOCAL mode: the last level's local counts from the leaf weights.  Segment
+// k covers the candidates of one query's leaf source level: weight w[i] is
+// added to every last-level candidate in list(i).
+struct PushSeg {
+    const unsigned long long *w;
+    const uint32_t *off;          // candidate-edge offsets (source level -> last level)
+    const uint32_t *list;         // entries: indices into C(u_last)
+    const uint32_t *cand;         // C(u_last)
+    unsigned long long *local;    // |Vg| x n block of the query
+    uint32_t n, u;                // query size, last query vertex
+    unsigned long long start, len;
+};
+
+__global__ void push_leaf(const PushSeg *__restrict__ seg, uint32_t nseg, unsigned long long total) {
+    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (seg[mid].start <= t) lo = mid; else hi = mid;
+        }
+        const PushSeg sg = seg[lo];
+        const unsigned long long i = t - sg.start;
+        const unsigned long long c = sg.w[i];
+        if (!c) continue;
+        for (uint32_t k = sg.off[i]; k < sg.off[i + 1]; ++k)
+            atomicAdd(&sg.local[(unsigned long long)sg.cand[sg.list[k]] * sg.n + sg.u], c);
+    }
+}
+
+// Leaf weights of LOCAL-mode plans whose last level has one backward edge:
+// one zeroed device array (*d_w, the caller frees), per plan a pointer or null.
+int leaf_weights(const std::vector<const asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                 std::vector<unsigned long long *> &lw, unsigned long long **d_w, cudaStream_t s) {
+    *d_w = nullptr;
+    lw.assign(cs.size(), nullptr);
+    std::vector<uint64_t> at(cs.size(), 0);
+    uint64_t total = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+        const asdm_plan &p = *plans[i];
+        const size_t n = p.order.size();
+        if (n < 2 || n != cs[i]->q.n || p.back[n - 1].size() != 1) continue;
+        at[i] = total;
+        total += cs[i]->ncand[p.order[p.back[n - 1][0].first]];
+        lw[i] = reinterpret_cast<unsigned long long *>(1);  // marker until the array exists
+    }
+    if (total == 0) {
+        lw.assign(cs.size(), nullptr);
+        return ASDM_OK;
+    }
+    ASDM_TRY(dalloc(d_w, total, s));
+    ASDM_CUDA(cudaMemsetAsync(*d_w, 0, total * sizeof(unsigned long long), s));
+    for (size_t i = 0; i < cs.size(); ++i)
+        if (lw[i]) lw[i] = *d_w + at[i];
+    return ASDM_OK;
+}
+
+// The pass after the kernel for those plans (local blocks as given).
+int push_leaf_weights(const std::vector<const asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                      const std::vector<unsigned long long *> &lw, const std::vector<unsigned long long *> &local,
+                      int num_sms, cudaStream_t s) {
+    std::vector<PushSeg> segs;
+    unsigned long long total = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+        if (!lw[i]) continue;
+        const asdm_cs &c = *cs[i];
+        const asdm_plan &p = *plans[i];
+        const size_t n = p.order.size();
+        const uint32_t e = p.back[n - 1][0].second;
+        const uint32_t src = p.order[p.back[n - 1][0].first], ul = p.order[n - 1];
+        PushSeg sg{lw[i], c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e], c.d_cand + c.cand_base[ul],
+                   local[i], (uint32_t)n, ul, total, c.ncand[src]};
+        segs.push_back(sg);
+        total += c.ncand[src];
+    }
+    if (segs.empty() || total == 0) return ASDM_OK;
+    PushSeg *d_seg = nullptr;
+    ASDM_TRY(dalloc(&d_seg, segs.size(), s));
+    int rc = ASDM_OK;
+    if (cudaMemcpyAsync(d_seg, segs.data(), segs.size() * sizeof(PushSeg), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        rc = fail(ASDM_ERR_CUDA, "leaf-weight upload failed");
+    } else {
+        const unsigned grid = (unsigned)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)num_sms * 32);
+        push_leaf<<<grid, 256, 0, s>>>(d_seg, (uint32_t)segs.size(), total);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "leaf-weight pass failed");
+    }
+    cudaStreamSynchronize(s);  // the upload reads a host vector
+    dfree(d_seg, s);
+    return rc;
 }
 
 // Cross indices: for candidate i of one query vertex, its index in the
@@ -1523,10 +1641,12 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     uint8_t *d_plan = nullptr;
     unsigned long long *d_ctr = nullptr, *d_local = nullptr, *d_ps = nullptr;
     uint32_t *d_rows = nullptr, *d_queue = nullptr, *d_xmap = nullptr;
+    unsigned long long *d_lw = nullptr;
     int rc = ASDM_OK;
     auto cleanup = [&]() {
         dfree(d_ps, s);
         dfree(d_xmap, s);
+        dfree(d_lw, s);
         dfree(d_plan, s);
         dfree(d_ctr, s);
         dfree(d_local, s);
@@ -1592,6 +1712,11 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
             a.xmap_a = td[0].xmap_a;
             a.xmap_z = td[0].xmap_z;
         }
+        if (mode == ASDM_MODE_LOCAL) {
+            std::vector<unsigned long long *> lwv;
+            if ((rc = leaf_weights({&cs}, {&plan}, lwv, &d_lw, s))) break;
+            a.lw = lwv[0];
+        }
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -1630,6 +1755,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         if (flags & kFlagOverflow) { rc = fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1"); break; }
         if (flags & kFlagTimeout) { rc = fail(ASDM_ERR_TIMEOUT, "time limit reached"); break; }
         if (flags & kFlagLimit) { rc = fail(ASDM_ERR_LIMIT, "count limit reached"); break; }
+        if (a.lw && (rc = push_leaf_weights({&cs}, {&plan}, {a.lw}, {d_local}, G->num_sms, s))) break;
         if ((mode & ASDM_MODE_LOCAL) && opt.local_counts) {
             if (cudaMemcpyAsync(opt.local_counts, d_local, local_n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 s) != cudaSuccess ||
@@ -1788,6 +1914,8 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     uint8_t *d_buf = nullptr;
     unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr, *d_cyc = nullptr;
     uint32_t *d_queue = nullptr, *d_xmap = nullptr;
+    unsigned long long *d_lw = nullptr;
+    std::vector<unsigned long long *> lwv;
     unsigned int *d_qflags = nullptr;
     int rc = ASDM_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1825,6 +1953,16 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
                 qd[li].xmap_a = td[li].xmap_a;
                 qd[li].xmap_z = td[li].xmap_z;
             }
+        }
+        if (local_mode) {
+            std::vector<const asdm_cs *> tcs(L);
+            std::vector<const asdm_plan *> tpl(L);
+            for (uint32_t li = 0; li < L; ++li) {
+                tcs[li] = cs[live[li]];
+                tpl[li] = plans[live[li]];
+            }
+            if ((rc = leaf_weights(tcs, tpl, lwv, &d_lw, s))) break;
+            for (uint32_t li = 0; li < L; ++li) qd[li].lw = lwv[li];
         }
         for (uint32_t li = 0; li < L; ++li) {
             qd[li].lv = reinterpret_cast<const DLevel *>(d_buf + offs[li].lv);
@@ -1943,6 +2081,17 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         }
         if (gflags & kFlagInternal) rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
         else if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
+        if (rc == ASDM_OK && local_mode && d_lw) {
+            std::vector<const asdm_cs *> tcs(L);
+            std::vector<const asdm_plan *> tpl(L);
+            std::vector<unsigned long long *> blocks(L);
+            for (uint32_t li = 0; li < L; ++li) {
+                tcs[li] = cs[live[li]];
+                tpl[li] = plans[live[li]];
+                blocks[li] = d_local + local_base[li];
+            }
+            rc = push_leaf_weights(tcs, tpl, lwv, blocks, G->num_sms, s);
+        }
         if (rc == ASDM_OK && local_mode) {
             for (uint32_t li = 0; li < L && rc == ASDM_OK; ++li)
                 if (local_out[live[li]] &&
@@ -1957,6 +2106,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     if (e1) cudaEventDestroy(e1);
     dfree(d_ps, s);
     dfree(d_xmap, s);
+    dfree(d_lw, s);
     dfree(d_cyc, s);
     dfree(d_buf, s);
     dfree(d_ctr, s);
