@@ -35,7 +35,7 @@ namespace asdm {
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
 bool tree_countable(const QueryGraph &q);
 int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
-                std::vector<char> &done);
+                std::vector<char> &done, const std::vector<unsigned long long *> *local = nullptr);
 
 namespace {
 
@@ -579,6 +579,12 @@ struct Warp {
         return MODE == ASDM_MODE_COUNT && L[n - 1].nback <= kLaneLeafLists;
     }
 
+    // LOCAL mode with a one-list last level and leaf weights: the last level
+    // of every level-(n-2) survivor is handled by its lane
+    __device__ __forceinline__ bool local_leaf_ok() const {
+        return MODE == ASDM_MODE_LOCAL && lw && L[n - 1].nback == 1;
+    }
+
     // For the level before the last: the candidate index in C(u_last) of every
     // earlier vertex the last level must avoid (kNone when it is not a
     // candidate there, kSelf when it is level d's own vertex).
@@ -880,6 +886,42 @@ struct Warp {
             }
             add_count(c);
             elems += touched;
+        } else if (d + 2 == n && local_leaf_ok()) {
+            // LOCAL: every survivor's last level by its lane: its count (list
+            // length minus the same-label earlier vertices lying in it), its
+            // own local count, a leaf weight for the pass after the kernel
+            // (which adds 1 to every list entry; the conflict vertices in the
+            // list are taken back out here)
+            unsigned long long c = 0;
+            if (ok) {
+                const DLevel lvL = L[n - 1];
+                const DBack bk = B[lvL.back_first];
+                const uint32_t ij = bk.level == d ? x : idx[bk.level];
+                const uint32_t a0 = bk.off[ij], a1 = bk.off[ij + 1];
+                c = a1 - a0;
+                for (uint32_t k = 0; k < lvL.nconf && c; ++k) {
+                    uint32_t y = fidx[k];
+                    if (y == kSelf) {
+                        const uint32_t v = lv.cand[x];
+                        y = lower_bound_u32(lvL.cand, lvL.ncand, v);
+                        if (y >= lvL.ncand || lvL.cand[y] != v) y = kNone;
+                    }
+                    if (y == kNone) continue;
+                    const uint32_t q = lower_bound_u32(bk.list + a0, a1 - a0, y);
+                    if (q < a1 - a0 && bk.list[a0 + q] == y) {
+                        --c;
+                        atomicAdd(&local[(unsigned long long)lvL.cand[y] * n + lvL.u], ~0ull);  // -1
+                    }
+                }
+                if (a1 > a0) atomicAdd(&lw[ij], 1ull);
+                if (c) atomicAdd(&local[(unsigned long long)lv.cand[x] * n + lv.u], c);
+                elems += 2;
+            }
+            ok = false;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+            if (c && lane < d) atomicAdd(&local[(unsigned long long)vid[lane] * n + L[lane].u], c);
+            add_count(c);
         } else if (d + 3 == n && lane_tail_ok(d)) {
             // the last two levels of every entry lane-parallel; entries whose
             // intersections are long stay buffered for the warp-wide tail
@@ -1063,7 +1105,7 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
                 --d;
             } else if (len == 0) {
                 --d;
-            } else if (d + 2 == n && W.lane_leaf_ok()) {
+            } else if (d + 2 == n && (W.lane_leaf_ok() || W.local_leaf_ok())) {
                 W.prepare_lane_leaf(d);
             } else if (W.lane_tail_ok(d)) {
                 W.prepare_lane_tail(d);
@@ -1109,7 +1151,7 @@ __device__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
         if (hi > lo) W.leaf(s);
         return true;
     }
-    if (s + 2 == W.n && W.lane_leaf_ok()) W.prepare_lane_leaf(s);
+    if (s + 2 == W.n && (W.lane_leaf_ok() || W.local_leaf_ok())) W.prepare_lane_leaf(s);
     else if (W.lane_tail_ok(s)) W.prepare_lane_tail(s);
     return dfs(a, W, lane, s, iter, deadline);
 }
@@ -1589,6 +1631,42 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
     if (opt.local_counts && (mode & ASDM_MODE_LOCAL))
         std::fill(opt.local_counts, opt.local_counts + (uint64_t)G->d.n * n, 0ull);
     if (!cs.nonempty) return ASDM_OK;
+    if (mode == ASDM_MODE_LOCAL && opt.local_counts && plan.order.size() == n && tree_countable(q)) {
+        // conflict-free tree: counts and local counts from the tree program
+        const uint64_t local_n = (uint64_t)G->d.n * n;
+        unsigned long long *blk = nullptr;
+        ASDM_TRY(dalloc(&blk, local_n, s));
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, s);
+        std::vector<uint64_t> tc;
+        std::vector<char> done;
+        std::vector<unsigned long long *> blocks{blk};
+        int trc = cudaMemsetAsync(blk, 0, local_n * sizeof(unsigned long long), s) == cudaSuccess
+                      ? tree_counts(G, {&cs}, tc, done, &blocks)
+                      : fail(ASDM_ERR_CUDA, "local-count reset failed");
+        cudaEventRecord(t1, s);
+        cudaEventSynchronize(t1);
+        float tms = 0.f;
+        cudaEventElapsedTime(&tms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (trc == ASDM_OK && done[0] &&
+            (cudaMemcpyAsync(opt.local_counts, blk, local_n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) !=
+                 cudaSuccess ||
+             cudaStreamSynchronize(s) != cudaSuccess))
+            trc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+        dfree(blk, s);
+        cudaStreamSynchronize(s);
+        if (trc != ASDM_OK) return trc;
+        if (done[0]) {
+            st.count = tc[0];
+            st.kernel_ms = tms;
+            if (opt.count_limit && st.count > opt.count_limit) return fail(ASDM_ERR_LIMIT, "count limit reached");
+            return ASDM_OK;
+        }
+    }
     if (mode == ASDM_MODE_COUNT && plan.order.size() == n && tree_countable(q)) {
         // conflict-free tree: the tree program counts it (the enumeration
         // below only when the program overflows)
@@ -1815,9 +1893,73 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     }
     if (agg) *agg = asdm_run_stats{};
     if (live.empty()) return ASDM_OK;
-    // COUNT mode: conflict-free tree queries are counted by the tree program
-    // (full plans only; prefix plans count partial matches)
+    // conflict-free tree queries are counted by the tree program (full plans
+    // only; prefix plans count partial matches); in LOCAL mode with their
+    // local counts, a few queries at a time
     float tree_ms = 0.f;
+    if (local_out) {
+        std::vector<uint32_t> tid;
+        for (uint32_t i : live)
+            if (plans[i]->order.size() == cs[i]->q.n && tree_countable(cs[i]->q)) tid.push_back(i);
+        std::vector<char> settled(Q, 0);
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, s);
+        int trc = ASDM_OK;
+        for (size_t at = 0; at < tid.size() && trc == ASDM_OK;) {
+            // up to 2 GiB of local-count blocks per round
+            std::vector<asdm_cs *> tcs;
+            std::vector<uint32_t> ids;
+            uint64_t words = 0;
+            for (; at < tid.size(); ++at) {
+                const uint64_t need = (uint64_t)G->d.n * cs[tid[at]]->q.n;
+                if (!ids.empty() && words + need > (1ull << 28)) break;
+                tcs.push_back(cs[tid[at]]);
+                ids.push_back(tid[at]);
+                words += need;
+            }
+            unsigned long long *blk = nullptr;
+            if ((trc = dalloc(&blk, words, s))) break;
+            std::vector<unsigned long long *> blocks;
+            uint64_t o = 0;
+            for (uint32_t i : ids) {
+                blocks.push_back(blk + o);
+                o += (uint64_t)G->d.n * cs[i]->q.n;
+            }
+            std::vector<uint64_t> tc;
+            std::vector<char> done;
+            trc = cudaMemsetAsync(blk, 0, words * sizeof(unsigned long long), s) == cudaSuccess
+                      ? tree_counts(G, tcs, tc, done, &blocks)
+                      : fail(ASDM_ERR_CUDA, "local-count reset failed");
+            for (size_t k = 0; k < ids.size() && trc == ASDM_OK; ++k) {
+                if (!done[k]) continue;
+                const uint32_t i = ids[k];
+                if (local_out[i] &&
+                    cudaMemcpyAsync(local_out[i], blocks[k], (uint64_t)G->d.n * cs[i]->q.n * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, s) != cudaSuccess)
+                    trc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+                settled[i] = 1;
+                counts[i] = tc[k];
+                if (count_limit && tc[k] > count_limit) status[i] = ASDM_ERR_LIMIT;
+                if (agg) agg->count += tc[k];
+            }
+            if (cudaStreamSynchronize(s) != cudaSuccess && trc == ASDM_OK) trc = fail(ASDM_ERR_CUDA, "local-count readback failed");
+            dfree(blk, s);
+        }
+        cudaEventRecord(t1, s);
+        cudaEventSynchronize(t1);
+        cudaEventElapsedTime(&tree_ms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (trc != ASDM_OK) return trc;
+        std::vector<uint32_t> rest;
+        for (uint32_t i : live)
+            if (!settled[i]) rest.push_back(i);
+        live.swap(rest);
+        if (agg) agg->kernel_ms += tree_ms;
+        if (live.empty()) return ASDM_OK;
+    }
     if (!local_out) {
         std::vector<asdm_cs *> tcs;
         std::vector<uint32_t> tid;

@@ -65,3 +65,31 @@ def test_tree_program_on_denser_trees_against_oracle(c0d_files, dg_c0d, tmp_path
         assert A.match(dg_c0d, q).count == want
         loc = A.match(dg_c0d, q, mode=A.MODE_LOCAL)
         assert int(loc.local_counts[:, 0].sum()) == want
+
+
+def _csv_matrix(path, n):
+    rows = [list(map(int, line.split(","))) for line in open(path) if line.strip()]
+    return np.asarray(rows, dtype=np.uint64).reshape(-1, n)
+
+
+def test_tree_program_local_counts_against_oracle_csv(c0d_files, dg_c0d, tmp_path):
+    g, dpath, _ = c0d_files
+    trees = []
+    for seed in range(30000, 34000):
+        q = g.random_walk_query(4 + seed % 4, seed, 2)
+        if conflict_free_tree(q):
+            trees.append(q)
+        if len(trees) == 10:
+            break
+    assert len(trees) >= 6
+    counts, status, mats = A.run_batch_local(dg_c0d, trees)
+    assert status.tolist() == [0] * len(trees)
+    for q, c, m in zip(trees, counts.tolist(), mats):
+        qp, csv = str(tmp_path / "q.graph"), str(tmp_path / "l.csv")
+        q.write(qp)
+        want, _ = O.oracle_run(qp, dpath, O.MODE_LOCAL, csv=csv)
+        assert c == want
+        ref = _csv_matrix(csv, q.n)
+        assert np.array_equal(m, ref)
+        single = A.match(dg_c0d, q, mode=A.MODE_LOCAL)
+        assert single.count == want and np.array_equal(single.local_counts, ref)
