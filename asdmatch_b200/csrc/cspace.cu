@@ -326,12 +326,15 @@ __device__ __forceinline__ uint32_t cand_index(const uint32_t *cb, const uint32_
     return (w & bit) ? cp[r >> 5] + (uint32_t)__popc(w & (bit - 1u)) : kNone;
 }
 
+// rstart (optional): each item's label-run start, its length in cnt (read
+// before cnt is overwritten with the count), both written by k3_bound.
 template <bool kFill>
 __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
                                                    const uint32_t *__restrict__ order,
                                                    uint32_t *__restrict__ cnt, const uint64_t *__restrict__ wpos,
-                                                   uint32_t *__restrict__ elist, unsigned long long *__restrict__ elems) {
+                                                   uint32_t *__restrict__ elist, unsigned long long *__restrict__ elems,
+                                                   const uint32_t *__restrict__ rstart) {
     const uint64_t total = item_base[nedges];
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -344,8 +347,13 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
         if (pos < total) {
             const uint32_t ei = find_segment(item_base, nedges, item);
             const EdgeDesc d = edges[ei];
-            const uint32_t i = (uint32_t)(item - item_base[ei]);
-            if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
+            if (rstart) {
+                b = rstart[item];
+                e = b + cnt[item];
+            } else {
+                const uint32_t i = (uint32_t)(item - item_base[ei]);
+                if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
+            }
             cb = d.cbits;
             cp = d.cpre;
         }
@@ -392,7 +400,8 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
 // Upper bound of every item's list: the length of the candidate's label run.
 __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
-                                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ub) {
+                                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ub,
+                                                   uint32_t *__restrict__ rstart) {
     const uint64_t total = item_base[nedges];
     for (uint64_t pos = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
          pos += (uint64_t)gridDim.x * blockDim.x) {
@@ -403,6 +412,7 @@ __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *_
         uint32_t b = 0, e = 0;
         if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
         ub[item] = e - b;
+        if (rstart) rstart[item] = b;
     }
 }
 
@@ -904,7 +914,9 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         // side in the CSR (grouping by vertex block across edges measured slower)
         const uint32_t *order = nullptr;
         ASDM_TRY(scr.alloc(&d_upos, nitems + 1));
-        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff);
+        uint32_t *rstart = nullptr;
+        ASDM_TRY(scr.alloc(&rstart, nitems));
+        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, rstart);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
         ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
@@ -914,7 +926,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             uint32_t *padded = nullptr;
             ASDM_TRY(scr.alloc(&padded, bound));
             k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, d_upos, padded,
-                                                    d_elems + 1);
+                                                    d_elems + 1, rstart);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
             ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
@@ -927,7 +939,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ASDM_CUDA(cudaGetLastError());
         } else {
             k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, nullptr, nullptr,
-                                                    d_elems + 1);
+                                                    d_elems + 1, nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
             ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
@@ -935,7 +947,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ASDM_CUDA(cudaStreamSynchronize(s));
             ASDM_TRY(dalloc(&arena->d_elist, total, s));
             k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, nullptr, d_wpos, arena->d_elist,
-                                                    nullptr);
+                                                    nullptr, nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         }
