@@ -37,7 +37,7 @@ struct TreeSeg {
 struct TreeChild {
     const uint32_t *off;              // candidate-edge offsets of (u -> c), by candidate of u
     const uint32_t *list;             // entries: indices into C(c)
-    const unsigned long long *w;      // weights of c's candidates
+    const unsigned long long *w;      // weights of c's candidates (null for a leaf: all 1)
     unsigned long long *s_out;        // local counts: the sum over the list, by candidate of u (or null)
 };
 
@@ -54,7 +54,7 @@ struct UpSeg {
 
 // local[v][u] = w_u(i) * up_u(i) for v = C(u)[i]
 struct LocSeg {
-    const unsigned long long *w, *up;   // up null at the root
+    const unsigned long long *w, *up;   // w null at a leaf, up null at the root
     const uint32_t *cand;
     unsigned long long *local;          // |Vg| x n block of the query
     uint32_t n, u, query, ncand;
@@ -101,8 +101,9 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                 w = ch.w;
                 list = ch.list;
             }
-            unsigned long long sum = 0;
-            const bool coop = mine && (e - b) > 32;
+            // a leaf child contributes its list length
+            unsigned long long sum = (mine && !w) ? (unsigned long long)(e - b) : 0ull;
+            const bool coop = mine && w && (e - b) > 32;
             uint32_t todo = __ballot_sync(0xffffffffu, coop);
             while (todo) {
                 const int src = __ffs(todo) - 1;
@@ -130,7 +131,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                     over |= pover;
                 }
             }
-            if (mine && !coop)
+            if (mine && w && !coop)
                 for (uint32_t x = b; x < e; ++x) {
                     const unsigned long long v = w[list[x]];
                     over |= sum + v < sum;
@@ -201,7 +202,7 @@ __global__ void tree_local(const LocSeg *__restrict__ segs, uint32_t nseg, unsig
          t += (unsigned long long)gridDim.x * blockDim.x) {
         const LocSeg sg = segs[seg_of(&segs[0].start, sizeof(LocSeg), nseg, t)];
         const uint32_t i = (uint32_t)(t - sg.start);
-        const unsigned long long a = sg.w[i], b = sg.up ? sg.up[i] : 1ull;
+        const unsigned long long a = sg.w ? sg.w[i] : 1ull, b = sg.up ? sg.up[i] : 1ull;
         if (__umul64hi(a, b) != 0) atomicOr(&overflow[sg.query], 1u);
         sg.local[(unsigned long long)sg.cand[i] * sg.n + sg.u] = a * b;
     }
@@ -328,8 +329,9 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
                 for (uint32_t e = q.off[it.u]; e < q.off[it.u + 1]; ++e) {
                     const uint32_t ch = q.nbr[e];
                     if (ch == it.parent) continue;
+                    const bool leaf = q.deg(ch) == 1;
                     kids.push_back(TreeChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
-                                             w + wptr_off(it.q, ch), local ? s_of(it.q, ch) : nullptr});
+                                             leaf ? nullptr : w + wptr_off(it.q, ch), local ? s_of(it.q, ch) : nullptr});
                 }
                 sg.nchild = (uint32_t)kids.size() - sg.child_first;
                 total += sg.ncand;
@@ -347,7 +349,7 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
             rc = fail(ASDM_ERR_CUDA, "tree-count upload failed");
             break;
         }
-        for (size_t h = 0; h < by_height.size() && rc == ASDM_OK; ++h) {
+        for (size_t h = 1; h < by_height.size() && rc == ASDM_OK; ++h) {  // leaves (height 0) weigh 1
             const unsigned long long total = lvl_total[h];
             if (total == 0) continue;
             const unsigned grid =
@@ -399,7 +401,7 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
                 const asdm_cs &c = *cs[qi];
                 for (uint32_t u = 0; u < c.q.n; ++u) {
                     const bool root = parent[qi][u] == kNone;
-                    LocSeg ls{w + wptr_off(qi, u), root ? nullptr : up + wptr_off(qi, u),
+                    LocSeg ls{(c.q.deg(u) == 1 && !root) ? nullptr : w + wptr_off(qi, u), root ? nullptr : up + wptr_off(qi, u),
                               c.d_cand + c.cand_base[u], (*local)[qi], c.q.n, u, qi, c.ncand[u], ltotal};
                     ltotal += c.ncand[u];
                     locs.push_back(ls);
