@@ -34,6 +34,7 @@ namespace asdm {
 
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
 bool tree_countable(const QueryGraph &q);
+bool tree_countable_conflicts(const QueryGraph &q);
 int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
                 std::vector<char> &done, const std::vector<unsigned long long *> *local = nullptr);
 
@@ -130,7 +131,9 @@ struct QDesc {
 // the reverse candidate edges last level -> level n-2), kTailLeaf when it
 // comes from an earlier level (the last level's list is then fixed by the
 // prefix).
-enum : uint32_t { kTailNone = 0, kTailChain = 1, kTailLeaf = 2 };
+// kTailIsect: level n-2 has two backward edges (a cycle closed there) and
+// the last level one; only the lane-parallel form at level n-3 handles it.
+enum : uint32_t { kTailNone = 0, kTailChain = 1, kTailLeaf = 2, kTailIsect = 3 };
 
 __host__ __device__ constexpr uint32_t warp_words(uint32_t n, uint32_t nb) { return 39 * n + 3 * nb + 96; }
 
@@ -255,7 +258,7 @@ struct Warp {
     }
 
     __device__ __forceinline__ bool closed_at(uint32_t d) const {
-        return MODE == ASDM_MODE_COUNT && tail != kTailNone && d + 2 == n;
+        return MODE == ASDM_MODE_COUNT && (tail == kTailChain || tail == kTailLeaf) && d + 2 == n;
     }
 
     // |a ∩ b| of two ascending lists, warp-wide: each lane looks up entries
@@ -359,6 +362,79 @@ struct Warp {
         return hits;
     }
 
+    // kTailIsect for one level-d entry x (d = n-3), by this lane alone: D = the intersection of level d+1's
+    // two lists, then per survivor y the last level: |list(y)| minus the
+    // conflict vertices in it (the last level's edge from level d+1), or the
+    // fixed list's length minus its conflict vertices and y's own vertex
+    // (edge from an earlier level).  Entries of D that are level-(d+1)
+    // conflicts are skipped.
+    __device__ bool lane_tail_isect(uint32_t d, uint32_t x, const uint32_t *ya, const uint32_t *yz, bool self,
+                                    unsigned long long &out, unsigned long long &touched) {
+        const uint32_t a = d + 1;
+        const DLevel La = L[a], Lz = L[a + 1];
+        const DBack b1 = B[La.back_first], b2 = B[La.back_first + 1], bz = B[Lz.back_first];
+        const uint32_t i1 = b1.level == d ? x : idx[b1.level], i2 = b2.level == d ? x : idx[b2.level];
+        const uint32_t *l1 = b1.list + b1.off[i1], *l2 = b2.list + b2.off[i2];
+        uint32_t n1 = b1.off[i1 + 1] - b1.off[i1], n2 = b2.off[i2 + 1] - b2.off[i2];
+        if (n1 > n2) {
+            const uint32_t *t = l1; l1 = l2; l2 = t;
+            const uint32_t tn = n1; n1 = n2; n2 = tn;
+        }
+        if (n1 > kLaneTailWork) return false;
+        const bool chain = bz.level == a;
+        const uint32_t *LL = nullptr;
+        uint32_t nl = 0, m = 0;
+        if (!chain) {
+            const uint32_t ijz = bz.level == d ? x : idx[bz.level];
+            LL = bz.list + bz.off[ijz];
+            nl = bz.off[ijz + 1] - bz.off[ijz];
+#pragma unroll
+            for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                if (yz[k] == kNone) continue;
+                const uint32_t q = lower_bound_u32(LL, nl, yz[k]);
+                m += q < nl && LL[q] == yz[k];
+            }
+        }
+        unsigned long long sum = 0;
+        uint32_t cur = 0;
+        for (uint32_t i = 0; i < n1 && cur < n2; ++i) {
+            const uint32_t y = l1[i];
+            cur = gallop_lb(l2, cur, n2, y);
+            if (cur >= n2 || l2[cur] != y) continue;
+            bool excl = false;
+#pragma unroll
+            for (uint32_t k = 0; k < kLaneTailConf; ++k) excl |= ya[k] == y;
+            if (excl) continue;
+            if (chain) {
+                const uint32_t a0 = bz.off[y], a1 = bz.off[y + 1];
+                unsigned long long c = a1 - a0;
+#pragma unroll
+                for (uint32_t k = 0; k < kLaneTailConf; ++k) {
+                    if (yz[k] == kNone) continue;
+                    const uint32_t q = lower_bound_u32(bz.list + a0, a1 - a0, yz[k]);
+                    c -= (q < a1 - a0 && bz.list[a0 + q] == yz[k]) ? 1ull : 0ull;
+                }
+                sum += c;
+            } else {
+                unsigned long long c = nl - m;
+                if (self) {
+                    // y's own vertex in the fixed list
+                    const uint32_t v = La.cand[y];
+                    uint32_t l2i = 0, h2 = nl;
+                    while (l2i < h2) {
+                        const uint32_t mid = (l2i + h2) >> 1;
+                        if (Lz.cand[LL[mid]] < v) l2i = mid + 1; else h2 = mid;
+                    }
+                    c -= (l2i < nl && Lz.cand[LL[l2i]] == v) ? 1ull : 0ull;
+                }
+                sum += c;
+            }
+        }
+        touched += n1 + 4;
+        out = sum;
+        return true;
+    }
+
     // The closed form of the last two levels for one level-d entry x (d =
     // n-3), by this lane alone; false (x left to the warp-wide path) when an
     // intersection would be long.  Same arithmetic as tail2 with the whole
@@ -406,6 +482,7 @@ struct Warp {
                 yz[k] = y;
             }
         }
+        if (tail == kTailIsect) return lane_tail_isect(d, x, ya, yz, self, out, touched);
         // entries of D that are level-(d+1) conflicts
         uint32_t xe[kLaneTailConf];
         uint32_t nexcl = 0;
@@ -1468,7 +1545,9 @@ int launch(const EnumArgs &a, uint32_t smem, int num_sms, cudaStream_t s) {
 // Closed form of the last two levels for a COUNT-mode plan (kTail*).
 uint32_t tail_mode(const asdm_plan &plan) {
     const size_t n = plan.order.size();
-    if (n < 3 || plan.back[n - 2].size() != 1 || plan.back[n - 1].size() != 1) return kTailNone;
+    if (n < 3 || plan.back[n - 1].size() != 1) return kTailNone;
+    if (plan.back[n - 2].size() == 2) return n >= 4 ? kTailIsect : kTailNone;
+    if (plan.back[n - 2].size() != 1) return kTailNone;
     return plan.back[n - 1][0].first == n - 2 ? kTailChain : kTailLeaf;
 }
 
@@ -1550,7 +1629,7 @@ int build_tails(const std::vector<const asdm_cs *> &cs, const std::vector<const 
         const uint32_t m = tail_mode(p);
         if (m == kTailNone) continue;
         const size_t n = p.order.size();
-        if (m == kTailLeaf) {
+        if (m != kTailChain) {
             out[i].mode = m;
             continue;
         }
@@ -1667,9 +1746,9 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
             return ASDM_OK;
         }
     }
-    if (mode == ASDM_MODE_COUNT && plan.order.size() == n && tree_countable(q)) {
-        // conflict-free tree: the tree program counts it (the enumeration
-        // below only when the program overflows)
+    if (mode == ASDM_MODE_COUNT && plan.order.size() == n && tree_countable_conflicts(q)) {
+        // tree: the tree program counts it (the enumeration below only when
+        // the program overflows)
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
@@ -1893,9 +1972,9 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     }
     if (agg) *agg = asdm_run_stats{};
     if (live.empty()) return ASDM_OK;
-    // conflict-free tree queries are counted by the tree program (full plans
-    // only; prefix plans count partial matches); in LOCAL mode with their
-    // local counts, a few queries at a time
+    // tree queries are counted by the tree program (full plans only; prefix
+    // plans count partial matches); in LOCAL mode the conflict-free ones with
+    // their local counts, a few queries at a time
     float tree_ms = 0.f;
     if (local_out) {
         std::vector<uint32_t> tid;
@@ -1964,7 +2043,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         std::vector<asdm_cs *> tcs;
         std::vector<uint32_t> tid;
         for (uint32_t i : live)
-            if (plans[i]->order.size() == cs[i]->q.n && tree_countable(cs[i]->q)) {
+            if (plans[i]->order.size() == cs[i]->q.n && tree_countable_conflicts(cs[i]->q)) {
                 tcs.push_back(cs[i]);
                 tid.push_back(i);
             }
@@ -2045,7 +2124,8 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         qd[li].nb = (uint32_t)bk.size();
         qd[li].nc = (uint32_t)cf.size();
         unsigned long long nt = 0;
-        const bool light = local_out == nullptr && n <= 4 && tail_mode(plan) != kTailNone;
+        const uint32_t tm = tail_mode(plan);
+        const bool light = local_out == nullptr && n <= 4 && (tm == kTailChain || tm == kTailLeaf);
         root_blocks(c, plan, qd[li].pairs, qd[li].blk, nt, light ? light_blk : 1);
         task_pre[li + 1] = task_pre[li] + nt;
         maxn = std::max(maxn, n);

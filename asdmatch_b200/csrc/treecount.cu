@@ -1,44 +1,66 @@
 // Exact counts of tree-shaped queries without enumeration.
 //
 // Within the candidate space, a map of the query vertices to candidates that
-// sends every query edge to a candidate edge is an embedding unless two
-// distinct query vertices land on the same data vertex.  Two vertices of
-// different labels never do (their candidate sets are disjoint), nor do two
-// adjacent vertices (the data graph has no self loops).  So when no two
-// non-adjacent query vertices share a label, the count of embeddings equals
-// the count of such maps, and for a tree query that count is a bottom-up
-// dynamic program over the candidate-edge lists:
+// sends every query edge to a candidate edge is a homomorphism; it is an
+// embedding when, in addition, no two query vertices of one label that are
+// not adjacent land on the same data vertex (the conflict pairs the
+// enumeration checks; vertices of different labels have disjoint candidate
+// sets, and adjacent ones differ because the data graph has no self loops).
+// For a tree query the count of homomorphisms is a bottom-up dynamic program
+// over the candidate-edge lists:
 //     w_u(i) = prod over children c of u of  sum over j in list_{u->c}(i) of  w_c(j)
-//     count  = sum over i of w_root(i)
-// (the reference reaches the same number by enumeration: adaptiveShareJoin
-// with ALL_LEVEL, matching/adaptive.cpp:1179-2279).  Arithmetic is uint64
-// with overflow detection; a query whose program overflows anywhere is left
-// to the enumeration kernels, which report ASDM_ERR_OVERFLOW if its count
-// itself exceeds 2^64 - 1.
+//     hom    = sum over i of w_root(i)
+// and the count of embeddings follows by inclusion-exclusion over the
+// partitions pi of each label's vertices into blocks of pairwise non-adjacent
+// vertices:
+//     count = sum over pi of  mu(pi) * hom(Q / pi),
+//     mu(pi) = prod over blocks B of (-1)^(|B|-1) (|B|-1)!
+// where Q / pi identifies the vertices of each block (one data vertex for the
+// whole block: a candidate of every member).  Every candidate edge is a data
+// edge between candidates and every data edge between candidates is a
+// candidate edge (K3 keeps all of them), so parallel edges of Q / pi are one
+// constraint; a query qualifies when every such quotient is again a tree.
+// (The reference reaches the same number by enumeration: adaptiveShareJoin
+// with ALL_LEVEL, matching/adaptive.cpp:1179-2279.)
+//
+// Arithmetic is modulo 2^64.  Each hom(Q / pi) is at most hom(Q) (a
+// homomorphism of the quotient composed with the quotient map is one of Q), so
+// when the identity partition's program does not overflow — checked — the
+// signed sum is exact.  A query whose identity program overflows is left to
+// the enumeration kernels, which report ASDM_ERR_OVERFLOW if its count itself
+// exceeds 2^64 - 1.
 #include <algorithm>
+#include <functional>
 
 #include "cs.cuh"
 
 namespace asdm {
 namespace {
 
-// One (query, query vertex) of a height level of the programs.
+// One (query, term, block) of a height level of the programs.  A block's
+// candidates are indexed like those of its representative member r (the
+// member its parent edge reaches); the other members' maps C(r) -> C(member)
+// (kNone where the vertex is not their candidate) zero the weights of the
+// candidates outside the intersection.
 struct TreeSeg {
-    unsigned long long *w;       // weights of u's candidates (output)
-    uint32_t ncand;              // |C(u)|
+    unsigned long long *w;       // weights of the block's candidates (output)
+    uint32_t ncand;              // |C(r)|
     uint32_t child_first;        // children in the TreeChild array
     uint32_t nchild;
     uint32_t query;              // index into counts / flags
     uint32_t root;               // 1: add the weights into the query's count
-    uint32_t pad;
+    uint32_t check;              // 1: the identity partition's program (overflow checked)
+    uint32_t val_first, nval;    // the other members' maps, in the map array
+    long long coef;              // mu(pi) of the term
     unsigned long long start;    // first item of this segment in the launch
 };
 
 struct TreeChild {
     const uint32_t *off;              // candidate-edge offsets of (u -> c), by candidate of u
     const uint32_t *list;             // entries: indices into C(c)
-    const unsigned long long *w;      // weights of c's candidates (null for a leaf: all 1)
+    const unsigned long long *w;      // weights of c's block (null for a one-vertex leaf: all 1)
     unsigned long long *s_out;        // local counts: the sum over the list, by candidate of u (or null)
+    const uint32_t *src;              // map C(r) -> C(u) when u is not the representative (else null)
 };
 
 // Local counts, top down: up_c(j) = sum over i in list_{c->u}(j) of
@@ -61,10 +83,12 @@ struct LocSeg {
     unsigned long long start;
 };
 
-// One thread per candidate of the level's query vertices; a list longer than
-// 32 entries is summed by the whole warp.
+// One thread per candidate of the level's blocks; a list longer than 32
+// entries is summed by the whole warp.  Sums and products wrap modulo 2^64;
+// the identity partition's program flags an overflow instead.
 __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsigned long long total,
-                           const TreeChild *__restrict__ kids, unsigned long long *__restrict__ counts,
+                           const TreeChild *__restrict__ kids, const uint32_t *const *__restrict__ maps,
+                           unsigned long long *__restrict__ counts, unsigned long long *__restrict__ homs,
                            unsigned int *__restrict__ overflow) {
     const uint32_t lane = threadIdx.x & 31;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
@@ -74,6 +98,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
         const bool valid = t < total;
         TreeSeg sg{};
         uint32_t i = 0;
+        bool alive = valid;
         if (valid) {
             uint32_t lo = 0, hi = nseg;
             while (hi - lo > 1) {
@@ -82,26 +107,28 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
             }
             sg = segs[lo];
             i = (uint32_t)(t - sg.start);
+            for (uint32_t k = 0; k < sg.nval && alive; ++k) alive = maps[sg.val_first + k][i] != kNone;
         }
-        unsigned long long acc = 1;
+        unsigned long long acc = alive ? 1ull : 0ull;
         bool over = false;
         // children are visited in lock step: k-th child of every lane's segment
-        uint32_t maxk = valid ? sg.nchild : 0;
+        uint32_t maxk = alive ? sg.nchild : 0;
 #pragma unroll
         for (int o = 16; o; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
         for (uint32_t k = 0; k < maxk; ++k) {
-            const bool mine = valid && k < sg.nchild;
+            const bool mine = alive && k < sg.nchild;
             uint32_t b = 0, e = 0;
             const unsigned long long *w = nullptr;
             const uint32_t *list = nullptr;
             if (mine) {
                 const TreeChild ch = kids[sg.child_first + k];
-                b = ch.off[i];
-                e = ch.off[i + 1];
+                const uint32_t iu = ch.src ? ch.src[i] : i;
+                b = ch.off[iu];
+                e = ch.off[iu + 1];
                 w = ch.w;
                 list = ch.list;
             }
-            // a leaf child contributes its list length
+            // a one-vertex leaf child contributes its list length
             unsigned long long sum = (mine && !w) ? (unsigned long long)(e - b) : 0ull;
             const bool coop = mine && w && (e - b) > 32;
             uint32_t todo = __ballot_sync(0xffffffffu, coop);
@@ -145,14 +172,17 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
             }
         }
         if (!valid) continue;
-        if (over) {
+        if (over && sg.check) {
             atomicOr(&overflow[sg.query], 1u);
             acc = 0;
         }
         sg.w[i] = acc;
         if (sg.root && acc) {
-            const unsigned long long old = atomicAdd(&counts[sg.query], acc);
-            if (old + acc < old) atomicOr(&overflow[sg.query], 1u);
+            atomicAdd(&counts[sg.query], (unsigned long long)sg.coef * acc);
+            if (sg.check) {
+                const unsigned long long old = atomicAdd(&homs[sg.query], acc);
+                if (old + acc < old) atomicOr(&overflow[sg.query], 1u);
+            }
         }
     }
 }
@@ -208,10 +238,138 @@ __global__ void tree_local(const LocSeg *__restrict__ segs, uint32_t nseg, unsig
     }
 }
 
+// C(r) -> C(u) for the members u of merged blocks: index in C(u) of each
+// candidate of r, or kNone.
+struct MapSeg {
+    const uint32_t *from, *to;
+    uint32_t *out;
+    uint32_t nto, pad;
+    unsigned long long start;
+};
+
+__global__ void tree_maps(const MapSeg *__restrict__ segs, uint32_t nseg, unsigned long long total) {
+    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        const MapSeg sg = segs[seg_of(&segs[0].start, sizeof(MapSeg), nseg, t)];
+        const uint32_t v = sg.from[t - sg.start];
+        const uint32_t j = lower_bound_u32(sg.to, sg.nto, v);
+        sg.out[t - sg.start] = (j < sg.nto && sg.to[j] == v) ? j : kNone;
+    }
+}
+
+constexpr size_t kMaxPartitions = 4096;  // partitions generated for one query
+constexpr size_t kMaxTerms = 64;         // terms counted for one query
+
+// One term of the inclusion-exclusion: a partition of the query vertices
+// into blocks, its quotient rooted at the block of vertex 0.
+struct BlockTree {
+    long long coef = 1;
+    bool identity = true;                         // every block one vertex (block b = vertex b)
+    uint32_t nb = 0;
+    std::vector<uint32_t> block;                  // by vertex
+    std::vector<std::vector<uint32_t>> members;   // by block, ascending
+    std::vector<uint32_t> rep;                    // representative member
+    std::vector<uint32_t> parent;                 // parent block (kNone at the root)
+    std::vector<uint32_t> pedge;                  // query edge (pfrom -> rep) from the parent block
+    std::vector<uint32_t> pfrom;                  // the parent block's member it leaves from
+    std::vector<uint32_t> height, depth;
+};
+
+// Roots the quotient of t's partition; false when it is not a tree.
+bool root_quotient(const QueryGraph &q, BlockTree &t) {
+    std::vector<std::pair<uint32_t, uint32_t>> qe;
+    for (uint32_t u = 0; u < q.n; ++u)
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            const uint32_t a = t.block[u], b = t.block[q.nbr[e]];
+            if (a == b) return false;
+            if (a < b) qe.emplace_back(a, b);
+        }
+    std::sort(qe.begin(), qe.end());
+    qe.erase(std::unique(qe.begin(), qe.end()), qe.end());
+    if (qe.size() + 1 != t.nb) return false;
+    t.rep.assign(t.nb, kNone);
+    t.parent.assign(t.nb, kNone);
+    t.pedge.assign(t.nb, kNone);
+    t.pfrom.assign(t.nb, kNone);
+    t.height.assign(t.nb, 0);
+    t.depth.assign(t.nb, 0);
+    std::vector<uint32_t> order{t.block[0]};
+    t.rep[t.block[0]] = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        const uint32_t B = order[k];
+        for (uint32_t u : t.members[B])
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                const uint32_t w = q.nbr[e], C = t.block[w];
+                if (C == B || t.rep[C] != kNone) continue;
+                t.rep[C] = w;
+                t.parent[C] = B;
+                t.pedge[C] = e;
+                t.pfrom[C] = u;
+                t.depth[C] = t.depth[B] + 1;
+                order.push_back(C);
+            }
+    }
+    if (order.size() != t.nb) return false;
+    for (size_t k = order.size(); k-- > 1;) {
+        const uint32_t C = order[k], B = t.parent[C];
+        t.height[B] = std::max(t.height[B], t.height[C] + 1);
+    }
+    return true;
+}
+
+// Every term of a tree query's count; false when the query does not qualify
+// (not a tree, a quotient with a cycle, too many partitions).
+bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out) {
+    out.clear();
+    if (q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) return false;
+    std::vector<uint32_t> block(q.n, kNone);
+    std::vector<std::vector<uint32_t>> members;
+    size_t generated = 0;
+    bool ok = true;
+    // vertex u joins a block of its label with no neighbour of u, or opens one
+    std::function<void(uint32_t)> place = [&](uint32_t u) {
+        if (!ok) return;
+        if (u == q.n) {
+            if (++generated > kMaxPartitions) { ok = false; return; }
+            BlockTree t;
+            t.nb = (uint32_t)members.size();
+            t.block = block;
+            t.members = members;
+            for (const auto &m : members) {
+                long long f = 1;
+                for (size_t k = 2; k < m.size(); ++k) f *= (long long)k;
+                t.coef *= (m.size() % 2 == 0) ? -f : f;
+                t.identity = t.identity && m.size() == 1;
+            }
+            if (!root_quotient(q, t) || out.size() >= kMaxTerms) { ok = false; return; }
+            out.push_back(std::move(t));
+            return;
+        }
+        for (uint32_t b = 0; b < members.size() && ok; ++b) {
+            if (q.lab[members[b][0]] != q.lab[u]) continue;
+            bool adj = false;
+            for (uint32_t w : members[b]) adj = adj || q.slot(u, w) >= 0;
+            if (adj) continue;
+            members[b].push_back(u);
+            block[u] = b;
+            place(u + 1);
+            members[b].pop_back();
+        }
+        if (!ok) return;
+        block[u] = (uint32_t)members.size();
+        members.push_back({u});
+        place(u + 1);
+        members.pop_back();
+    };
+    place(0);
+    if (!ok) out.clear();
+    return ok;
+}
+
 }  // namespace
 
-// A query the program counts exactly: connected tree, no two non-adjacent
-// vertices with one label.
+// A query whose count (and local counts) the program gives with the identity
+// partition alone: connected tree, no two non-adjacent vertices with one label.
 bool tree_countable(const QueryGraph &q) {
     if (q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) return false;
     for (uint32_t u = 0; u < q.n; ++u)
@@ -220,80 +378,93 @@ bool tree_countable(const QueryGraph &q) {
     return true;
 }
 
+// A tree query whose count the program gives by inclusion-exclusion: every
+// quotient by same-label blocks is a tree (always so when the same-label
+// vertices are at distance 2: siblings, or grandparent and grandchild).
+bool tree_countable_conflicts(const QueryGraph &q) {
+    std::vector<BlockTree> t;
+    return block_trees(q, t);
+}
+
 // Counts every countable query of `cs` (non-empty candidate spaces on graph
-// G); done[i] = 1 and counts[i] set for the queries it settled.
+// G); done[i] = 1 and counts[i] set for the queries it settled.  With local
+// counts only queries without conflicts are taken.
 int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
                 std::vector<char> &done, const std::vector<unsigned long long *> *local) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
     counts.assign(Q, 0);
     done.assign(Q, 0);
-    // rooted trees, vertices grouped by height
-    struct Item { uint32_t q, u, parent; };
+    // (query, term, block) grouped by the block's height (and depth)
+    struct Item { uint32_t q, t, b; };
     std::vector<std::vector<Item>> by_height, by_depth;
-    std::vector<uint64_t> qwb(Q, 0);  // per query: first weight
-    std::vector<std::vector<uint32_t>> parent(Q);
+    std::vector<std::vector<BlockTree>> trees(Q);
+    std::vector<std::vector<std::vector<uint64_t>>> woff(Q);  // first weight of (query, term, block)
     uint64_t wtotal = 0;
     std::vector<uint32_t> take;
+    // maps C(rep) -> C(member) of merged blocks, one per (query, rep, member)
+    std::vector<MapSeg> msegs;
+    std::vector<std::vector<std::pair<uint64_t, uint32_t>>> mkey(Q);  // ((rep << 32) | member, seg)
+    uint64_t mtotal = 0;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         const asdm_cs &c = *cs[qi];
-        if (!c.nonempty || !tree_countable(c.q)) continue;
-        const QueryGraph &q = c.q;
-        // root at vertex 0; BFS gives parents, heights from the leaves up
-        std::vector<uint32_t> order{0}, par(q.n, kNone), height(q.n, 0);
-        std::vector<char> seen(q.n, 0);
-        seen[0] = 1;
-        for (size_t k = 0; k < order.size(); ++k)
-            for (uint32_t e = q.off[order[k]]; e < q.off[order[k] + 1]; ++e) {
-                const uint32_t w = q.nbr[e];
-                if (!seen[w]) { seen[w] = 1; par[w] = order[k]; order.push_back(w); }
+        if (!c.nonempty || !block_trees(c.q, trees[qi])) continue;
+        if (local && trees[qi].size() != 1) continue;
+        woff[qi].resize(trees[qi].size());
+        for (uint32_t ti = 0; ti < trees[qi].size(); ++ti) {
+            const BlockTree &t = trees[qi][ti];
+            woff[qi][ti].resize(t.nb);
+            for (uint32_t b = 0; b < t.nb; ++b) {
+                woff[qi][ti][b] = wtotal;
+                wtotal += c.ncand[t.rep[b]];
+                if (by_height.size() <= t.height[b]) by_height.resize(t.height[b] + 1);
+                by_height[t.height[b]].push_back(Item{qi, ti, b});
+                if (by_depth.size() <= t.depth[b]) by_depth.resize(t.depth[b] + 1);
+                by_depth[t.depth[b]].push_back(Item{qi, ti, b});
+                for (uint32_t u : t.members[b]) {
+                    if (u == t.rep[b]) continue;
+                    const uint64_t key = ((uint64_t)t.rep[b] << 32) | u;
+                    bool have = false;
+                    for (auto &kv : mkey[qi]) have = have || kv.first == key;
+                    if (have) continue;
+                    mkey[qi].emplace_back(key, (uint32_t)msegs.size());
+                    msegs.push_back(MapSeg{c.d_cand + c.cand_base[t.rep[b]], c.d_cand + c.cand_base[u], nullptr,
+                                           c.ncand[u], 0, mtotal});
+                    mtotal += c.ncand[t.rep[b]];
+                }
             }
-        if (order.size() != q.n) continue;
-        for (size_t k = order.size(); k-- > 1;) height[par[order[k]]] = std::max(height[par[order[k]]], height[order[k]] + 1);
-        qwb[qi] = wtotal;
-        for (uint32_t u = 0; u < q.n; ++u) wtotal += c.ncand[u];
-        for (uint32_t u = 0; u < q.n; ++u) {
-            if (by_height.size() <= height[u]) by_height.resize(height[u] + 1);
-            by_height[height[u]].push_back(Item{qi, u, par[u]});
         }
-        {
-            std::vector<uint32_t> depth(q.n, 0);
-            for (size_t k = 1; k < order.size(); ++k) depth[order[k]] = depth[par[order[k]]] + 1;
-            for (uint32_t u = 0; u < q.n; ++u) {
-                if (by_depth.size() <= depth[u]) by_depth.resize(depth[u] + 1);
-                by_depth[depth[u]].push_back(Item{qi, u, par[u]});
-            }
-        }
-        parent[qi] = par;
         take.push_back(qi);
     }
     if (take.empty()) return ASDM_OK;
-    auto wptr_off = [&](uint32_t qi, uint32_t u) {
-        uint64_t o = qwb[qi];
-        for (uint32_t v = 0; v < u; ++v) o += cs[qi]->ncand[v];
-        return o;
+    auto is_leaf1 = [&](uint32_t qi, uint32_t ti, uint32_t b) {
+        const BlockTree &t = trees[qi][ti];
+        return t.height[b] == 0 && t.members[b].size() == 1;
     };
+    auto wptr_off = [&](uint32_t qi, uint32_t u) { return woff[qi][0][u]; };  // identity term: block = vertex
     // S_{parent(c), c} has |C(parent)| entries, at sslot[query][c]
     std::vector<std::vector<uint64_t>> sslot(Q);
     uint64_t stotal = 0;
     if (local) {
-        for (uint32_t qi : take) {
-            const asdm_cs &c = *cs[qi];
-            sslot[qi].assign(c.q.n, 0);
-        }
+        for (uint32_t qi : take) sslot[qi].assign(cs[qi]->q.n, 0);
         for (const auto &lv : by_height)
-            for (const Item &it : lv)
-                if (it.parent != kNone) {
-                    sslot[it.q][it.u] = stotal;
-                    stotal += cs[it.q]->ncand[it.parent];
+            for (const Item &it : lv) {
+                const uint32_t par = trees[it.q][it.t].parent[it.b];
+                if (par != kNone) {
+                    sslot[it.q][it.b] = stotal;
+                    stotal += cs[it.q]->ncand[par];
                 }
+            }
     }
     unsigned long long *sbase = nullptr;
     auto s_of = [&](uint32_t qi, uint32_t ch) { return sbase + sslot[qi][ch]; };
-    unsigned long long *w = nullptr, *d_counts = nullptr, *sums = nullptr, *up = nullptr;
+    unsigned long long *w = nullptr, *d_counts = nullptr, *d_homs = nullptr, *sums = nullptr, *up = nullptr;
     unsigned int *d_over = nullptr;
+    uint32_t *d_mapbuf = nullptr;
     TreeSeg *d_segs = nullptr;
     TreeChild *d_kids = nullptr;
+    MapSeg *d_mseg = nullptr;
+    const uint32_t **d_maps = nullptr;
     UpSeg *d_up = nullptr;
     LocSeg *d_loc = nullptr;
     const unsigned long long **d_sibs = nullptr;
@@ -301,14 +472,41 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
     // candidate of the parent u) and up_u (laid out like the weights)
     int rc = ASDM_OK;
     do {
-        if ((rc = dalloc(&w, wtotal, s)) || (rc = dalloc(&d_counts, Q, s)) || (rc = dalloc(&d_over, Q, s))) break;
+        if ((rc = dalloc(&w, wtotal, s)) || (rc = dalloc(&d_counts, 2ull * Q, s)) || (rc = dalloc(&d_over, Q, s)))
+            break;
+        d_homs = d_counts + Q;
         if (local && ((rc = dalloc(&sums, std::max<uint64_t>(stotal, 1), s)) || (rc = dalloc(&up, wtotal, s)))) break;
         sbase = sums;
-        if (cudaMemsetAsync(d_counts, 0, Q * sizeof(unsigned long long), s) != cudaSuccess ||
+        if (cudaMemsetAsync(d_counts, 0, 2ull * Q * sizeof(unsigned long long), s) != cudaSuccess ||
             cudaMemsetAsync(d_over, 0, Q * sizeof(unsigned int), s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "tree-count reset failed");
             break;
         }
+        // member maps of merged blocks
+        std::vector<const uint32_t *> maps;
+        if (mtotal) {
+            if ((rc = dalloc(&d_mapbuf, mtotal, s)) || (rc = dalloc(&d_mseg, msegs.size(), s))) break;
+            for (auto &m : msegs) m.out = d_mapbuf + m.start;
+            if (cudaMemcpyAsync(d_mseg, msegs.data(), msegs.size() * sizeof(MapSeg), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "tree-count map upload failed");
+                break;
+            }
+            const unsigned grid =
+                (unsigned)std::min<unsigned long long>((mtotal + 255) / 256, (unsigned long long)G->num_sms * 32);
+            tree_maps<<<grid, 256, 0, s>>>(d_mseg, (uint32_t)msegs.size(), mtotal);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "tree-count map kernel failed");
+                break;
+            }
+        }
+        auto map_of = [&](uint32_t qi, uint32_t r, uint32_t u) -> const uint32_t * {
+            const uint64_t key = ((uint64_t)r << 32) | u;
+            for (auto &kv : mkey[qi])
+                if (kv.first == key) return msegs[kv.second].out;
+            return nullptr;
+        };
         // every level's segments and children, uploaded once
         std::vector<TreeSeg> segs;
         std::vector<TreeChild> kids;
@@ -317,22 +515,32 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
         for (size_t h = 0; h < by_height.size(); ++h) {
             unsigned long long total = 0;
             for (const Item &it : by_height[h]) {
+                if (is_leaf1(it.q, it.t, it.b)) continue;  // weighs 1: its parent takes the list length
                 const asdm_cs &c = *cs[it.q];
                 const QueryGraph &q = c.q;
+                const BlockTree &t = trees[it.q][it.t];
+                const uint32_t r = t.rep[it.b];
                 TreeSeg sg{};
-                sg.w = w + wptr_off(it.q, it.u);
-                sg.ncand = c.ncand[it.u];
+                sg.w = w + woff[it.q][it.t][it.b];
+                sg.ncand = c.ncand[r];
                 sg.child_first = (uint32_t)kids.size();
                 sg.query = it.q;
-                sg.root = it.parent == kNone ? 1u : 0u;
+                sg.root = t.parent[it.b] == kNone ? 1u : 0u;
+                sg.check = t.identity ? 1u : 0u;
+                sg.coef = t.coef;
+                sg.val_first = (uint32_t)maps.size();
+                for (uint32_t u : t.members[it.b])
+                    if (u != r) maps.push_back(map_of(it.q, r, u));
+                sg.nval = (uint32_t)maps.size() - sg.val_first;
                 sg.start = total;
-                for (uint32_t e = q.off[it.u]; e < q.off[it.u + 1]; ++e) {
-                    const uint32_t ch = q.nbr[e];
-                    if (ch == it.parent) continue;
-                    const bool leaf = q.deg(ch) == 1;
+                for (uint32_t C = 0; C < t.nb; ++C) {
+                    if (t.parent[C] != it.b) continue;
+                    const uint32_t e = t.pedge[C], u = t.pfrom[C];
                     kids.push_back(TreeChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
-                                             leaf ? nullptr : w + wptr_off(it.q, ch), local ? s_of(it.q, ch) : nullptr});
+                                             is_leaf1(it.q, it.t, C) ? nullptr : w + woff[it.q][it.t][C],
+                                             local ? s_of(it.q, C) : nullptr, u == r ? nullptr : map_of(it.q, r, u)});
                 }
+                (void)q;
                 sg.nchild = (uint32_t)kids.size() - sg.child_first;
                 total += sg.ncand;
                 segs.push_back(sg);
@@ -340,22 +548,28 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
             lvl_first.push_back(segs.size());
             lvl_total.push_back(total);
         }
-        if (kids.empty()) kids.push_back(TreeChild{nullptr, nullptr, nullptr});
-        if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s))) break;
+        if (kids.empty()) kids.push_back(TreeChild{});
+        if (maps.empty()) maps.push_back(nullptr);
+        if (segs.empty()) segs.push_back(TreeSeg{});
+        if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s)) ||
+            (rc = dalloc(&d_maps, maps.size(), s)))
+            break;
         if (cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(TreeSeg), cudaMemcpyHostToDevice, s) !=
                 cudaSuccess ||
             cudaMemcpyAsync(d_kids, kids.data(), kids.size() * sizeof(TreeChild), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(d_maps, maps.data(), maps.size() * sizeof(void *), cudaMemcpyHostToDevice, s) !=
                 cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "tree-count upload failed");
             break;
         }
-        for (size_t h = 1; h < by_height.size() && rc == ASDM_OK; ++h) {  // leaves (height 0) weigh 1
+        for (size_t h = 0; h < by_height.size() && rc == ASDM_OK; ++h) {
             const unsigned long long total = lvl_total[h];
             if (total == 0) continue;
             const unsigned grid =
                 (unsigned)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)G->num_sms * 32);
             tree_level<<<grid, 256, 0, s>>>(d_segs + lvl_first[h], (uint32_t)(lvl_first[h + 1] - lvl_first[h]),
-                                            total, d_kids, d_counts, d_over);
+                                            total, d_kids, d_maps, d_counts, d_homs, d_over);
             ::asdm::count_launch();
             if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "tree-count kernel failed");
         }
@@ -371,25 +585,26 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
             for (size_t dpt = 1; dpt < by_depth.size(); ++dpt) {
                 unsigned long long total = 0;
                 for (const Item &it : by_depth[dpt]) {
+                    // identity terms only: block b is vertex b
                     const asdm_cs &c = *cs[it.q];
                     const QueryGraph &q = c.q;
-                    const uint32_t u = it.parent;
-                    const int k = q.slot(it.u, u);  // edge (c -> u)
-                    const uint32_t e = q.off[it.u] + (uint32_t)k;
+                    const std::vector<uint32_t> &par = trees[it.q][0].parent;
+                    const uint32_t u = par[it.b];
+                    const int k = q.slot(it.b, u);  // edge (c -> u)
+                    const uint32_t e = q.off[it.b] + (uint32_t)k;
                     UpSeg sg{};
-                    sg.up = up + wptr_off(it.q, it.u);
+                    sg.up = up + wptr_off(it.q, it.b);
                     sg.off = c.d_eoff + c.eoff_base[e];
                     sg.list = c.d_elist + c.elist_base[e];
-                    const std::vector<uint32_t> &par = parent[it.q];
                     sg.up_u = par[u] == kNone ? nullptr : up + wptr_off(it.q, u);
                     sg.sib_first = (uint32_t)sibs.size();
                     for (uint32_t e2 = q.off[u]; e2 < q.off[u + 1]; ++e2) {
                         const uint32_t c2 = q.nbr[e2];
-                        if (par[c2] == u && c2 != it.u) sibs.push_back(s_of(it.q, c2));
+                        if (par[c2] == u && c2 != it.b) sibs.push_back(s_of(it.q, c2));
                     }
                     sg.nsib = (uint32_t)sibs.size() - sg.sib_first;
                     sg.query = it.q;
-                    sg.ncand = c.ncand[it.u];
+                    sg.ncand = c.ncand[it.b];
                     sg.start = total;
                     total += sg.ncand;
                     ups.push_back(sg);
@@ -400,8 +615,8 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
             for (uint32_t qi : take) {
                 const asdm_cs &c = *cs[qi];
                 for (uint32_t u = 0; u < c.q.n; ++u) {
-                    const bool root = parent[qi][u] == kNone;
-                    LocSeg ls{(c.q.deg(u) == 1 && !root) ? nullptr : w + wptr_off(qi, u), root ? nullptr : up + wptr_off(qi, u),
+                    const bool root = trees[qi][0].parent[u] == kNone;
+                    LocSeg ls{is_leaf1(qi, 0, u) ? nullptr : w + wptr_off(qi, u), root ? nullptr : up + wptr_off(qi, u),
                               c.d_cand + c.cand_base[u], (*local)[qi], c.q.n, u, qi, c.ncand[u], ltotal};
                     ltotal += c.ncand[u];
                     locs.push_back(ls);
@@ -456,6 +671,9 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
     } while (false);
     dfree(d_segs, s);
     dfree(d_kids, s);
+    dfree(d_maps, s);
+    dfree(d_mseg, s);
+    dfree(d_mapbuf, s);
     dfree(d_up, s);
     dfree(d_sibs, s);
     dfree(d_loc, s);
