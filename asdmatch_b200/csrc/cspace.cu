@@ -221,8 +221,7 @@ struct CompDesc {
     uint32_t lbase;         // vbl_off[l(u)]
     uint32_t phantom;       // append data vertex 0 when fewer than len survive
     uint32_t pad;
-    uint32_t *cbits;        // or null: membership bitset of the result
-    uint32_t *cpre;         //          and the result's size before each word
+    uint2 *cmem;            // or null: per word of the result, {membership bits, result size before it}
 };
 
 __device__ __forceinline__ uint32_t comp_word(const CompDesc &d, uint32_t w) {
@@ -297,10 +296,7 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
     for (int k = 0; k < kItems; ++k) {
         const uint32_t w = my + k;
         if (w >= d.words) break;
-        if (d.cbits) {
-            d.cbits[w] = x[k];
-            d.cpre[w] = pos;
-        }
+        if (d.cmem) d.cmem[w] = make_uint2(x[k], pos);
         for (uint32_t y = x[k]; y; y &= y - 1) o[pos++] = vbl[d.lbase + 32 * w + (uint32_t)(__ffs(y) - 1)];
     }
     // the last tile of a segment records the segment size
@@ -314,16 +310,17 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
 // ---- K3b: candidate edges ---------------------------------------------------
 struct EdgeDesc {
     const uint32_t *cand_u;   // C(u)
-    const uint32_t *cbits;    // membership of C(u2) by rank in l(u2)
-    const uint32_t *cpre;     // |C(u2)| before each word
+    const uint2 *cmem;        // per word of ranks in l(u2): {membership of C(u2), |C(u2)| before it}
     uint32_t ncand_u;
     uint32_t label_u2;
 };
 
-// Index in C(u2) of the vertex of rank r in l(u2), or kNone.
-__device__ __forceinline__ uint32_t cand_index(const uint32_t *cb, const uint32_t *cp, uint32_t r) {
-    const uint32_t w = cb[r >> 5], bit = 1u << (r & 31u);
-    return (w & bit) ? cp[r >> 5] + (uint32_t)__popc(w & (bit - 1u)) : kNone;
+// Index in C(u2) of the vertex of rank r in l(u2), or kNone (one 8-byte
+// load: the word's bits and prefix side by side).
+__device__ __forceinline__ uint32_t cand_index(const uint2 *cm, uint32_t r) {
+    const uint2 w = cm[r >> 5];
+    const uint32_t bit = 1u << (r & 31u);
+    return (w.x & bit) ? w.y + (uint32_t)__popc(w.x & (bit - 1u)) : kNone;
 }
 
 // rstart (optional): each item's label-run start, its length in cnt (read
@@ -343,7 +340,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
         const uint64_t pos = base + lane;
         const uint64_t item = (order && pos < total) ? order[pos] : pos;
         uint32_t b = 0, e = 0;
-        const uint32_t *cb = nullptr, *cp = nullptr;
+        const uint2 *cm = nullptr;
         if (pos < total) {
             const uint32_t ei = find_segment(item_base, nedges, item);
             const EdgeDesc d = edges[ei];
@@ -354,8 +351,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
                 const uint32_t i = (uint32_t)(item - item_base[ei]);
                 if (i < d.ncand_u) label_run(g, d.cand_u[i], d.label_u2, b, e);
             }
-            cb = d.cbits;
-            cp = d.cpre;
+            cm = d.cmem;
         }
         scanned += e - b;
         const bool coop = (e - b) > kLongRun;
@@ -366,13 +362,12 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
             const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            const uint32_t *mb = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)cb, src);
-            const uint32_t *mp = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)cp, src);
+            const uint2 *mm = (const uint2 *)__shfl_sync(0xffffffffu, (unsigned long long)cm, src);
             uint64_t o = __shfl_sync(0xffffffffu, out, src);
             uint32_t c = 0;
             for (uint32_t k0 = bb; k0 < ee; k0 += 32) {
                 const uint32_t k = k0 + lane;
-                const uint32_t idx = k < ee ? cand_index(mb, mp, g.nbr_rank[k]) : kNone;
+                const uint32_t idx = k < ee ? cand_index(mm, g.nbr_rank[k]) : kNone;
                 const uint32_t hit = __ballot_sync(0xffffffffu, idx != kNone);
                 if (kFill && idx != kNone) elist[o + __popc(hit & ((1u << lane) - 1))] = idx;
                 o += __popc(hit);
@@ -381,8 +376,9 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
             if ((int)lane == src) mine = c;
         }
         if (!coop) {
+#pragma unroll 4
             for (uint32_t k = b; k < e; ++k) {
-                const uint32_t idx = cand_index(cb, cp, g.nbr_rank[k]);
+                const uint32_t idx = cand_index(cm, g.nbr_rank[k]);
                 if (idx != kNone) {
                     if (kFill) elist[out++] = idx;
                     ++mine;
@@ -787,8 +783,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                     passes.push_back(PassDesc{sptr[qp.seg0 + p], bits + fword[su] + (1ull + slot) * words[su], q.lab[u], 0});
                     lens.push_back(slen[qp.seg0 + p]);
                 }
-                segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr,
-                                        nullptr});
+                segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr});
                 seg_ids.push_back(su);
                 bit_words_read += (uint64_t)(1 + __builtin_popcount(need)) * words[su];
             }
@@ -828,9 +823,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     arena->stream = s;
     std::vector<uint64_t> mword(nseg + 1, 0);
     for (uint32_t i = 0; i < nseg; ++i) mword[i + 1] = mword[i] + words[i];
-    uint32_t *cbits = nullptr, *cpre = nullptr;
-    ASDM_TRY(scr.alloc(&cbits, mword[nseg]));
-    ASDM_TRY(scr.alloc(&cpre, mword[nseg]));
+    uint2 *cmem = nullptr;
+    ASDM_TRY(scr.alloc(&cmem, mword[nseg]));
     {
         std::vector<CompDesc> segs;
         std::vector<uint32_t> seg_ids;
@@ -841,7 +835,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                 const uint32_t all = q.deg(u) ? ((q.deg(u) == 32 ? 0xFFFFFFFFu : (1u << q.deg(u)) - 1u)) : 0u;
                 const uint32_t su = qp.seg0 + u;
                 segs.push_back(CompDesc{bits + fword[su], words[su], all, qp.lsize[u], qp.lbase[u], 0, 0,
-                                        cbits + mword[su], cpre + mword[su]});
+                                        cmem + mword[su]});
                 seg_ids.push_back(su);
                 bit_words_read += (uint64_t)(1 + q.deg(u)) * words[su];
             }
@@ -882,8 +876,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                 const uint32_t u2 = q.nbr[e];
                 const uint32_t s2 = qp.seg0 + u2;
-                edges.push_back(EdgeDesc{arena->d_cand + cs.cand_base[u], cbits + mword[s2], cpre + mword[s2],
-                                         cs.ncand[u], q.lab[u2]});
+                edges.push_back(EdgeDesc{arena->d_cand + cs.cand_base[u], cmem + mword[s2], cs.ncand[u], q.lab[u2]});
                 item_base.push_back(item_base.back() + cs.ncand[u] + 1);
             }
     }

@@ -141,6 +141,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                 const uint32_t *ll = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)list, src);
                 unsigned long long part = 0;
                 bool pover = false;
+#pragma unroll 4
                 for (uint32_t x = bb + lane; x < ee; x += 32) {
                     const unsigned long long v = ww[ll[x]];
                     pover |= part + v < part;
@@ -159,6 +160,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                 }
             }
             if (mine && w && !coop)
+#pragma unroll 4
                 for (uint32_t x = b; x < e; ++x) {
                     const unsigned long long v = w[list[x]];
                     over |= sum + v < sum;
@@ -261,7 +263,7 @@ constexpr size_t kMaxPartitions = 4096;  // partitions generated for one query
 constexpr size_t kMaxTerms = 64;         // terms counted for one query
 
 // One term of the inclusion-exclusion: a partition of the query vertices
-// into blocks, its quotient rooted at the block of vertex 0.
+// into blocks, its quotient rooted at one block.
 struct BlockTree {
     long long coef = 1;
     bool identity = true;                         // every block one vertex (block b = vertex b)
@@ -275,8 +277,9 @@ struct BlockTree {
     std::vector<uint32_t> height, depth;
 };
 
-// Roots the quotient of t's partition; false when it is not a tree.
-bool root_quotient(const QueryGraph &q, BlockTree &t) {
+// Roots the quotient of t's partition at the block of vertex `root`
+// (its representative); false when the quotient is not a tree.
+bool root_quotient(const QueryGraph &q, BlockTree &t, uint32_t root = 0) {
     std::vector<std::pair<uint32_t, uint32_t>> qe;
     for (uint32_t u = 0; u < q.n; ++u)
         for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
@@ -293,8 +296,8 @@ bool root_quotient(const QueryGraph &q, BlockTree &t) {
     t.pfrom.assign(t.nb, kNone);
     t.height.assign(t.nb, 0);
     t.depth.assign(t.nb, 0);
-    std::vector<uint32_t> order{t.block[0]};
-    t.rep[t.block[0]] = 0;
+    std::vector<uint32_t> order{t.block[root]};
+    t.rep[t.block[root]] = root;
     for (size_t k = 0; k < order.size(); ++k) {
         const uint32_t B = order[k];
         for (uint32_t u : t.members[B])
@@ -317,9 +320,24 @@ bool root_quotient(const QueryGraph &q, BlockTree &t) {
     return true;
 }
 
+// Device work of a rooted term: one item per candidate of every block that
+// is not a one-vertex leaf, and one per entry of the lists summed into its
+// parent (a one-vertex leaf's parent takes the list length).
+uint64_t term_cost(const BlockTree &t, const asdm_cs &c) {
+    uint64_t cost = 0;
+    for (uint32_t b = 0; b < t.nb; ++b) {
+        if (t.height[b] == 0 && t.members[b].size() == 1) continue;
+        cost += c.ncand[t.rep[b]];
+        if (t.parent[b] != kNone) cost += c.etotal[t.pedge[b]];
+    }
+    return cost;
+}
+
 // Every term of a tree query's count; false when the query does not qualify
-// (not a tree, a quotient with a cycle, too many partitions).
-bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out) {
+// (not a tree, a quotient with a cycle, too many partitions).  With a built
+// candidate space each term is rooted where its program reads the fewest
+// list entries.
+bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out, const asdm_cs *cs = nullptr) {
     out.clear();
     if (q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) return false;
     std::vector<uint32_t> block(q.n, kNone);
@@ -342,6 +360,18 @@ bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out) {
                 t.identity = t.identity && m.size() == 1;
             }
             if (!root_quotient(q, t) || out.size() >= kMaxTerms) { ok = false; return; }
+            if (cs) {
+                BlockTree best = t;
+                uint64_t best_cost = term_cost(t, *cs);
+                for (uint32_t r = 1; r < q.n; ++r) {
+                    if (t.members[t.block[r]][0] != r) continue;  // one root per block: its first member
+                    BlockTree alt = t;
+                    if (!root_quotient(q, alt, r)) continue;
+                    const uint64_t cost = term_cost(alt, *cs);
+                    if (cost < best_cost) { best_cost = cost; best = std::move(alt); }
+                }
+                t = std::move(best);
+            }
             out.push_back(std::move(t));
             return;
         }
@@ -408,7 +438,7 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
     uint64_t mtotal = 0;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         const asdm_cs &c = *cs[qi];
-        if (!c.nonempty || !block_trees(c.q, trees[qi])) continue;
+        if (!c.nonempty || !block_trees(c.q, trees[qi], &c)) continue;
         if (local && trees[qi].size() != 1) continue;
         woff[qi].resize(trees[qi].size());
         for (uint32_t ti = 0; ti < trees[qi].size(); ++ti) {
