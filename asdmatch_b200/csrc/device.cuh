@@ -42,10 +42,27 @@ struct DevGraph {
     const uint32_t *run_start = nullptr;     // nruns
     const uint32_t *nbr_rank = nullptr;      // m2: pos_in_label of nbr[k]
     const uint2 *rank_info = nullptr;        // n, in vbl order: {degree, bit (l mod 32) per neighbour label l}
+    // n x (nlabels + 1), or null: row v holds, for every label l, the first
+    // edge of v whose neighbour has label >= l (then off[v+1]); the run of l is
+    // [row[l], row[l+1]).  Built when it fits kLabPosCap bytes.
+    const uint32_t *lab_pos = nullptr;
 };
+
+constexpr uint64_t kLabPosCap = 1ull << 30;
 
 // [b, e) edge range of label l in w's adjacency (empty if w has no such neighbour).
 __device__ __forceinline__ void label_run(const DevGraph &g, uint32_t w, uint32_t l, uint32_t &b, uint32_t &e) {
+    if (g.lab_pos) {
+        // one row of the dense table: both ends in one or two sectors
+        if (l < g.nlabels) {
+            const uint32_t *r = g.lab_pos + (uint64_t)w * (g.nlabels + 1) + l;
+            b = r[0];
+            e = r[1];
+        } else {
+            b = e = 0;
+        }
+        return;
+    }
     uint32_t lo = g.run_off[w], hi = g.run_off[w + 1];
     const uint32_t end = hi;
     while (lo < hi) {

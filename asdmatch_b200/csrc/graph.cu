@@ -104,6 +104,22 @@ __global__ void rank_infos(DevGraph g, uint2 *__restrict__ info) {
     }
 }
 
+// Dense label-run table: one thread per (vertex, label) entry.
+__global__ void write_lab_pos(DevGraph g, uint32_t *__restrict__ lab_pos) {
+    const uint32_t stride = g.nlabels + 1;
+    const uint64_t total = (uint64_t)g.n * stride;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(t / stride), l = (uint32_t)(t - (uint64_t)v * stride);
+        uint32_t lo = g.run_off[v], hi = g.run_off[v + 1];
+        const uint32_t end = hi;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (g.run_lab[mid] < l) lo = mid + 1; else hi = mid;
+        }
+        lab_pos[t] = lo < end ? g.run_start[lo] : g.off[v + 1];
+    }
+}
+
 __global__ void narrow_u64(const uint64_t *__restrict__ in, uint32_t *__restrict__ out, uint64_t n) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         out[i] = (uint32_t)in[i];
@@ -221,6 +237,19 @@ extern "C" int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, 
     ASDM_CUDA(cudaGetLastError());
     d.nbr_rank = d_nbr_rank;
     d.rank_info = d_rank_info;
+    const uint64_t lp_words = (uint64_t)n * (nlabels + 1);
+    if (n && lp_words * sizeof(uint32_t) <= kLabPosCap) {
+        uint32_t *lp = nullptr;
+        if (cudaMalloc((void **)&lp, lp_words * sizeof(uint32_t)) == cudaSuccess) {
+            write_lab_pos<<<(unsigned)std::min<uint64_t>((lp_words + 255) / 256, (uint64_t)g->num_sms * 32), 256, 0, s>>>(
+                d, lp);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+            d.lab_pos = lp;
+        } else {
+            cudaGetLastError();  // no room: label runs are searched instead
+        }
+    }
     dfree(runs, s); dfree(bad, s); dfree(run_pos, s);
     ASDM_CUDA(cudaStreamSynchronize(s));
     // the run arrays live in their own allocation; remember it for free()
@@ -233,6 +262,7 @@ extern "C" int asdm_graph_free(asdm_graph *g) {
     if (!g) return ASDM_OK;
     cudaStreamSynchronize(g->stream);
     cudaFree((void *)g->d.run_lab);  // run_lab heads the run allocation
+    if (g->d.lab_pos) cudaFree((void *)g->d.lab_pos);
     cudaFree(g->buf);
     cudaStreamDestroy(g->stream);
     delete g;
