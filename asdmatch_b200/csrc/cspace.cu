@@ -393,6 +393,80 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
     }
 }
 
+// The padded fill with the neighbour scan spread over the lanes: a warp takes
+// 32 consecutive items and walks the concatenation of their label runs 32
+// entries at a time, a lane per entry, so every lane has a membership lookup
+// in flight whatever the run lengths.  In: cnt = run lengths, rstart = run
+// starts (k3_bound), upos = padded positions; out: each item's hits packed in
+// order at the front of its padded region, cnt = their number.
+__global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__restrict__ edges,
+                                                  const uint64_t *__restrict__ item_base, uint32_t nedges,
+                                                  uint32_t *__restrict__ cnt, const uint64_t *__restrict__ upos,
+                                                  const uint32_t *__restrict__ rstart, uint32_t *__restrict__ padded,
+                                                  unsigned long long *__restrict__ elems) {
+    constexpr uint32_t kWarps = kBlock / 32;
+    __shared__ uint64_t s_pre[kWarps][33];   // exclusive prefix of the run lengths (s_pre[32] = total)
+    __shared__ uint64_t s_out[kWarps][32];   // padded position of each item
+    __shared__ const uint2 *s_cm[kWarps][32];
+    __shared__ uint32_t s_rs[kWarps][32], s_hits[kWarps][32];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t total = item_base[nedges];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t scanned = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+        const uint64_t item = base + lane;
+        uint64_t len = 0;
+        if (item < total) {
+            const uint32_t ei = find_segment(item_base, nedges, item);
+            s_cm[wid][lane] = edges[ei].cmem;
+            len = cnt[item];
+            s_rs[wid][lane] = rstart[item];
+            s_out[wid][lane] = upos[item];
+        }
+        uint64_t inc = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += y;
+        }
+        s_pre[wid][lane + 1] = inc;
+        if (lane == 0) s_pre[wid][0] = 0;
+        s_hits[wid][lane] = 0;
+        __syncwarp();
+        const uint64_t S = s_pre[wid][32];
+        scanned += S;
+        for (uint64_t j0 = 0; j0 < S; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            const bool valid = j < S;
+            // owner: the last item whose run starts at or before j (empty
+            // runs share their start with the next item and come first)
+            uint32_t lo = 0, hi = 32;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_pre[wid][mid] <= j) lo = mid; else hi = mid;
+            }
+            const uint32_t it = lo;
+            const uint64_t first = s_pre[wid][it];
+            uint32_t idx = kNone;
+            if (valid) idx = cand_index(s_cm[wid][it], g.nbr_rank[s_rs[wid][it] + (uint32_t)(j - first)]);
+            const uint32_t mask = __ballot_sync(0xffffffffu, idx != kNone);
+            // the item's lanes in this round are contiguous, from lane f
+            const uint32_t f = first > j0 ? (uint32_t)(first - j0) : 0u;
+            const uint32_t mine = mask & ~((1u << f) - 1u);
+            const uint32_t done = s_hits[wid][it];
+            if (idx != kNone) padded[s_out[wid][it] + done + __popc(mine & ((1u << lane) - 1u))] = idx;
+            const uint32_t next_it = __shfl_down_sync(0xffffffffu, it, 1);
+            const bool last = valid && (lane == 31 || j + 1 == S || next_it != it);
+            __syncwarp();
+            if (last) s_hits[wid][it] = done + __popc(mine & ((2u << lane) - 1u));
+            __syncwarp();
+        }
+        if (item < total) cnt[item] = s_hits[wid][lane];
+        __syncwarp();
+    }
+    if (elems && lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
+}
+
 // Upper bound of every item's list: the length of the candidate's label run.
 __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
@@ -918,8 +992,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         if (bound <= kPaddedEdgeCap) {
             uint32_t *padded = nullptr;
             ASDM_TRY(scr.alloc(&padded, bound));
-            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, d_upos, padded,
-                                                    d_elems + 1, rstart);
+            k3_flat<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, d_upos, rstart, padded, d_elems + 1);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
             ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_wpos, nitems, true, s));
