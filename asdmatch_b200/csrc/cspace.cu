@@ -172,40 +172,54 @@ __global__ void k2_keys(const PassDesc *__restrict__ passes, const uint64_t *__r
     }
 }
 
+// A warp takes 32 items and marks the concatenation of their label runs 32
+// entries at a time, a lane per entry (every lane has a reduction to issue,
+// whatever the run lengths).
 __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__restrict__ passes,
                                                   const uint64_t *__restrict__ prefix, uint32_t npass,
                                                   const uint32_t *__restrict__ order,
                                                   unsigned long long *__restrict__ elems) {
+    constexpr uint32_t kWarps = kBlock / 32;
+    __shared__ uint64_t s_pre[kWarps][33];   // exclusive prefix of the run lengths (s_pre[32] = total)
+    __shared__ uint32_t *s_mb[kWarps][32];
+    __shared__ uint32_t s_b[kWarps][32];
     const uint64_t total = prefix[npass];
-    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint64_t scanned = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint64_t pos = base + lane;
-        const uint64_t item = (order && pos < total) ? order[pos] : pos;
         uint32_t b = 0, e = 0;
-        uint32_t *mb = nullptr;
         if (pos < total) {
+            const uint64_t item = order ? order[pos] : pos;
             const uint32_t p = find_segment(prefix, npass, item);
             const PassDesc d = passes[p];
-            const uint32_t w = d.src[item - prefix[p]];
-            label_run(g, w, d.label, b, e);
-            mb = d.mbits;
+            label_run(g, d.src[item - prefix[p]], d.label, b, e);
+            s_mb[wid][lane] = d.mbits;
         }
-        scanned += e - b;
-        const bool coop = (e - b) > kLongRun;
-        uint32_t todo = __ballot_sync(0xffffffffu, coop);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            uint32_t *mm = (uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)mb, src);
-            for (uint32_t k = bb + lane; k < ee; k += 32) mark(g, mm, k);
+        s_b[wid][lane] = b;
+        uint64_t inc = e - b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += y;
         }
-        if (!coop)
-            for (uint32_t k = b; k < e; ++k) mark(g, mb, k);
+        s_pre[wid][lane + 1] = inc;
+        if (lane == 0) s_pre[wid][0] = 0;
+        __syncwarp();
+        const uint64_t S = s_pre[wid][32];
+        scanned += S;
+        for (uint64_t j = lane; j < S; j += 32) {
+            // owner: the last item whose run starts at or before j
+            uint32_t lo = 0, hi = 32;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_pre[wid][mid] <= j) lo = mid; else hi = mid;
+            }
+            mark(g, s_mb[wid][lo], s_b[wid][lo] + (uint32_t)(j - s_pre[wid][lo]));
+        }
+        __syncwarp();
     }
-    for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
     if (lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
 }
 
