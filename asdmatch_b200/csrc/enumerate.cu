@@ -368,7 +368,7 @@ struct Warp {
     // fixed list's length minus its conflict vertices and y's own vertex
     // (edge from an earlier level).  Entries of D that are level-(d+1)
     // conflicts are skipped.
-    __device__ bool lane_tail_isect(uint32_t d, uint32_t x, const uint32_t *ya, const uint32_t *yz, bool self,
+    __device__ __forceinline__ bool lane_tail_isect(uint32_t d, uint32_t x, const uint32_t *ya, const uint32_t *yz, bool self,
                                     unsigned long long &out, unsigned long long &touched) {
         const uint32_t a = d + 1;
         const DLevel La = L[a], Lz = L[a + 1];
@@ -1201,7 +1201,7 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
 // Level `s` set up from the prefix in W.idx[0..s-1], restricted to driver
 // positions [lo, hi); then searched to the end.
 template <uint32_t MODE, bool MULTI>
-__device__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint32_t s, uint32_t lo, uint32_t hi,
+__device__ __forceinline__ bool run_range(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint32_t s, uint32_t lo, uint32_t hi,
                           uint32_t &iter, uint64_t deadline) {
     if (W.closed_at(s)) {
         W.setup(s, false);
