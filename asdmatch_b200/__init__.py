@@ -807,7 +807,7 @@ def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float
 
 
 def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
-             min_blocks=(1, 4, 5, 6), lane_leaf=(32, 96, 256), planners=(PLANNER_DP, PLANNER_GREEDY),
+             min_blocks=(1, 3, 4, 5), lane_leaf=(32, 96, 256), planners=(PLANNER_DP, PLANNER_GREEDY),
              root_blocks=(16, 64, 256), run=None):
     """Times the caller's batch under every kernel configuration (with the
     graph's current planner and root-block size), then every planner, then

@@ -91,8 +91,8 @@ extern "C" int asdm_graph_stream(asdm_graph *g, void **stream) {
 
 extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
     if (!g || !t) return fail(ASDM_ERR_INVALID, "null argument");
-    if (t->enum_min_blocks != 1 && (t->enum_min_blocks < 4 || t->enum_min_blocks > 6))
-        return fail(ASDM_ERR_INVALID, "enum_min_blocks must be 1, 4, 5 or 6");
+    if (t->enum_min_blocks < 1 || t->enum_min_blocks > 6)
+        return fail(ASDM_ERR_INVALID, "enum_min_blocks must be 1 to 6");
     if (t->lane_leaf_max > 4096) return fail(ASDM_ERR_INVALID, "lane_leaf_max must be <= 4096");
     if (t->root_block_min < 1 || t->root_block_min > 256) return fail(ASDM_ERR_INVALID, "root_block_min must be 1..256");
     if (t->planner != ASDM_PLANNER_DP && t->planner != ASDM_PLANNER_GREEDY)

@@ -2233,6 +2233,8 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             // register-budget variant chosen by the tuner (min blocks per SM)
             void (*k)(EnumArgs) = enum_batch_kernel<1>;
             switch (G->tuning.enum_min_blocks) {
+                case 2: k = enum_batch_kernel<2>; break;
+                case 3: k = enum_batch_kernel<3>; break;
                 case 4: k = enum_batch_kernel<4>; break;
                 case 5: k = enum_batch_kernel<5>; break;
                 case 6: k = enum_batch_kernel<6>; break;

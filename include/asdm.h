@@ -108,7 +108,7 @@ int asdm_graph_free(asdm_graph *g);
  * (asdmatch_b200.autotune) by timing the caller's own batch.
  *   enum_min_blocks: register budget of the batched enumeration kernel, as
  *     resident 256-thread blocks per SM it must allow (1 = compiler's choice,
- *     4, 5 or 6); more blocks hide more load latency but spill registers.
+ *     up to 6); more blocks hide more load latency but spill registers.
  *   lane_leaf_max: the last query level is evaluated one partial match per
  *     lane (instead of one per warp) when its shortest list has at most this
  *     many entries (the merge / gallop split of the intersection).
