@@ -22,6 +22,7 @@
 // looking a neighbour's index up in C(u2)'s membership bitset and per-word
 // prefix counts.
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <queue>
 
@@ -145,6 +146,23 @@ __global__ void __launch_bounds__(kBlock) k1_filter(FilterArgs a) {
             }
             if (lane == 0 && total) atomicAdd(&a.fcount[u], total);
         }
+    }
+}
+
+// F(u) of query vertices whose filter inputs (label, degree, neighbour-label
+// counts) repeat an earlier vertex of the group: copied from that vertex's
+// bitset instead of filtered again.
+struct CopySeg {
+    const uint32_t *src;
+    uint32_t *dst;
+};
+
+__global__ void __launch_bounds__(kBlock) copy_words(const CopySeg *__restrict__ segs, const uint64_t *__restrict__ prefix,
+                                                     uint32_t nseg) {
+    const uint64_t total = prefix[nseg];
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = find_segment(prefix, nseg, t);
+        segs[k].dst[t - prefix[k]] = segs[k].src[t - prefix[k]];
     }
 }
 
@@ -502,9 +520,14 @@ __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *_
 
 // Dense copy of the padded lists: a lane per item copies a short list, the
 // warp together copies every list longer than 32 entries.
-__global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ upos, const uint32_t *__restrict__ cnt,
+// The same pass turns the counts (cnt) into each item's offset within its
+// edge's list, records each edge's first entry and flags a list offset past
+// 2^32 (the work of k3_offsets).
+__global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ upos, uint32_t *__restrict__ cnt,
                                                   const uint64_t *__restrict__ wpos, uint64_t nitems,
-                                                  const uint32_t *__restrict__ padded, uint32_t *__restrict__ elist) {
+                                                  const uint32_t *__restrict__ padded, uint32_t *__restrict__ elist,
+                                                  const uint64_t *__restrict__ item_base, uint32_t nedges,
+                                                  uint64_t *__restrict__ edge_start, uint32_t *__restrict__ bad) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t base = ((uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < nitems;
@@ -512,6 +535,14 @@ __global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ u
         const uint64_t my = base + lane;
         const uint32_t c = my < nitems ? cnt[my] : 0u;
         const uint64_t from = my < nitems ? upos[my] : 0, to = my < nitems ? wpos[my] : 0;
+        if (my < nitems) {
+            const uint32_t ei = find_segment(item_base, nedges, my);
+            const uint64_t first = item_base[ei];
+            const uint64_t rel = to - wpos[first];
+            if (rel > 0xFFFFFFFFull) atomicExch(bad, 1u);
+            cnt[my] = (uint32_t)rel;
+            if (my == first) edge_start[ei] = to;
+        }
         if (c <= kLongRun)
             for (uint32_t k = 0; k < c; ++k) elist[to + k] = padded[from + k];
         uint32_t todo = __ballot_sync(0xffffffffu, c > kLongRun);
@@ -741,54 +772,101 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             }
         }
     }
-    // segment tables: padded item ranges for K1, bitset layout [F | slot 0 | slot 1 | ...]
-    std::vector<uint64_t> seg(nseg + 1, 0), fword(nseg + 1, 0);
-    std::vector<uint32_t> lbase(nseg), llen(nseg), qdeg(nseg), words(nseg), qnlc, qnlc_off(nseg + 1, 0);
+    // bitset layout [F | slot 0 | slot 1 | ...] per query vertex; K1 filters
+    // one query vertex per distinct (label, degree, neighbour-label counts)
+    // and copies F to the others
+    std::vector<uint64_t> fword(nseg + 1, 0);
+    std::vector<uint32_t> words(nseg);
+    std::vector<uint64_t> seg{0}, kfword;               // K1 segments (distinct signatures)
+    std::vector<uint32_t> lbase, llen, qdeg, qnlc, qnlc_off{0};
+    std::map<std::vector<uint32_t>, uint32_t> sig_k1;   // signature -> K1 segment
+    std::vector<uint32_t> k1_of(nseg);
     for (const QPlan &qp : P) {
         const QueryGraph &q = qp.cs->q;
         for (uint32_t u = 0; u < q.n; ++u) {
             const uint32_t sg = qp.seg0 + u;
             words[sg] = (qp.lsize[u] + 31) / 32;
-            seg[sg + 1] = seg[sg] + 32ull * words[sg];
             fword[sg + 1] = fword[sg] + (uint64_t)(q.deg(u) + 1) * words[sg];
-            lbase[sg] = qp.lbase[u];
-            llen[sg] = qp.lsize[u];
-            qdeg[sg] = q.deg(u);
+            std::vector<uint32_t> sig{q.lab[u], q.deg(u)};
             for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
                 const uint32_t l = q.lab[q.nbr[e]];
-                if (qnlc.size() > 2 * qnlc_off[sg] && qnlc[qnlc.size() - 2] == l) qnlc.back()++;
-                else { qnlc.push_back(l); qnlc.push_back(1); }
+                if (sig.size() > 2 && sig[sig.size() - 2] == l) sig.back()++;
+                else { sig.push_back(l); sig.push_back(1); }
             }
-            qnlc_off[sg + 1] = (uint32_t)(qnlc.size() / 2);
+            auto it = sig_k1.find(sig);
+            if (it != sig_k1.end()) {
+                k1_of[sg] = it->second;
+                continue;
+            }
+            const uint32_t k = (uint32_t)lbase.size();
+            sig_k1.emplace(sig, k);
+            k1_of[sg] = k;
+            seg.push_back(seg.back() + 32ull * words[sg]);
+            kfword.push_back(fword[sg]);
+            lbase.push_back(qp.lbase[u]);
+            llen.push_back(qp.lsize[u]);
+            qdeg.push_back(q.deg(u));
+            qnlc.insert(qnlc.end(), sig.begin() + 2, sig.end());
+            qnlc_off.push_back((uint32_t)(qnlc.size() / 2));
         }
     }
+    const uint32_t nk1 = (uint32_t)lbase.size();
+    kfword.push_back(0);
     uint32_t *bits = nullptr, *d_fcount = nullptr, *d_lbase = nullptr, *d_llen = nullptr, *d_qdeg = nullptr,
              *d_qnlc = nullptr, *d_qnlc_off = nullptr;
     uint64_t *d_seg = nullptr, *d_fword = nullptr;
     unsigned long long *d_elems = nullptr;
     ASDM_TRY(scr.alloc(&bits, fword[nseg]));
     ASDM_CUDA(cudaMemsetAsync(bits, 0, std::max<uint64_t>(fword[nseg], 1) * sizeof(uint32_t), s));
+    if (lbase.empty()) {
+        lbase.push_back(0);
+        llen.push_back(0);
+        qdeg.push_back(0);
+    }
     ASDM_TRY(scr.upload(&d_seg, seg));
-    ASDM_TRY(scr.upload(&d_fword, fword));
+    ASDM_TRY(scr.upload(&d_fword, kfword));
     ASDM_TRY(scr.upload(&d_lbase, lbase));
     ASDM_TRY(scr.upload(&d_llen, llen));
     ASDM_TRY(scr.upload(&d_qdeg, qdeg));
     if (qnlc.empty()) qnlc.push_back(0);
     ASDM_TRY(scr.upload(&d_qnlc, qnlc));
     ASDM_TRY(scr.upload(&d_qnlc_off, qnlc_off));
-    ASDM_TRY(scr.alloc(&d_fcount, nseg));
+    ASDM_TRY(scr.alloc(&d_fcount, std::max<uint32_t>(nk1, 1)));
     ASDM_TRY(scr.alloc(&d_elems, 2));
-    ASDM_CUDA(cudaMemsetAsync(d_fcount, 0, nseg * sizeof(uint32_t), s));
+    ASDM_CUDA(cudaMemsetAsync(d_fcount, 0, std::max<uint32_t>(nk1, 1) * sizeof(uint32_t), s));
     ASDM_CUDA(cudaMemsetAsync(d_elems, 0, 2 * sizeof(unsigned long long), s));
-    if (seg[nseg]) {
-        FilterArgs fa{g, bits, d_seg, d_fword, d_lbase, d_llen, d_qdeg, d_qnlc, d_qnlc_off, nseg, d_fcount};
-        k1_filter<<<grid_for(seg[nseg] / kK1Words, G->num_sms), kBlock, 0, s>>>(fa);
+    if (seg[nk1]) {
+        FilterArgs fa{g, bits, d_seg, d_fword, d_lbase, d_llen, d_qdeg, d_qnlc, d_qnlc_off, nk1, d_fcount};
+        k1_filter<<<grid_for(seg[nk1] / kK1Words, G->num_sms), kBlock, 0, s>>>(fa);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
     }
-    std::vector<uint32_t> fcount(nseg, 0);
-    ASDM_CUDA(cudaMemcpyAsync(fcount.data(), d_fcount, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    uint64_t copied_words = 0;
+    {
+        // F of the repeated signatures
+        std::vector<CopySeg> cps;
+        std::vector<uint64_t> cpre{0};
+        for (uint32_t sg = 0; sg < nseg; ++sg) {
+            const uint32_t k = k1_of[sg];
+            if (kfword[k] == fword[sg]) continue;  // the vertex K1 filtered
+            cps.push_back(CopySeg{bits + kfword[k], bits + fword[sg]});
+            cpre.push_back(cpre.back() + words[sg]);
+        }
+        copied_words = cpre.back();
+        if (!cps.empty() && cpre.back()) {
+            CopySeg *d_cps = nullptr;
+            uint64_t *d_cpre = nullptr;
+            ASDM_TRY(scr.upload(&d_cps, cps));
+            ASDM_TRY(scr.upload(&d_cpre, cpre));
+            copy_words<<<grid_for(cpre.back(), G->num_sms), kBlock, 0, s>>>(d_cps, d_cpre, (uint32_t)cps.size());
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
+        }
+    }
+    std::vector<uint32_t> kcount(std::max<uint32_t>(nk1, 1), 0), fcount(nseg, 0);
+    ASDM_CUDA(cudaMemcpyAsync(kcount.data(), d_fcount, kcount.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     ASDM_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t sg = 0; sg < nseg; ++sg) fcount[sg] = kcount[k1_of[sg]];
 
     uint32_t maxwave = 0;
     for (QPlan &qp : P) {
@@ -1013,8 +1091,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
             ASDM_CUDA(cudaStreamSynchronize(s));
             ASDM_TRY(dalloc(&arena->d_elist, total, s));
-            k3_pack<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_upos, arena->d_eoff, d_wpos, nitems,
-                                                                           padded, arena->d_elist);
+            k3_pack<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_upos, arena->d_eoff, d_wpos, nitems, padded,
+                                                                   arena->d_elist, d_ib, ne, d_estart, d_bad);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         } else {
@@ -1030,10 +1108,11 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                                                     nullptr, nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
+            k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, arena->d_eoff, d_estart,
+                                                                      d_bad);
+            ::asdm::count_launch();
+            ASDM_CUDA(cudaGetLastError());
         }
-        k3_offsets<<<grid_for(nitems, G->num_sms), kBlock, 0, s>>>(d_ib, ne, d_wpos, arena->d_eoff, d_estart, d_bad);
-        ::asdm::count_launch();
-        ASDM_CUDA(cudaGetLastError());
         uint32_t bad = 0;
         ASDM_CUDA(cudaMemcpyAsync(estart.data(), d_estart, ne * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         ASDM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -1048,9 +1127,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     cudaEventElapsedTime(&ms, ev0, ev1);
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
-    // K1 reads 8 bytes per vertex of each query vertex's label; K2 and K3
-    // read one rank per scanned neighbour; compaction reads the bitsets it ANDs
-    const uint64_t bytes = 8ull * seg[nseg] + 4ull * (elems[0] + elems[1]) + 4ull * bit_words_read;
+    // K1 reads 8 bytes per vertex of the label of each distinct query-vertex
+    // signature (and copies F words for the repeats); K2 and K3 read one rank
+    // per scanned neighbour; compaction reads the bitsets it ANDs
+    const uint64_t bytes = 8ull * seg.back() + 8ull * copied_words + 4ull * (elems[0] + elems[1]) + 4ull * bit_words_read;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         QPlan &qp = P[qi];
         asdm_cs &cs = *qp.cs;
