@@ -241,6 +241,126 @@ __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__
     if (lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
 }
 
+// Pull form of a marking pass (p -> u): the bit of each candidate x of u
+// (F(u) for passes from earlier BFS neighbours, Ctd(u) for the later ones:
+// the final AND discards the rest) is set when some neighbour of x with label
+// l(p) lies in Ctd(p).  Same bits on those candidates as pushing from S(p);
+// the phantom vertex 0 of S(p) is pushed separately.  A warp takes 32 words
+// of candidates; each lane scans one candidate's label run, stopping at its
+// first member of Ctd(p), and runs left open after kPullLane entries are
+// finished by the whole warp 32 entries at a time.
+struct PullDesc {
+    const uint32_t *xbits;   // candidates to test, by rank in l(u)
+    uint32_t *mbits;         // u's slot bitset for p
+    const uint32_t *sbits;   // membership of Ctd(p), by rank in l(p)
+    uint32_t lbase;          // vbl_off[l(u)]
+    uint32_t label;          // l(p)
+    uint32_t words;          // words of xbits
+    uint32_t pad;
+};
+
+constexpr uint32_t kPullLane = 16;
+
+// Position of the n-th (0-based) set bit of w; n < popc(w).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t n) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t width = 16; width; width >>= 1) {
+        const uint32_t low = __popc(w & ((1u << width) - 1u));
+        if (n >= low) {
+            n -= low;
+            w >>= width;
+            pos += width;
+        }
+    }
+    return pos;
+}
+
+__device__ __forceinline__ bool pull_member(const DevGraph &g, const uint32_t *sb, uint32_t k) {
+    const uint32_t z = g.nbr_rank[k];
+    return (sb[z >> 5] >> (z & 31u)) & 1u;
+}
+
+__global__ void __launch_bounds__(kBlock) k2_pull(DevGraph g, const PullDesc *__restrict__ passes,
+                                                  const uint64_t *__restrict__ group_pre, uint32_t npass,
+                                                  unsigned long long *__restrict__ elems) {
+    constexpr uint32_t kWarps = kBlock / 32;
+    __shared__ uint32_t s_out[kWarps][32];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t ngroups = group_pre[npass];
+    const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+    uint64_t scanned = 0;
+    s_out[wid][lane] = 0;
+    __syncwarp();
+    for (uint64_t grp = (uint64_t)blockIdx.x * kWarps + wid; grp < ngroups; grp += nwarps) {
+        const uint32_t pi = find_segment(group_pre, npass, grp);
+        const PullDesc d = passes[pi];
+        const uint32_t w0 = (uint32_t)(grp - group_pre[pi]) * 32;
+        const uint32_t f = (w0 + lane < d.words) ? d.xbits[w0 + lane] : 0u;
+        // inclusive prefix of the candidates per word
+        uint32_t pre = __popc(f);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= (uint32_t)o) pre += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, pre, 31);
+        for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+            const uint32_t t = t0 + lane;
+            // owner word: the first lane whose inclusive prefix exceeds t
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step; step >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, pre, o + step - 1);
+                if (v <= t) o += step;
+            }
+            o = min(o, 31u);
+            const uint32_t word = __shfl_sync(0xffffffffu, f, o);
+            const uint32_t before = __shfl_sync(0xffffffffu, pre - __popc(f), o);
+            const bool mine = t < total;
+            uint32_t bit = 0, b = 0, e = 0;
+            if (mine) {
+                bit = nth_set_bit(word, t - before);
+                const uint32_t x = g.vbl[d.lbase + 32 * (w0 + o) + bit];
+                label_run(g, x, d.label, b, e);
+            }
+            bool hit = false;
+            const uint32_t stop = min(e, b + kPullLane);
+            uint32_t k = b;
+            for (; k < stop && !hit; ++k) hit = pull_member(g, d.sbits, k);
+            scanned += k - b;
+            // runs still open: the whole warp scans them
+            uint32_t todo = __ballot_sync(0xffffffffu, mine && !hit && k < e);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t kk = __shfl_sync(0xffffffffu, k, src), ee = __shfl_sync(0xffffffffu, e, src);
+                bool found = false;
+                uint32_t seen = 0;
+                for (uint32_t base = kk; base < ee && !found; base += 32) {
+                    const uint32_t j = base + lane;
+                    found = __any_sync(0xffffffffu, j < ee && pull_member(g, d.sbits, j));
+                    seen += min(32u, ee - base);
+                }
+                if ((int)lane == src) {
+                    hit = found;
+                    scanned += seen;
+                }
+            }
+            if (hit) atomicOr(&s_out[wid][o], 1u << bit);
+        }
+        __syncwarp();
+        const uint32_t m = s_out[wid][lane];
+        if (m) {
+            atomicOr(&d.mbits[w0 + lane], m);
+            s_out[wid][lane] = 0;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o; o >>= 1) scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
+    if (lane == 0 && scanned) atomicAdd(elems, (unsigned long long)scanned);
+}
+
 // ---- K3a: compaction of bitsets into vertex lists, word by word ------------
 constexpr int kItems = 8;               // words per thread
 constexpr int kTile = kBlock * kItems;  // words per tile
@@ -254,6 +374,7 @@ struct CompDesc {
     uint32_t phantom;       // append data vertex 0 when fewer than len survive
     uint32_t pad;
     uint2 *cmem;            // or null: per word of the result, {membership bits, result size before it}
+    uint32_t *sbits;        // or null: the result's membership bits alone
 };
 
 __device__ __forceinline__ uint32_t comp_word(const CompDesc &d, uint32_t w) {
@@ -329,6 +450,7 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
         const uint32_t w = my + k;
         if (w >= d.words) break;
         if (d.cmem) d.cmem[w] = make_uint2(x[k], pos);
+        if (d.sbits) d.sbits[w] = x[k];
         for (uint32_t y = x[k]; y; y &= y - 1) o[pos++] = vbl[d.lbase + 32 * w + (uint32_t)(__ffs(y) - 1)];
     }
     // the last tile of a segment records the segment size
@@ -575,14 +697,16 @@ unsigned grid_for(uint64_t items, int num_sms) {
 
 // One compaction over the given segments into one new device buffer (*out,
 // the caller frees it): segment i's vertices at *out + start[i], size[i] of
-// them (plus, where asked, the phantom vertex).
+// them (plus, where asked, the phantom vertex; (*added)[i] says whether it
+// was appended).
 int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, std::vector<uint64_t> &start,
-            std::vector<uint32_t> &sizes) {
+            std::vector<uint32_t> &sizes, std::vector<char> *added = nullptr) {
     cudaStream_t s = G->stream;
     const uint32_t nseg = (uint32_t)segs.size();
     *out = nullptr;
     sizes.assign(nseg, 0);
     start.assign(nseg, 0);
+    if (added) added->assign(nseg, 0);
     if (nseg == 0) return ASDM_OK;
     std::vector<uint64_t> tile_first(nseg + 1, 0);
     for (uint32_t i = 0; i < nseg; ++i) tile_first[i + 1] = tile_first[i] + (segs[i].words + kTile - 1) / kTile;
@@ -628,6 +752,10 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
             break;
         }
         for (uint32_t i = 0; i < nseg; ++i) start[i] = pos[tile_first[i]] + i;
+        if (added) {
+            // segments that got the phantom vertex 0 appended
+            for (uint32_t i = 0; i < nseg; ++i) (*added)[i] = sizes[i] != pos[tile_first[i + 1]] - pos[tile_first[i]];
+        }
     } while (false);
     dfree(d_segs, s); dfree(d_tf, s); dfree(d_cnt, s); dfree(d_pos, s); dfree(d_sc, s);
     if (rc != ASDM_OK) dfree(*out, s);
@@ -700,6 +828,35 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     dfree(order, s);
     dfree(d_p, s);
     dfree(d_prefix, s);
+    return rc;
+}
+
+// All pull passes of one phase in one launch.
+int run_pulls(asdm_graph *G, const std::vector<PullDesc> &pulls, unsigned long long *d_elems) {
+    cudaStream_t s = G->stream;
+    const uint32_t np = (uint32_t)pulls.size();
+    if (np == 0) return ASDM_OK;
+    std::vector<uint64_t> gpre(np + 1, 0);
+    for (uint32_t i = 0; i < np; ++i) gpre[i + 1] = gpre[i] + (pulls[i].words + 31) / 32;
+    if (gpre[np] == 0) return ASDM_OK;
+    PullDesc *d_p = nullptr;
+    uint64_t *d_pre = nullptr;
+    int rc = ASDM_OK;
+    do {
+        if ((rc = dalloc(&d_p, np, s)) || (rc = dalloc(&d_pre, np + 1, s))) break;
+        if (upload_async(G, d_p, pulls.data(), np * sizeof(PullDesc)) != cudaSuccess ||
+            upload_async(G, d_pre, gpre.data(), (np + 1) * sizeof(uint64_t)) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "pull-pass upload failed");
+            break;
+        }
+        const uint64_t blocks = (gpre[np] + kBlock / 32 - 1) / (kBlock / 32);
+        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)G->num_sms * 32));
+        k2_pull<<<grid, kBlock, 0, s>>>(G->d, d_p, d_pre, np, d_elems);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "pull pass failed");
+    } while (false);
+    dfree(d_p, s);
+    dfree(d_pre, s);
     return rc;
 }
 
@@ -925,12 +1082,33 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             maxwave = std::max(maxwave, qp.wave[u]);
         }
     }
-    // storage S(u) = Ctd(u) (+ vertex 0), one buffer per wave
-    std::vector<const uint32_t *> sptr(nseg, nullptr);
-    std::vector<uint64_t> slen(nseg, 0);
+    // Ctd(u) as a membership bitset per query vertex (and whether the
+    // storage S(u) scanned by the reference gets the phantom vertex 0)
+    std::vector<uint64_t> mword(nseg + 1, 0);
+    for (uint32_t i = 0; i < nseg; ++i) mword[i + 1] = mword[i] + words[i];
+    uint32_t *sbits = nullptr, *d_zero = nullptr;
+    ASDM_TRY(scr.alloc(&sbits, std::max<uint64_t>(mword[nseg], 1)));
+    ASDM_TRY(scr.alloc(&d_zero, 1));
+    ASDM_CUDA(cudaMemsetAsync(d_zero, 0, sizeof(uint32_t), s));
+    std::vector<char> phantom(nseg, 0);
     uint64_t bit_words_read = 0;
+    // a pass p -> u: pulled over u's candidates, plus the push of the phantom
+    // vertex when S(p) has it
+    auto add_pass = [&](std::vector<PullDesc> &pulls, std::vector<PassDesc> &pushes, std::vector<uint64_t> &lens,
+                        const QPlan &qp, uint32_t u, uint32_t e, const uint32_t *xbits) {
+        const QueryGraph &q = qp.cs->q;
+        const uint32_t p = q.nbr[e], su = qp.seg0 + u, sp = qp.seg0 + p, slot = e - q.off[u];
+        uint32_t *mb = bits + fword[su] + (1ull + slot) * words[su];
+        pulls.push_back(PullDesc{xbits, mb, sbits + mword[sp], qp.lbase[u], q.lab[p], words[su], 0});
+        bit_words_read += words[su];
+        if (phantom[sp]) {
+            pushes.push_back(PassDesc{d_zero, mb, q.lab[u], 0});
+            lens.push_back(1);
+        }
+    };
     for (uint32_t w = 0; w <= maxwave; ++w) {
-        std::vector<PassDesc> passes;
+        std::vector<PullDesc> pulls;
+        std::vector<PassDesc> pushes;
         std::vector<uint64_t> lens;
         std::vector<CompDesc> segs;
         std::vector<uint32_t> seg_ids;
@@ -942,53 +1120,48 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                 const uint32_t su = qp.seg0 + u;
                 uint32_t need = 0;
                 for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-                    const uint32_t p = q.nbr[e];
-                    if (qp.rank[p] >= qp.rank[u]) continue;
-                    const uint32_t slot = e - q.off[u];
-                    need |= 1u << slot;
-                    passes.push_back(PassDesc{sptr[qp.seg0 + p], bits + fword[su] + (1ull + slot) * words[su], q.lab[u], 0});
-                    lens.push_back(slen[qp.seg0 + p]);
+                    if (qp.rank[q.nbr[e]] >= qp.rank[u]) continue;
+                    need |= 1u << (e - q.off[u]);
+                    add_pass(pulls, pushes, lens, qp, u, e, bits + fword[su]);  // over F(u)
                 }
-                segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr});
+                segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr,
+                                        sbits + mword[su]});
                 seg_ids.push_back(su);
                 bit_words_read += (uint64_t)(1 + __builtin_popcount(need)) * words[su];
             }
         }
-        ASDM_TRY(run_passes(G, passes, lens, d_elems));
+        ASDM_TRY(run_pulls(G, pulls, d_elems));
+        ASDM_TRY(run_passes(G, pushes, lens, d_elems));
         uint32_t *sbuf = nullptr;
         std::vector<uint64_t> start;
         std::vector<uint32_t> sizes;
-        ASDM_TRY(compact(G, segs, &sbuf, start, sizes));
+        std::vector<char> added;
+        ASDM_TRY(compact(G, segs, &sbuf, start, sizes, &added));
         scr.keep(sbuf);
-        for (size_t i = 0; i < seg_ids.size(); ++i) {
-            sptr[seg_ids[i]] = sbuf + start[i];
-            slen[seg_ids[i]] = sizes[i];
-        }
+        for (size_t i = 0; i < seg_ids.size(); ++i) phantom[seg_ids[i]] = added[i];
     }
-    // remaining passes (neighbours later in the BFS order), all queries at once
+    // remaining passes (neighbours later in the BFS order), all queries at
+    // once, over Ctd(u)
     {
-        std::vector<PassDesc> passes;
+        std::vector<PullDesc> pulls;
+        std::vector<PassDesc> pushes;
         std::vector<uint64_t> lens;
         for (const QPlan &qp : P) {
             if (qp.empty) continue;
             const QueryGraph &q = qp.cs->q;
             for (uint32_t u = 0; u < q.n; ++u)
                 for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
-                    const uint32_t p = q.nbr[e];
-                    if (qp.rank[p] < qp.rank[u]) continue;
-                    const uint32_t su = qp.seg0 + u, slot = e - q.off[u];
-                    passes.push_back(PassDesc{sptr[qp.seg0 + p], bits + fword[su] + (1ull + slot) * words[su], q.lab[u], 0});
-                    lens.push_back(slen[qp.seg0 + p]);
+                    if (qp.rank[q.nbr[e]] < qp.rank[u]) continue;
+                    add_pass(pulls, pushes, lens, qp, u, e, sbits + mword[qp.seg0 + u]);
                 }
         }
-        ASDM_TRY(run_passes(G, passes, lens, d_elems));
+        ASDM_TRY(run_pulls(G, pulls, d_elems));
+        ASDM_TRY(run_passes(G, pushes, lens, d_elems));
     }
     // final candidate sets into the group's arena, with the membership
     // bitsets and per-word prefix counts that K3 looks indices up in
     auto arena = std::make_shared<CsArena>();
     arena->stream = s;
-    std::vector<uint64_t> mword(nseg + 1, 0);
-    for (uint32_t i = 0; i < nseg; ++i) mword[i + 1] = mword[i] + words[i];
     uint2 *cmem = nullptr;
     ASDM_TRY(scr.alloc(&cmem, mword[nseg]));
     {
