@@ -47,44 +47,6 @@ __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ pr
     return lo;
 }
 
-// ---- Visiting order: items grouped by the data vertex they read ------------
-// A K2 work item reads one storage vertex's label runs and adjacency.  Items
-// of a group arrive in per-query order, so popular vertices would be fetched
-// from HBM once per query and pass; grouping the items by vertex id block
-// (kBucketShift) keeps a block's adjacency in L2 while its items run.  The
-// order inside a block does not matter: marking is an atomic OR.
-constexpr uint32_t kBucketShift = 12;
-
-__global__ void bucket_count(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ cnt) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-        const uint64_t i = base + lane;
-        const bool valid = i < n;
-        const uint32_t key = valid ? keys[i] : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        if (valid && (uint32_t)(__ffs(peers) - 1) == lane) atomicAdd(&cnt[key], (unsigned long long)__popc(peers));
-    }
-}
-
-// cursor: exclusive prefix of the counts; order[cursor[key]++] = item
-__global__ void bucket_scatter(const uint32_t *__restrict__ keys, uint64_t n, unsigned long long *__restrict__ cursor,
-                               uint32_t *__restrict__ order) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-        const uint64_t i = base + lane;
-        const bool valid = i < n;
-        const uint32_t key = valid ? keys[i] : 0xFFFFFFFFu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-        unsigned long long at = 0;
-        if (valid && leader == lane) at = atomicAdd(&cursor[key], (unsigned long long)__popc(peers));
-        at = __shfl_sync(0xffffffffu, at, leader);
-        if (valid) order[at + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)i;
-    }
-}
-
 // ---- K1: label + degree + NLC filter --------------------------------------
 // One segment per (query, query vertex) of a group; a segment's items are
 // the ranks 0 .. |V_l(u)| - 1 of u's label, padded to a multiple of 32 so
@@ -167,8 +129,10 @@ __global__ void __launch_bounds__(kBlock) copy_words(const CopySeg *__restrict__
 }
 
 // ---- K2: neighbour marking passes -------------------------------------------
+// Push form (used for the phantom vertex 0 of a storage): every l(u)-neighbour
+// of a listed vertex gets its bit in u's slot bitset.
 struct PassDesc {
-    const uint32_t *src;  // storage S(p): vertex ids
+    const uint32_t *src;  // vertex ids
     uint32_t *mbits;      // u's bitset for p
     uint32_t label;       // l(u)
     uint32_t pad;
@@ -179,23 +143,11 @@ __device__ __forceinline__ void mark(const DevGraph &g, uint32_t *mb, uint32_t k
     atomicOr(&mb[r >> 5], 1u << (r & 31u));  // result unused: a fire-and-forget reduction
 }
 
-// Bucket keys of the pass items (storage vertex >> kBucketShift).
-__global__ void k2_keys(const PassDesc *__restrict__ passes, const uint64_t *__restrict__ prefix, uint32_t npass,
-                        uint32_t *__restrict__ keys) {
-    const uint64_t total = prefix[npass];
-    for (uint64_t item = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; item < total;
-         item += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = find_segment(prefix, npass, item);
-        keys[item] = passes[p].src[item - prefix[p]] >> kBucketShift;
-    }
-}
-
 // A warp takes 32 items and marks the concatenation of their label runs 32
 // entries at a time, a lane per entry (every lane has a reduction to issue,
 // whatever the run lengths).
 __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__restrict__ passes,
                                                   const uint64_t *__restrict__ prefix, uint32_t npass,
-                                                  const uint32_t *__restrict__ order,
                                                   unsigned long long *__restrict__ elems) {
     constexpr uint32_t kWarps = kBlock / 32;
     __shared__ uint64_t s_pre[kWarps][33];   // exclusive prefix of the run lengths (s_pre[32] = total)
@@ -209,7 +161,7 @@ __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__
         const uint64_t pos = base + lane;
         uint32_t b = 0, e = 0;
         if (pos < total) {
-            const uint64_t item = order ? order[pos] : pos;
+            const uint64_t item = pos;
             const uint32_t p = find_segment(prefix, npass, item);
             const PassDesc d = passes[p];
             label_run(g, d.src[item - prefix[p]], d.label, b, e);
@@ -443,7 +395,7 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
     }
     __syncthreads();
     const uint64_t seg_first = tile_pos[tile_first[sidx]];
-    uint32_t *o = out + seg_first + sidx;
+    uint32_t *o = out ? out + seg_first + sidx : nullptr;  // null: sizes and bitsets only
     uint32_t pos = (uint32_t)(tile_pos[t] - seg_first) + (warp ? wsum[warp - 1] : 0) + v - c;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
@@ -451,12 +403,16 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
         if (w >= d.words) break;
         if (d.cmem) d.cmem[w] = make_uint2(x[k], pos);
         if (d.sbits) d.sbits[w] = x[k];
-        for (uint32_t y = x[k]; y; y &= y - 1) o[pos++] = vbl[d.lbase + 32 * w + (uint32_t)(__ffs(y) - 1)];
+        if (o)
+            for (uint32_t y = x[k]; y; y &= y - 1) o[pos++] = vbl[d.lbase + 32 * w + (uint32_t)(__ffs(y) - 1)];
     }
     // the last tile of a segment records the segment size
     if (threadIdx.x == 0 && t + 1 == tile_first[sidx + 1]) {
         uint32_t size = (uint32_t)(tile_pos[t + 1] - seg_first);
-        if (d.phantom && size < d.len) o[size++] = 0;  // the reference's zero-filled storage tail
+        if (d.phantom && size < d.len) {  // the reference's zero-filled storage tail
+            if (o) o[size] = 0;
+            ++size;
+        }
         seg_count[sidx] = size;
     }
 }
@@ -698,12 +654,13 @@ unsigned grid_for(uint64_t items, int num_sms) {
 // One compaction over the given segments into one new device buffer (*out,
 // the caller frees it): segment i's vertices at *out + start[i], size[i] of
 // them (plus, where asked, the phantom vertex; (*added)[i] says whether it
-// was appended).
+// was appended).  With out null only the sizes and the segments' bitset
+// outputs are produced.
 int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, std::vector<uint64_t> &start,
             std::vector<uint32_t> &sizes, std::vector<char> *added = nullptr) {
     cudaStream_t s = G->stream;
     const uint32_t nseg = (uint32_t)segs.size();
-    *out = nullptr;
+    if (out) *out = nullptr;
     sizes.assign(nseg, 0);
     start.assign(nseg, 0);
     if (added) added->assign(nseg, 0);
@@ -718,7 +675,7 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
     std::vector<uint64_t> pos(ntiles + 1, 0);
     do {
         if (ntiles == 0) {
-            if ((rc = dalloc(out, nseg, s))) break;
+            if (out && (rc = dalloc(out, nseg, s))) break;
             for (uint32_t i = 0; i < nseg; ++i) start[i] = i;
             break;
         }
@@ -742,8 +699,8 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
             rc = fail(ASDM_ERR_CUDA, "compaction readback failed");
             break;
         }
-        if ((rc = dalloc(out, pos[ntiles] + nseg, s))) break;
-        k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, *out, d_sc);
+        if (out && (rc = dalloc(out, pos[ntiles] + nseg, s))) break;
+        k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, out ? *out : nullptr, d_sc);
         ::asdm::count_launch();
         if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "compaction write failed"); break; }
         if (cudaMemcpyAsync(sizes.data(), d_sc, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -758,38 +715,7 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
         }
     } while (false);
     dfree(d_segs, s); dfree(d_tf, s); dfree(d_cnt, s); dfree(d_pos, s); dfree(d_sc, s);
-    if (rc != ASDM_OK) dfree(*out, s);
-    return rc;
-}
-
-// Positions of n items grouped by their keys (vertex blocks) into *order (the
-// caller frees it); *order stays null when n does not fit 32-bit positions
-// or is too small to matter.
-int bucket_order(asdm_graph *G, const uint32_t *d_keys, uint64_t n, uint64_t nb, uint32_t **order) {
-    cudaStream_t s = G->stream;
-    *order = nullptr;
-    if (n < (1u << 16) || n >= 0xFFFFFFFFull) return ASDM_OK;
-    unsigned long long *cnt = nullptr;
-    uint64_t *cur = nullptr;
-    int rc = ASDM_OK;
-    do {
-        if ((rc = dalloc(&cnt, nb, s)) || (rc = dalloc(&cur, nb + 1, s)) || (rc = dalloc(order, n, s))) break;
-        if (cudaMemsetAsync(cnt, 0, nb * sizeof(unsigned long long), s) != cudaSuccess) {
-            rc = fail(ASDM_ERR_CUDA, "bucket reset failed");
-            break;
-        }
-        bucket_count<<<grid_for(n, G->num_sms), kBlock, 0, s>>>(d_keys, n, cnt);
-        ::asdm::count_launch();
-        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "bucket count failed"); break; }
-        if ((rc = scan_exclusive_u64(reinterpret_cast<const uint64_t *>(cnt), cur, nb, true, s))) break;
-        bucket_scatter<<<grid_for(n, G->num_sms), kBlock, 0, s>>>(d_keys, n, reinterpret_cast<unsigned long long *>(cur),
-                                                                   *order);
-        ::asdm::count_launch();
-        if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "bucket scatter failed"); break; }
-    } while (false);
-    dfree(cnt, s);
-    dfree(cur, s);
-    if (rc != ASDM_OK) dfree(*order, s);
+    if (rc != ASDM_OK && out) dfree(*out, s);
     return rc;
 }
 
@@ -807,25 +733,10 @@ int run_passes(asdm_graph *G, const std::vector<PassDesc> &passes, const std::ve
     ASDM_TRY(dalloc(&d_prefix, np + 1, s));
     ASDM_CUDA(upload_async(G, d_p, passes.data(), np * sizeof(PassDesc)));
     ASDM_CUDA(upload_async(G, d_prefix, prefix.data(), (np + 1) * sizeof(uint64_t)));
-    uint32_t *keys = nullptr, *order = nullptr;
     int rc = ASDM_OK;
-    if (prefix[np] >= (1u << 16) && prefix[np] < 0xFFFFFFFFull) {
-        rc = dalloc(&keys, prefix[np], s);
-        if (rc == ASDM_OK) {
-            k2_keys<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(d_p, d_prefix, np, keys);
-            ::asdm::count_launch();
-            rc = cudaGetLastError() == cudaSuccess
-                     ? bucket_order(G, keys, prefix[np], ((uint64_t)G->d.n >> kBucketShift) + 1, &order)
-                                                   : fail(ASDM_ERR_CUDA, "pass key kernel failed");
-        }
-    }
-    if (rc == ASDM_OK) {
-        k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, order, d_elems);
-        ::asdm::count_launch();
-        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
-    }
-    dfree(keys, s);
-    dfree(order, s);
+    k2_pass<<<grid_for(prefix[np], G->num_sms), kBlock, 0, s>>>(G->d, d_p, d_prefix, np, d_elems);
+    ::asdm::count_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "marking pass failed");
     dfree(d_p, s);
     dfree(d_prefix, s);
     return rc;
@@ -1132,12 +1043,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         }
         ASDM_TRY(run_pulls(G, pulls, d_elems));
         ASDM_TRY(run_passes(G, pushes, lens, d_elems));
-        uint32_t *sbuf = nullptr;
         std::vector<uint64_t> start;
         std::vector<uint32_t> sizes;
         std::vector<char> added;
-        ASDM_TRY(compact(G, segs, &sbuf, start, sizes, &added));
-        scr.keep(sbuf);
+        ASDM_TRY(compact(G, segs, nullptr, start, sizes, &added));  // Ctd(u) bitsets; no vertex lists
         for (size_t i = 0; i < seg_ids.size(); ++i) phantom[seg_ids[i]] = added[i];
     }
     // remaining passes (neighbours later in the BFS order), all queries at
