@@ -132,10 +132,11 @@ __global__ void __launch_bounds__(kBlock) copy_words(const CopySeg *__restrict__
 // Push form (used for the phantom vertex 0 of a storage): every l(u)-neighbour
 // of a listed vertex gets its bit in u's slot bitset.
 struct PassDesc {
-    const uint32_t *src;  // vertex ids
-    uint32_t *mbits;      // u's bitset for p
-    uint32_t label;       // l(u)
+    const uint32_t *src;   // vertex ids
+    uint32_t *mbits;       // u's bitset for p
+    uint32_t label;        // l(u)
     uint32_t pad;
+    const uint32_t *cond;  // or null: the pass runs only where *cond is nonzero
 };
 
 __device__ __forceinline__ void mark(const DevGraph &g, uint32_t *mb, uint32_t k) {
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(kBlock) k2_pass(DevGraph g, const PassDesc *__
             const uint64_t item = pos;
             const uint32_t p = find_segment(prefix, npass, item);
             const PassDesc d = passes[p];
-            label_run(g, d.src[item - prefix[p]], d.label, b, e);
+            if (!d.cond || *d.cond) label_run(g, d.src[item - prefix[p]], d.label, b, e);
             s_mb[wid][lane] = d.mbits;
         }
         s_b[wid][lane] = b;
@@ -327,6 +328,7 @@ struct CompDesc {
     uint32_t pad;
     uint2 *cmem;            // or null: per word of the result, {membership bits, result size before it}
     uint32_t *sbits;        // or null: the result's membership bits alone
+    uint32_t *ph;           // or null: set to 1 when the phantom vertex was appended, else 0
 };
 
 __device__ __forceinline__ uint32_t comp_word(const CompDesc &d, uint32_t w) {
@@ -409,10 +411,12 @@ __global__ void __launch_bounds__(kBlock) k3_write(const CompDesc *__restrict__ 
     // the last tile of a segment records the segment size
     if (threadIdx.x == 0 && t + 1 == tile_first[sidx + 1]) {
         uint32_t size = (uint32_t)(tile_pos[t + 1] - seg_first);
-        if (d.phantom && size < d.len) {  // the reference's zero-filled storage tail
+        const bool ph = d.phantom && size < d.len;  // the reference's zero-filled storage tail
+        if (ph) {
             if (o) o[size] = 0;
             ++size;
         }
+        if (d.ph) *d.ph = ph ? 1u : 0u;
         seg_count[sidx] = size;
     }
 }
@@ -653,17 +657,16 @@ unsigned grid_for(uint64_t items, int num_sms) {
 
 // One compaction over the given segments into one new device buffer (*out,
 // the caller frees it): segment i's vertices at *out + start[i], size[i] of
-// them (plus, where asked, the phantom vertex; (*added)[i] says whether it
-// was appended).  With out null only the sizes and the segments' bitset
-// outputs are produced.
+// them (plus, where asked, the phantom vertex).  With out null only the
+// segments' device outputs (bitsets, phantom flags) are produced, with no
+// wait for the device.
 int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, std::vector<uint64_t> &start,
-            std::vector<uint32_t> &sizes, std::vector<char> *added = nullptr) {
+            std::vector<uint32_t> &sizes) {
     cudaStream_t s = G->stream;
     const uint32_t nseg = (uint32_t)segs.size();
     if (out) *out = nullptr;
     sizes.assign(nseg, 0);
     start.assign(nseg, 0);
-    if (added) added->assign(nseg, 0);
     if (nseg == 0) return ASDM_OK;
     std::vector<uint64_t> tile_first(nseg + 1, 0);
     for (uint32_t i = 0; i < nseg; ++i) tile_first[i + 1] = tile_first[i] + (segs[i].words + kTile - 1) / kTile;
@@ -693,14 +696,21 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
         ::asdm::count_launch();
         if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "compaction count failed"); break; }
         if ((rc = scan_exclusive_u32(d_cnt, d_pos, ntiles, true, s))) break;
+        if (!out) {
+            // bitsets and flags only: nothing for the host to read back
+            k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, nullptr, d_sc);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "compaction write failed");
+            break;
+        }
         if (cudaMemcpyAsync(pos.data(), d_pos, (ntiles + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s) !=
                 cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "compaction readback failed");
             break;
         }
-        if (out && (rc = dalloc(out, pos[ntiles] + nseg, s))) break;
-        k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, out ? *out : nullptr, d_sc);
+        if ((rc = dalloc(out, pos[ntiles] + nseg, s))) break;
+        k3_write<<<(unsigned)ntiles, kBlock, 0, s>>>(d_segs, d_tf, nseg, d_pos, G->d.vbl, *out, d_sc);
         ::asdm::count_launch();
         if (cudaGetLastError() != cudaSuccess) { rc = fail(ASDM_ERR_CUDA, "compaction write failed"); break; }
         if (cudaMemcpyAsync(sizes.data(), d_sc, nseg * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -709,10 +719,6 @@ int compact(asdm_graph *G, const std::vector<CompDesc> &segs, uint32_t **out, st
             break;
         }
         for (uint32_t i = 0; i < nseg; ++i) start[i] = pos[tile_first[i]] + i;
-        if (added) {
-            // segments that got the phantom vertex 0 appended
-            for (uint32_t i = 0; i < nseg; ++i) (*added)[i] = sizes[i] != pos[tile_first[i + 1]] - pos[tile_first[i]];
-        }
     } while (false);
     dfree(d_segs, s); dfree(d_tf, s); dfree(d_cnt, s); dfree(d_pos, s); dfree(d_sc, s);
     if (rc != ASDM_OK && out) dfree(*out, s);
@@ -997,14 +1003,16 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     // storage S(u) scanned by the reference gets the phantom vertex 0)
     std::vector<uint64_t> mword(nseg + 1, 0);
     for (uint32_t i = 0; i < nseg; ++i) mword[i + 1] = mword[i] + words[i];
-    uint32_t *sbits = nullptr, *d_zero = nullptr;
+    uint32_t *sbits = nullptr, *d_zero = nullptr, *d_ph = nullptr;
     ASDM_TRY(scr.alloc(&sbits, std::max<uint64_t>(mword[nseg], 1)));
     ASDM_TRY(scr.alloc(&d_zero, 1));
+    ASDM_TRY(scr.alloc(&d_ph, std::max<uint32_t>(nseg, 1)));
     ASDM_CUDA(cudaMemsetAsync(d_zero, 0, sizeof(uint32_t), s));
-    std::vector<char> phantom(nseg, 0);
+    ASDM_CUDA(cudaMemsetAsync(d_ph, 0, std::max<uint32_t>(nseg, 1) * sizeof(uint32_t), s));
     uint64_t bit_words_read = 0;
     // a pass p -> u: pulled over u's candidates, plus the push of the phantom
-    // vertex when S(p) has it
+    // vertex, which runs where S(p) has it (a flag the compaction of Ctd(p)
+    // sets on the device: the waves run without host reads)
     auto add_pass = [&](std::vector<PullDesc> &pulls, std::vector<PassDesc> &pushes, std::vector<uint64_t> &lens,
                         const QPlan &qp, uint32_t u, uint32_t e, const uint32_t *xbits) {
         const QueryGraph &q = qp.cs->q;
@@ -1012,17 +1020,14 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         uint32_t *mb = bits + fword[su] + (1ull + slot) * words[su];
         pulls.push_back(PullDesc{xbits, mb, sbits + mword[sp], qp.lbase[u], q.lab[p], words[su], 0});
         bit_words_read += words[su];
-        if (phantom[sp]) {
-            pushes.push_back(PassDesc{d_zero, mb, q.lab[u], 0});
-            lens.push_back(1);
-        }
+        pushes.push_back(PassDesc{d_zero, mb, q.lab[u], 0, d_ph + sp});
+        lens.push_back(1);
     };
     for (uint32_t w = 0; w <= maxwave; ++w) {
         std::vector<PullDesc> pulls;
         std::vector<PassDesc> pushes;
         std::vector<uint64_t> lens;
         std::vector<CompDesc> segs;
-        std::vector<uint32_t> seg_ids;
         for (const QPlan &qp : P) {
             if (qp.empty) continue;
             const QueryGraph &q = qp.cs->q;
@@ -1036,8 +1041,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
                     add_pass(pulls, pushes, lens, qp, u, e, bits + fword[su]);  // over F(u)
                 }
                 segs.push_back(CompDesc{bits + fword[su], words[su], need, qp.lsize[u], qp.lbase[u], 1, 0, nullptr,
-                                        sbits + mword[su]});
-                seg_ids.push_back(su);
+                                        sbits + mword[su], d_ph + su});
                 bit_words_read += (uint64_t)(1 + __builtin_popcount(need)) * words[su];
             }
         }
@@ -1045,9 +1049,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         ASDM_TRY(run_passes(G, pushes, lens, d_elems));
         std::vector<uint64_t> start;
         std::vector<uint32_t> sizes;
-        std::vector<char> added;
-        ASDM_TRY(compact(G, segs, nullptr, start, sizes, &added));  // Ctd(u) bitsets; no vertex lists
-        for (size_t i = 0; i < seg_ids.size(); ++i) phantom[seg_ids[i]] = added[i];
+        ASDM_TRY(compact(G, segs, nullptr, start, sizes));  // Ctd(u) bitsets and phantom flags only
     }
     // remaining passes (neighbours later in the BFS order), all queries at
     // once, over Ctd(u)

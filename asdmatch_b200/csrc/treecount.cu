@@ -97,7 +97,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
         const unsigned long long t = base + lane;
         const bool valid = t < total;
         TreeSeg sg{};
-        uint32_t i = 0;
+        uint32_t i = 0, seg = 0xFFFFFFFFu;
         bool alive = valid;
         if (valid) {
             uint32_t lo = 0, hi = nseg;
@@ -105,6 +105,7 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                 const uint32_t mid = (lo + hi) >> 1;
                 if (segs[mid].start <= t) lo = mid; else hi = mid;
             }
+            seg = lo;
             sg = segs[lo];
             i = (uint32_t)(t - sg.start);
             for (uint32_t k = 0; k < sg.nval && alive; ++k) alive = maps[sg.val_first + k][i] != kNone;
@@ -173,17 +174,40 @@ __global__ void tree_level(const TreeSeg *__restrict__ segs, uint32_t nseg, unsi
                 acc *= sum;
             }
         }
-        if (!valid) continue;
-        if (over && sg.check) {
-            atomicOr(&overflow[sg.query], 1u);
-            acc = 0;
+        if (valid) {
+            if (over && sg.check) {
+                atomicOr(&overflow[sg.query], 1u);
+                acc = 0;
+            }
+            sg.w[i] = acc;
         }
-        sg.w[i] = acc;
-        if (sg.root && acc) {
-            atomicAdd(&counts[sg.query], (unsigned long long)sg.coef * acc);
-            if (sg.check) {
-                const unsigned long long old = atomicAdd(&homs[sg.query], acc);
-                if (old + acc < old) atomicOr(&overflow[sg.query], 1u);
+        // root weights: summed over each segment's lanes (a segment's lanes
+        // are contiguous), then one atomic per segment and warp
+        const bool root = valid && sg.root;
+        if (__any_sync(0xffffffffu, root)) {
+            const uint32_t key = root ? seg : 0xFFFFFFFFu;
+            unsigned long long v = root ? (unsigned long long)sg.coef * acc : 0ull;
+            unsigned long long h = (root && sg.check) ? acc : 0ull;
+            bool ov = false;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long yv = __shfl_down_sync(0xffffffffu, v, o);
+                const unsigned long long yh = __shfl_down_sync(0xffffffffu, h, o);
+                const bool yo = __shfl_down_sync(0xffffffffu, ov, o);
+                const uint32_t yk = __shfl_down_sync(0xffffffffu, key, o);
+                if (lane + o < 32 && yk == key) {
+                    v += yv;
+                    ov |= yo || h + yh < h;
+                    h += yh;
+                }
+            }
+            const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+            if (root && (lane == 0 || prev != key)) {
+                if (v) atomicAdd(&counts[sg.query], v);
+                if (sg.check) {
+                    const unsigned long long old = h ? atomicAdd(&homs[sg.query], h) : 0ull;
+                    if (ov || old + h < old) atomicOr(&overflow[sg.query], 1u);
+                }
             }
         }
     }
