@@ -600,7 +600,8 @@ __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *_
     }
 }
 
-// Dense copy of the padded lists.
+// Dense copy of the padded lists: a lane per item copies a short list, the
+// warp together copies every list longer than 32 entries.
 // The same pass turns the counts (cnt) into each item's offset within its
 // edge's list, records each edge's first entry and flags a list offset past
 // 2^32 (the work of k3_offsets).
@@ -624,28 +625,15 @@ __global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ u
             cnt[my] = (uint32_t)rel;
             if (my == first) edge_start[ei] = to;
         }
-        // the 32 items' dense lists are one contiguous range: copy it a lane
-        // per entry (coalesced writes), each entry read from its item's
-        // padded list
-        uint64_t inc = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= (uint32_t)o) inc += y;
-        }
-        const uint64_t excl = inc - c;
-        const uint64_t S = __shfl_sync(0xffffffffu, inc, 31), wbase = __shfl_sync(0xffffffffu, to, 0);
-        for (uint64_t j0 = 0; j0 < S; j0 += 32) {
-            const uint64_t j = j0 + lane;
-            uint32_t o = 0;  // owner: the first lane whose inclusive prefix exceeds j
-#pragma unroll
-            for (uint32_t step = 16; step; step >>= 1) {
-                const uint64_t v = __shfl_sync(0xffffffffu, inc, o + step - 1);
-                if (v <= j) o += step;
-            }
-            o = min(o, 31u);
-            const uint64_t ex = __shfl_sync(0xffffffffu, excl, o), fr = __shfl_sync(0xffffffffu, from, o);
-            if (j < S) elist[wbase + j] = padded[fr + (j - ex)];
+        if (c <= kLongRun)
+            for (uint32_t k = 0; k < c; ++k) elist[to + k] = padded[from + k];
+        uint32_t todo = __ballot_sync(0xffffffffu, c > kLongRun);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
+            const uint64_t f = __shfl_sync(0xffffffffu, from, src), t = __shfl_sync(0xffffffffu, to, src);
+            for (uint32_t k = lane; k < cc; k += 32) elist[t + k] = padded[f + k];
         }
     }
 }
