@@ -463,7 +463,7 @@ def main():
                                    "what": "one query per launch sequence (asdm_candidate_space, asdm_plan_create, "
                                            "asdm_run_plan)"},
                        batched_over_plain=plain_ms / ms,
-                       cs_build_roofline={"kernels": "K1-K3 (k1_filter, k2_pass, compaction, k3_bound/edges/pack)",
+                       cs_build_roofline={"kernels": "K1-K3 (k1_filter, k2_pull, compaction, k3_bound/flat/pack)",
                                           "bound": "hbm", "achieved": cs_achieved, "peak": peak, "unit": "GB/s",
                                           "frac": cs_achieved / peak, "algorithmic_bytes_per_step": cs_bytes,
                                           "device_ms_per_step": cs_ms, "traffic": traffic_cs},
