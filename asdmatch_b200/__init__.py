@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -292,6 +293,9 @@ class DeviceGraph:
         self._h = h
         self.n = g.n
         self.host = g
+        # candidate spaces built on this graph: they free their device memory
+        # on the graph's stream, so they are closed before the graph is
+        self._spaces = weakref.WeakSet()
 
     def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None,
                    root_block_min: Optional[int] = None):
@@ -313,6 +317,11 @@ class DeviceGraph:
         return s.value or 0
 
     def close(self):
+        for cs in list(getattr(self, "_spaces", ())):
+            try:
+                cs.close()
+            except Exception:
+                pass
         if self._h is not None and self._h.value:
             _g_free(self._h)
         self._h = None
@@ -336,6 +345,7 @@ class CandidateSpace:
         self.q = q
         self.dg = dg
         self.nonempty = bool(ne.value)
+        dg._spaces.add(self)
 
     def build_cand_cfl(self) -> bool:
         """The reference's return value: False when some candidate set is empty."""
@@ -373,6 +383,7 @@ class CandidateSpace:
         obj.q = q
         obj.dg = dg
         obj.nonempty = nonempty
+        dg._spaces.add(obj)
         return obj
 
     def build_stats(self):

@@ -103,6 +103,9 @@ int asdm_gen_query(const asdm_host_graph *g, uint32_t size, int density, uint64_
  * relation/graph.h:34-56). ASDM_ERR_INVALID if a list is not (label,id)-sorted. */
 int asdm_graph_upload(const uint32_t *offsets, const uint32_t *nbrs, const uint32_t *labels,
                       uint32_t n, uint64_t m2, uint32_t nlabels, asdm_graph **out);
+/* Frees the device graph.  Free every candidate space built on it first: a
+ * candidate space frees its device memory on the graph's stream and reads the
+ * graph when it is freed. */
 int asdm_graph_free(asdm_graph *g);
 /* Knobs of the enumeration kernels, per data graph; chosen by the autotuner
  * (asdmatch_b200.autotune) by timing the caller's own batch.

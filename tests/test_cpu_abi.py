@@ -124,3 +124,23 @@ def test_device_entry_points_fail_cleanly_without_gpu():
     with pytest.raises(A.AsdmError) as e:
         A.DeviceGraph(g)
     assert e.value.code == A.ERR_CUDA
+
+
+def test_graph_close_frees_its_candidate_spaces_first():
+    """A candidate space frees its device memory on its graph's stream, so
+    DeviceGraph.close() closes the candidate spaces still alive on it before
+    freeing the graph (host bookkeeping only: stand-in handles, no device)."""
+    import weakref
+
+    class StandInGraph:
+        pass
+
+    g = StandInGraph()
+    g._spaces = weakref.WeakSet()
+    g._h = None
+    spaces = [A.CandidateSpace._wrap(0, None, g, False) for _ in range(3)]
+    assert len(g._spaces) == 3
+    A.DeviceGraph.close(g)
+    assert all(cs._h is None for cs in spaces)
+    del spaces
+    assert len(g._spaces) == 0
