@@ -14,8 +14,9 @@
 //     Ctd(root) = F(root),   Ctd(u) = F(u) ∩ ⋂_{p ∈ before(u)} N_l(u)(S(p)),
 //     C(u) = F(u) ∩ ⋂_{p ∈ N_q(u)} N_l(u)(S(p)),
 // computed wave by wave along the CFL BFS order (a vertex's wave is one more
-// than the latest wave among its earlier neighbours).  Marking is an atomic
-// OR into a bitset, so the order of the scans inside a wave does not matter.
+// than the latest wave among its earlier neighbours).  The slot bitset of a
+// pass p -> u is computed in pull form: a candidate's bit is set when one of
+// its l(p)-neighbours lies in Ctd(p) (the phantom vertex 0 is pushed).
 // Compaction ANDs the required bitsets word by word and writes the surviving
 // vertices in id order.  K3 builds the candidate edges
 // (buildCandidateEdge(false), :458-487) as CSR lists of indices into C(u2),
@@ -442,7 +443,6 @@ __device__ __forceinline__ uint32_t cand_index(const uint2 *cm, uint32_t r) {
 template <bool kFill>
 __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
-                                                   const uint32_t *__restrict__ order,
                                                    uint32_t *__restrict__ cnt, const uint64_t *__restrict__ wpos,
                                                    uint32_t *__restrict__ elist, unsigned long long *__restrict__ elems,
                                                    const uint32_t *__restrict__ rstart) {
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
     uint64_t scanned = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint64_t pos = base + lane;
-        const uint64_t item = (order && pos < total) ? order[pos] : pos;
+        const uint64_t item = pos;
         uint32_t b = 0, e = 0;
         const uint2 *cm = nullptr;
         if (pos < total) {
@@ -584,12 +584,12 @@ __global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__
 // Upper bound of every item's list: the length of the candidate's label run.
 __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                    const uint64_t *__restrict__ item_base, uint32_t nedges,
-                                                   const uint32_t *__restrict__ order, uint32_t *__restrict__ ub,
+                                                   uint32_t *__restrict__ ub,
                                                    uint32_t *__restrict__ rstart) {
     const uint64_t total = item_base[nedges];
     for (uint64_t pos = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
          pos += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t item = order ? order[pos] : pos;
+        const uint64_t item = pos;
         const uint32_t ei = find_segment(item_base, nedges, item);
         const EdgeDesc d = edges[ei];
         const uint32_t i = (uint32_t)(item - item_base[ei]);
@@ -789,9 +789,6 @@ struct Scratch {
         int rc = dalloc(p, n, s);
         if (rc == ASDM_OK) ptrs.push_back((void *)*p);
         return rc;
-    }
-    void keep(void *p) {
-        if (p) ptrs.push_back(p);
     }
     template <typename T>
     int upload(T **p, const std::vector<T> &h) {
@@ -1155,11 +1152,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         // K3 keeps edge-major order: a warp's lanes take consecutive candidates
         // of one edge, whose ascending ids put their adjacency runs side by
         // side in the CSR (grouping by vertex block across edges measured slower)
-        const uint32_t *order = nullptr;
         ASDM_TRY(scr.alloc(&d_upos, nitems + 1));
         uint32_t *rstart = nullptr;
         ASDM_TRY(scr.alloc(&rstart, nitems));
-        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, rstart);
+        k3_bound<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, rstart);
         ::asdm::count_launch();
         ASDM_CUDA(cudaGetLastError());
         ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
@@ -1180,7 +1176,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
         } else {
-            k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, arena->d_eoff, nullptr, nullptr,
+            k3_edges<false><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, nullptr, nullptr,
                                                     d_elems + 1, nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
@@ -1188,7 +1184,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
             ASDM_CUDA(cudaMemcpyAsync(&total, d_wpos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
             ASDM_CUDA(cudaStreamSynchronize(s));
             ASDM_TRY(dalloc(&arena->d_elist, total, s));
-            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, order, nullptr, d_wpos, arena->d_elist,
+            k3_edges<true><<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, nullptr, d_wpos, arena->d_elist,
                                                     nullptr, nullptr);
             ::asdm::count_launch();
             ASDM_CUDA(cudaGetLastError());
