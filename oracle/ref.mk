@@ -2,7 +2,12 @@
 # where they lie, into oracle/_ref/ (git-ignored).  Used only as a checker by
 # tests/ and by bench.py's CPU-baseline leg; the product never links it.
 #
-#   make -f oracle/ref.mk REF=/root/reference          (from the repo root)
+#   make -f oracle/ref.mk [REF=<reference tree>]        (from the repo root)
+#   make -s -f oracle/ref.mk refdir                      (prints the tree used)
+#
+# The reference tree is REF, else $ASDM_REFERENCE_DIR, else the default below;
+# this recipe is the one place that names it (tests and the build entry point
+# ask it with `refdir`).
 #
 # No reference build system is run: GLPK 4.55's C sources and the reference's
 # C++ sources are compiled directly with the flags below (GLPK's shipped
@@ -10,7 +15,7 @@
 # rebuilt from .c/.cpp).  The reference's compile-time modes
 # (config/config.h:38-40) are passed with -D, which config.h leaves alone
 # because its own #defines of them are commented out.
-REF      ?= /root/reference
+REF      ?= $(or $(ASDM_REFERENCE_DIR),/root/reference)
 OUT      ?= oracle/_ref
 CXX      ?= g++
 CC       ?= gcc
@@ -62,7 +67,10 @@ $(OUT)/$(1): oracle/ref_harness.cpp $(REF_CPP) $(OUT)/libglpk_src.a
 endef
 $(foreach v,$(VARIANTS),$(eval $(call VARIANT_RULE,$(v))))
 
+refdir:
+	@echo $(REF)
+
 clean:
 	rm -rf $(OUT)
 
-.PHONY: all clean
+.PHONY: all clean refdir

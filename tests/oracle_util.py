@@ -16,6 +16,27 @@ REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 MODE_COUNT, MODE_LOCAL, MODE_EMBED = 0, 1, 2
 
 
+def reference_tree():
+    """The reference source tree oracle/ref.mk builds from (that recipe holds
+    the location; $ASDM_REFERENCE_DIR overrides it), or None when absent."""
+    try:
+        r = subprocess.run(["make", "-s", "-f", "oracle/ref.mk", "refdir"], cwd=ROOT, capture_output=True,
+                           text=True, timeout=30)
+    except (OSError, subprocess.TimeoutExpired):
+        return None
+    d = r.stdout.strip()
+    return d if r.returncode == 0 and d and os.path.isdir(d) else None
+
+
+def reference_file(*parts):
+    """A file of the reference tree (e.g. its yeast dataset), or None."""
+    d = reference_tree()
+    if d is None:
+        return None
+    p = os.path.join(d, *parts)
+    return p if os.path.exists(p) else None
+
+
 def build_oracle():
     if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(
             os.path.join(ROOT, "oracle", "asdm_oracle.cpp")):

@@ -5,8 +5,9 @@ import tarfile
 import pytest
 
 import asdmatch_b200 as A
+import oracle_util as O
 
-YEAST = "/root/reference/dataset/yeast.tar.gz"
+YEAST = O.reference_file("dataset", "yeast.tar.gz")
 
 
 def test_write_then_read_round_trip(tmp_path):
@@ -34,7 +35,7 @@ def test_garbage_and_missing_files_are_rejected(tmp_path):
     assert e.value.code == A.ERR_IO
 
 
-@pytest.mark.skipif(not os.path.exists(YEAST), reason="needs the reference's yeast fixtures")
+@pytest.mark.skipif(not YEAST, reason="needs the reference's yeast fixtures")
 def test_reads_the_reference_card_files(tmp_path):
     with tarfile.open(YEAST) as t:
         t.extractall(tmp_path)
