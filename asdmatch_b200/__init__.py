@@ -126,13 +126,14 @@ _gemm = _sig("asdm_gemm_bf16", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.
                                          C.POINTER(C.c_float)])
 class BatchOpts(C.Structure):
     _fields_ = [("time_limit_s", C.c_double), ("count_limit", C.c_uint64), ("cards", C.POINTER(_vp)),
-                ("estimator", _vp), ("learned_max_subset", C.c_uint32)]
+                ("estimator", _vp), ("learned_max_subset", C.c_uint32), ("query_time_limit_s", C.c_double)]
 
 
 _run_batch_ex = _sig("asdm_run_batch_ex", C.c_int,
                      [_vp, C.c_uint32, _u32p, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, C.POINTER(BatchOpts), _u64p,
                       C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(RunStats)])
 _cs_edge_totals = _sig("asdm_cs_edge_totals", C.c_int, [_vp, _u64p])
+_cs_lower_bound = _sig("asdm_cs_count_lower_bound", C.c_int, [_vp, _u64p, C.POINTER(C.c_int)])
 _est_create = _sig("asdm_est_create", C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(_vp)])
 _est_train = _sig("asdm_est_train_step", C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_float), _u32p, _u32p, _u32p,
                                                    C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)])
@@ -273,7 +274,7 @@ class HostGraph:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _hg_free is not None:  # module globals are gone at interpreter exit
             _hg_free(h)
             self._h = _vp()
 
@@ -356,6 +357,14 @@ class CandidateSpace:
         out = np.zeros(max(int(self.q.offsets[-1]), 1), np.uint64)
         _check(_cs_edge_totals(self._h, _ptr(out, _u64p)))
         return out[:int(self.q.offsets[-1])]
+
+    def count_lower_bound(self):
+        """(bound, exceeds): a lower bound of the embedding count (capped at
+        2^64 - 1) and whether it shows the count is at least 2^64."""
+        lb = C.c_uint64()
+        ex = C.c_int()
+        _check(_cs_lower_bound(self._h, C.byref(lb), C.byref(ex)), "lower bound")
+        return int(lb.value), bool(ex.value)
 
     def prefix_counts(self, orders: Sequence[Sequence[int]], time_limit_s: float = 0.0, count_limit: int = 0):
         """Partial-match counts of each prefix (a connected sequence of query
@@ -475,7 +484,7 @@ class Card:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _card_free is not None:  # module globals are gone at interpreter exit
             _card_free(h)
             self._h = None
 
@@ -503,7 +512,7 @@ class Plan:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _plan_free is not None:  # module globals are gone at interpreter exit
             _plan_free(h)
             self._h = None
 
@@ -651,12 +660,15 @@ def run_batch_local(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s:
 
 def run_batch_ex(dg: DeviceGraph, b: BatchInput, time_limit_s: float = 0.0, count_limit: int = 0,
                  cards: Optional[Sequence[Optional["Card"]]] = None, estimator: Optional["Estimator"] = None,
-                 learned_max_subset: int = 0) -> RunStats:
-    """Batched counting with per-query count limits, plan caches or learned
-    plans; results in b.counts / b.status."""
+                 learned_max_subset: int = 0, query_time_limit_s: float = 0.0) -> RunStats:
+    """Batched counting with per-query count limits, per-query GPU-time
+    budgets (query_time_limit_s: the time a query may take as if it ran alone
+    on the GPU; past it that query alone reports ERR_TIMEOUT), plan caches or
+    learned plans; results in b.counts / b.status."""
     opts = BatchOpts()
     opts.time_limit_s = time_limit_s
     opts.count_limit = count_limit
+    opts.query_time_limit_s = query_time_limit_s
     if estimator is not None:
         opts.estimator = estimator._h
         opts.learned_max_subset = learned_max_subset
@@ -690,7 +702,7 @@ def candidate_spaces(dg: DeviceGraph, queries: Sequence[HostGraph], b: Optional[
 
 
 def run_planned(css: Sequence[CandidateSpace], plans: Sequence[Optional["Plan"]], time_limit_s: float = 0.0,
-                count_limit: int = 0):
+                count_limit: int = 0, query_time_limit_s: float = 0.0):
     """One persistent launch over given candidate spaces and plans: (counts, status, RunStats)."""
     nq = len(css)
     ch = (_vp * max(1, nq))(*[c._h for c in css])
@@ -698,6 +710,7 @@ def run_planned(css: Sequence[CandidateSpace], plans: Sequence[Optional["Plan"]]
     opts = BatchOpts()
     opts.time_limit_s = time_limit_s
     opts.count_limit = count_limit
+    opts.query_time_limit_s = query_time_limit_s
     counts = np.zeros(max(1, nq), np.uint64)
     status = np.zeros(max(1, nq), np.int32)
     st = RunStats()
@@ -805,7 +818,7 @@ class Estimator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _est_free is not None:  # module globals are gone at interpreter exit
             _est_free(h)
             self._h = None
 
@@ -836,9 +849,10 @@ def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
         nonlocal want
         dg.set_tuning(mb, ll, pl, rb)
         run(dg, batch)  # warm
+        ok = batch.status == OK
         if want is None:
-            want = batch.counts.copy()
-        elif not np.array_equal(batch.counts, want):
+            want = (batch.counts.copy(), ok.copy())
+        elif not np.array_equal(batch.counts[ok & want[1]], want[0][ok & want[1]]):
             raise AsdmError(ERR_INTERNAL, "tuning changed a count")
         times = []
         for _ in range(reps):

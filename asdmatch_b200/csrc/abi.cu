@@ -187,7 +187,7 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
 int build_prefix_plan(const asdm_cs &cs, const uint32_t *order, uint32_t depth, asdm_plan &p);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out, uint64_t *cycles = nullptr);
+                    uint64_t *const *local_out, uint64_t *cycles = nullptr, double query_time_s = 0.0);
 int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
                        std::vector<asdm_plan> &plans);
 }  // namespace asdm
@@ -201,7 +201,7 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
                           const uint64_t *q_lab_base, const uint32_t *q_labels, double time_limit_s,
                           uint64_t count_limit, const asdm_card *const *cards, asdm_estimator *est,
                           uint32_t est_kmax, uint64_t *counts, int *status, asdm_run_stats *stats,
-                          uint64_t *const *local_out) {
+                          uint64_t *const *local_out, double query_time_s = 0.0) {
     clear_error();
     if (stats) *stats = asdm_run_stats{};
     if (!g || (nq && (!q_sizes || !q_off_base || !q_offsets || !q_nbr_base || !q_nbrs || !q_lab_base || !q_labels ||
@@ -283,7 +283,7 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
             for (uint32_t id : run_ids) lo.push_back(local_out[id]);
         asdm_run_stats gs{};
         rc = run_batch_count(g, run_cs, run_plans, time_limit_s, count_limit, c.data(), st.data(), &gs,
-                             local_out ? lo.data() : nullptr);
+                             local_out ? lo.data() : nullptr, nullptr, query_time_s);
         if (stats) {
             stats->count += gs.count;
             stats->intersections += gs.intersections;
@@ -324,7 +324,7 @@ extern "C" int asdm_run_batch_ex(asdm_graph *g, uint32_t nq, const uint32_t *q_s
     if (!opts) return fail(ASDM_ERR_INVALID, "null options");
     return run_batch_impl(g, nq, q_sizes, q_off_base, q_offsets, q_nbr_base, q_nbrs, q_lab_base, q_labels,
                           opts->time_limit_s, opts->count_limit, opts->cards, opts->estimator,
-                          opts->learned_max_subset, counts, status, stats, local_counts);
+                          opts->learned_max_subset, counts, status, stats, local_counts, opts->query_time_limit_s);
 }
 
 extern "C" int asdm_run_batch_local(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
@@ -476,9 +476,10 @@ extern "C" int asdm_run_planned_profile(uint32_t nq, asdm_cs *const *cs, const a
     std::vector<int> st(run_ids.size());
     const double tl = opts ? opts->time_limit_s : 0.0;
     const uint64_t cl = opts ? opts->count_limit : 0;
+    const double qt = opts ? opts->query_time_limit_s : 0.0;
     std::vector<uint64_t> cy(cycles ? run_ids.size() : 0);
     const int rc = run_batch_count(g, run_cs, run_plans, tl, cl, c.data(), st.data(), stats, nullptr,
-                                   cycles ? cy.data() : nullptr);
+                                   cycles ? cy.data() : nullptr, qt);
     if (cycles)
         for (uint32_t i = 0; i < nq; ++i) cycles[i] = 0;
     for (size_t k = 0; k < run_ids.size(); ++k) {

@@ -37,6 +37,8 @@ bool tree_countable(const QueryGraph &q);
 bool tree_countable_conflicts(const QueryGraph &q);
 int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
                 std::vector<char> &done, const std::vector<unsigned long long *> *local = nullptr);
+int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<char> &proven,
+                    std::vector<uint64_t> *lower = nullptr);
 
 namespace {
 
@@ -44,8 +46,8 @@ constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr uint32_t kFull = 0xffffffffu;
 
-enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4, kFlagInternal = 8, kFlagLimit = 16 };
-constexpr uint32_t kStopFlags = kFlagOverflow | kFlagTimeout | kFlagInternal | kFlagLimit;
+enum : uint32_t { kFlagOverflow = 1, kFlagTimeout = 2, kFlagCapacity = 4, kFlagLimit = 16 };
+constexpr uint32_t kStopFlags = kFlagOverflow | kFlagTimeout | kFlagLimit;
 enum : int {
     kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5,
     kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrTailLane = 11,
@@ -55,7 +57,11 @@ enum : int {
 // sequence number per slot): a record is [query, level s, lo, hi, idx[0..s-1]].
 constexpr uint32_t kRecWords = 4 + 32;
 constexpr uint64_t kQueueCap = 1u << 16;      // power of two
-constexpr uint32_t kIdlePolls = 1u << 20;     // an idle warp gives up after this many polls
+// An idle warp polls the ring until no warp is working, a stop flag is set or
+// the run's deadline passes; without a deadline it leaves after kIdleMaxNs
+// (the working warps then finish their own ranges, so no work is lost).
+constexpr uint64_t kIdleMaxNs = 3600ull * 1000000000ull;
+constexpr uint32_t kIdleSleepMaxNs = 2048;   // poll back-off ceiling
 
 struct DLevel {
     const uint32_t *cand;  // C(u)
@@ -100,6 +106,10 @@ struct EnumArgs {
     uint32_t nquery, maxn, maxnb;
     unsigned long long *qcounts;
     unsigned int *qflags;
+    // per-query time budget (batches): warp-nanoseconds a query may use,
+    // summed over warps (0 = none), and what each query has used
+    unsigned long long q_budget_ns;
+    unsigned long long *qwork;
     // closed form of the last two levels (single-query kernel; QDesc for batches)
     const unsigned long long *ps;
     const uint32_t *rev_off, *rev_list;
@@ -206,6 +216,7 @@ struct Warp {
     unsigned long long *local;  // |Vg| x n local counts of the current query (MODE_LOCAL)
     unsigned long long count = 0, inter = 0, elems = 0, tails_lane = 0, tails_warp = 0;
     bool overflow = false;
+    uint64_t t_mark = 0;   // lane 0: when this warp's time was last charged to its query
     const unsigned long long *ps;        // kTailChain: prefix sums over the driver edge of level n-2
     const uint32_t *rev_off, *rev_list;  // kTailChain: candidate edges last level -> level n-2
     uint32_t tail;                       // kTail* of the current query
@@ -235,6 +246,33 @@ struct Warp {
         fidx = scur + maxnb;
         fta = fidx + 32;
         ftz = fta + 32;
+    }
+
+    // Charges this warp's time since the last mark to its query's budget
+    // (lane 0; batches with a per-query time budget).
+    __device__ __forceinline__ void charge() {
+        if (MULTI && a.q_budget_ns && lane == 0) {
+            const uint64_t now = globaltimer();
+            const unsigned long long dt = now - t_mark;
+            t_mark = now;
+            const unsigned long long used = atomicAdd(&a.qwork[q], dt) + dt;
+            if (used > a.q_budget_ns) atomicOr(&a.qflags[q], kFlagTimeout);
+        }
+    }
+
+    // Starts charging time to the current query (lane 0).
+    __device__ __forceinline__ void mark() {
+        if (MULTI && a.q_budget_ns && lane == 0) t_mark = globaltimer();
+    }
+
+    // Batches: whether the current query was stopped (count limit reached or
+    // time budget used up); its remaining work is abandoned.
+    __device__ __forceinline__ bool query_stopped() {
+        if (!MULTI || !(a.count_limit || a.q_budget_ns)) return false;
+        charge();
+        uint32_t st = 0;
+        if (lane == 0) st = *(volatile unsigned int *)&a.qflags[q] & (kFlagLimit | kFlagTimeout);
+        return __shfl_sync(kFull, st, 0) != 0;
     }
 
     // Switches to query qq of a batch (its plan is read from global memory).
@@ -873,21 +911,28 @@ struct Warp {
     }
 
     // Idle: polls the donation ring.  Returns the claimed position, or ~0
-    // when no warp is working any more (or the poll budget ran out).  The
+    // when no warp is working any more, a stop flag is set, or the wait's
+    // time bound (the run's deadline, else kIdleMaxNs) has passed.  The
     // caller copies the record and then calls release().
-    __device__ unsigned long long take_queued() {
+    __device__ unsigned long long take_queued(uint64_t deadline) {
         unsigned long long pos = ~0ull;
         if (lane == 0) {
             volatile unsigned long long *vc = (volatile unsigned long long *)a.ctr;
             atomicAdd(&a.ctr[kCtrIdle], 1ull);
-            for (uint32_t it = 0; it < kIdlePolls; ++it) {
+            const uint64_t t0 = globaltimer();
+            const uint64_t until = deadline ? deadline : t0 + kIdleMaxNs;
+            uint32_t nap = 128;
+            for (uint32_t it = 0;; ++it) {
                 const unsigned long long p = vc[kCtrHead];
                 const unsigned long long seq = *(volatile unsigned long long *)&a.qseq[p & (kQueueCap - 1)];
                 if (seq == p + 1) {
                     if (atomicCAS(&a.ctr[kCtrHead], p, p + 1) == p) { pos = p; break; }
+                    nap = 128;
                 } else if (seq < p + 1) {
                     if (vc[kCtrActive] == 0 || (vc[kCtrFlags] & kStopFlags)) break;
-                    __nanosleep(256);
+                    if ((it & 255u) == 255u && globaltimer() > until) break;
+                    __nanosleep(nap);
+                    nap = min(2 * nap, kIdleSleepMaxNs);
                 }
             }
             if (pos != ~0ull) atomicAdd(&a.ctr[kCtrActive], 1ull);
@@ -1152,11 +1197,7 @@ __device__ bool dfs(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane, uint
                 want = idle > pend && (long long)pend >= 0;
             }
             if (__shfl_sync(kFull, st, 0)) return false;
-            if (MULTI && a.count_limit) {
-                uint32_t lim = 0;
-                if (lane == 0) lim = *(volatile unsigned int *)&a.qflags[W.q] & kFlagLimit;
-                if (__shfl_sync(kFull, lim, 0)) return true;  // abandon this query's subtree
-            }
+            if (W.query_stopped()) return true;  // abandon this query's subtree
             if (__shfl_sync(kFull, want, 0)) W.try_donate(base, d);
         }
         if (W.pos[d] < W.cnt[d]) {
@@ -1266,8 +1307,9 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                 }
                 unsigned long long t = b * K;
                 unsigned long long t_end = min(t + K, P);
-                // a query past its count limit is abandoned
-                if (MULTI && a.count_limit && (*(volatile unsigned int *)&a.qflags[W.q] & kFlagLimit)) t_end = t;
+                // a query past its count limit or time budget is abandoned
+                W.mark();
+                if (W.query_stopped()) t_end = t;
                 if (W.n == 1) {
                     for (; t < t_end; ++t) {
                         if (lane == 0) {
@@ -1298,6 +1340,7 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                         ++i0;
                     }
                 }
+                W.charge();
                 if (lane == 0) {
                     if (MULTI && a.qcycles) atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
                     atomicAdd(&a.ctr[kCtrActive], ~0ull);
@@ -1306,7 +1349,7 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
             }
             roots_left = false;
         }
-        const unsigned long long qpos = W.take_queued();
+        const unsigned long long qpos = W.take_queued(deadline);
         if (qpos == ~0ull) break;
         const volatile uint32_t *rec = a.queue + (qpos & (kQueueCap - 1)) * kRecWords;
         if (MULTI) W.bind(rec[0]);
@@ -1319,7 +1362,9 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
         W.release(qpos);
         __syncwarp();
         const long long c0 = clock64();
-        stop = !run_range(a, W, lane, s, lo, hi, iter, deadline);
+        W.mark();
+        if (!W.query_stopped()) stop = !run_range(a, W, lane, s, lo, hi, iter, deadline);
+        W.charge();
         if (lane == 0) {
             if (MULTI && a.qcycles) atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
             atomicAdd(&a.ctr[kCtrActive], ~0ull);
@@ -1770,6 +1815,12 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
             return ASDM_OK;
         }
     }
+    if (mode == ASDM_MODE_COUNT && plan.order.size() == n) {
+        // a lower bound at or above 2^64 settles the query without enumeration
+        std::vector<char> proven;
+        ASDM_TRY(overflow_bounds(G, {&cs}, proven));
+        if (proven[0]) return fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1 (shown by a lower bound)");
+    }
     // device plan
     std::vector<DLevel> lv(n);
     std::vector<DBack> bk;
@@ -1908,7 +1959,6 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         st.list_bytes = 4ull * ctr[kCtrElems];
         st.tasks = std::min<uint64_t>(ctr[kCtrTask], a.ntasks);  // claimed root tasks
         const uint32_t flags = (uint32_t)ctr[kCtrFlags];
-        if (flags & kFlagInternal) { rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready"); break; }
         if (flags & kFlagOverflow) { rc = fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1"); break; }
         if (flags & kFlagTimeout) { rc = fail(ASDM_ERR_TIMEOUT, "time limit reached"); break; }
         if (flags & kFlagLimit) { rc = fail(ASDM_ERR_LIMIT, "count limit reached"); break; }
@@ -1960,7 +2010,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
 // counts[i] / status[i] receive each query's result.
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out, uint64_t *cycles) {
+                    uint64_t *const *local_out, uint64_t *cycles, double query_time_s) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
     std::vector<uint32_t> live;  // queries with a non-empty candidate space
@@ -2077,6 +2127,42 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             if (agg) agg->kernel_ms += tree_ms;
             if (live.empty()) return ASDM_OK;
         }
+        // queries whose count a lower bound shows to be at least 2^64 are settled as overflows
+        std::vector<asdm_cs *> ocs;
+        std::vector<uint32_t> oid;
+        for (uint32_t i : live)
+            if (plans[i]->order.size() == cs[i]->q.n) {
+                ocs.push_back(cs[i]);
+                oid.push_back(i);
+            }
+        if (!ocs.empty()) {
+            cudaEvent_t t0, t1;
+            cudaEventCreate(&t0);
+            cudaEventCreate(&t1);
+            cudaEventRecord(t0, G->stream);
+            std::vector<char> proven;
+            const int brc = overflow_bounds(G, ocs, proven);
+            cudaEventRecord(t1, G->stream);
+            cudaEventSynchronize(t1);
+            float bms = 0.f;
+            cudaEventElapsedTime(&bms, t0, t1);
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            if (brc != ASDM_OK) return brc;
+            std::vector<char> settled(Q, 0);
+            for (size_t k = 0; k < oid.size(); ++k)
+                if (proven[k]) {
+                    settled[oid[k]] = 1;
+                    counts[oid[k]] = 0;
+                    status[oid[k]] = ASDM_ERR_OVERFLOW;
+                }
+            std::vector<uint32_t> rest;
+            for (uint32_t i : live)
+                if (!settled[i]) rest.push_back(i);
+            live.swap(rest);
+            if (agg) agg->kernel_ms += bms;
+            if (live.empty()) return ASDM_OK;
+        }
     }
     const uint32_t L = (uint32_t)live.size();
     // host images of all plans, then one upload
@@ -2135,6 +2221,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
     const uint64_t tp_at = append(task_pre.data(), task_pre.size() * sizeof(unsigned long long));
     uint8_t *d_buf = nullptr;
     unsigned long long *d_ctr = nullptr, *d_qcounts = nullptr, *d_local = nullptr, *d_ps = nullptr, *d_cyc = nullptr;
+    unsigned long long *d_qwork = nullptr;
     uint32_t *d_queue = nullptr, *d_xmap = nullptr;
     unsigned long long *d_lw = nullptr;
     std::vector<unsigned long long *> lwv;
@@ -2154,9 +2241,11 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
                 break;
             }
         }
-        if ((rc = dalloc(&d_buf, hp.size(), s)) || (rc = dalloc(&d_ctr, kCtrN, s)) || (rc = dalloc(&d_qcounts, L, s)) ||
-            (rc = dalloc(&d_qflags, L, s)) || (rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s)))
+        if ((rc = dalloc(&d_buf, hp.size(), s)) || (rc = dalloc(&d_ctr, kCtrN, s)) ||
+            (rc = dalloc(&d_qcounts, 2ull * L, s)) || (rc = dalloc(&d_qflags, L, s)) ||
+            (rc = dalloc(&d_queue, kQueueCap * kRecWords + 2 * kQueueCap, s)))
             break;
+        d_qwork = d_qcounts + L;
         if (!local_mode) {
             std::vector<const asdm_cs *> tcs(L);
             std::vector<const asdm_plan *> tpl(L);
@@ -2195,7 +2284,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         std::memcpy(hp.data() + qd_at, qd.data(), L * sizeof(QDesc));
         if (cudaMemcpyAsync(d_buf, hp.data(), hp.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemsetAsync(d_ctr, 0, kCtrN * sizeof(unsigned long long), s) != cudaSuccess ||
-            cudaMemsetAsync(d_qcounts, 0, L * sizeof(unsigned long long), s) != cudaSuccess ||
+            cudaMemsetAsync(d_qcounts, 0, 2ull * L * sizeof(unsigned long long), s) != cudaSuccess ||
             cudaMemsetAsync(d_qflags, 0, L * sizeof(unsigned int), s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "batch upload failed");
             break;
@@ -2214,6 +2303,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         a.maxnb = maxnb;
         a.qcounts = d_qcounts;
         a.qflags = d_qflags;
+        a.qwork = d_qwork;
         if (cycles) {
             if ((rc = dalloc(&d_cyc, L, s))) break;
             if (cudaMemsetAsync(d_cyc, 0, L * sizeof(unsigned long long), s) != cudaSuccess) {
@@ -2251,6 +2341,9 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
                 rc = fail(ASDM_ERR_INVALID, "batch plans too large for shared memory (%u bytes)", smem);
                 break;
             }
+            // a query's budget: its time alone on the GPU, as warp-time over every resident warp
+            if (query_time_s > 0)
+                a.q_budget_ns = (unsigned long long)(query_time_s * 1e9 * (double)per_sm * G->num_sms * kWarps);
             k<<<(unsigned)(per_sm * G->num_sms), kThreads, smem, s>>>(a);
             ::asdm::count_launch();
             if (cudaGetLastError() != cudaSuccess) {
@@ -2289,10 +2382,10 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         for (uint32_t li = 0; li < L; ++li) {
             const uint32_t i = live[li];
             counts[i] = qc[li];
-            if (gflags & kFlagInternal) status[i] = ASDM_ERR_INTERNAL;
-            else if (gflags & kFlagTimeout) status[i] = ASDM_ERR_TIMEOUT;
-            else if (qf[li] & kFlagOverflow) status[i] = ASDM_ERR_OVERFLOW;
+            // a proven overflow outranks a stop; a count limit reached is final too
+            if (qf[li] & kFlagOverflow) status[i] = ASDM_ERR_OVERFLOW;
             else if (qf[li] & kFlagLimit) status[i] = ASDM_ERR_LIMIT;
+            else if ((gflags | qf[li]) & kFlagTimeout) status[i] = ASDM_ERR_TIMEOUT;
         }
         if (agg) {
             agg->count += ctr[kCtrCount];
@@ -2303,8 +2396,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             agg->tails_lane = ctr[kCtrTailLane];
             agg->tails_warp = ctr[kCtrTailWarp];
         }
-        if (gflags & kFlagInternal) rc = fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
-        else if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
+        if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
         if (rc == ASDM_OK && local_mode && d_lw) {
             std::vector<const asdm_cs *> tcs(L);
             std::vector<const asdm_plan *> tpl(L);
@@ -2379,6 +2471,20 @@ extern "C" int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const 
     asdm_plan_free(plan);
     asdm_cs_free(cs);
     return rc;
+}
+
+extern "C" int asdm_cs_count_lower_bound(asdm_cs *cs, uint64_t *lower, int *exceeds) {
+    clear_error();
+    if (!cs || !lower || !exceeds) return fail(ASDM_ERR_INVALID, "null argument");
+    *lower = 0;
+    *exceeds = 0;
+    if (!cs->nonempty) return ASDM_OK;
+    std::vector<char> proven;
+    std::vector<uint64_t> lb;
+    ASDM_TRY(overflow_bounds(cs->g, {cs}, proven, &lb));
+    *lower = lb[0];
+    *exceeds = proven[0] ? 1 : 0;
+    return ASDM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2520,7 +2626,6 @@ extern "C" int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, d
     stats->list_bytes = 4ull * ctr[kCtrElems];
     stats->tasks = std::min<uint64_t>(ctr[kCtrTask], a.ntasks);
     const uint32_t flags = (uint32_t)ctr[kCtrFlags];
-    if (flags & kFlagInternal) return fail(ASDM_ERR_INTERNAL, "work-donation record never became ready");
     if (flags & kFlagOverflow) return fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1");
     if (flags & kFlagTimeout) return fail(ASDM_ERR_TIMEOUT, "time limit reached");
     if (flags & kFlagLimit) return fail(ASDM_ERR_LIMIT, "count limit reached");

@@ -440,11 +440,12 @@ bool tree_countable_conflicts(const QueryGraph &q) {
     return block_trees(q, t);
 }
 
-// Counts every countable query of `cs` (non-empty candidate spaces on graph
-// G); done[i] = 1 and counts[i] set for the queries it settled.  With local
-// counts only queries without conflicts are taken.
-int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
-                std::vector<char> &done, const std::vector<unsigned long long *> *local) {
+namespace {
+
+// tree_counts for one chunk of queries (all of whose device state is
+// allocated at once).
+int tree_counts_chunk(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
+                      std::vector<char> &done, const std::vector<unsigned long long *> *local) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
     counts.assign(Q, 0);
@@ -741,6 +742,614 @@ int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uin
         cudaStreamSynchronize(s);
     }
     return rc;
+}
+
+// Device words (weights and member maps) a query's tree program needs, or 0
+// when it does not qualify.
+uint64_t tree_words(const asdm_cs &c) {
+    std::vector<BlockTree> t;
+    if (!c.nonempty || !block_trees(c.q, t)) return 0;
+    uint64_t w = 0;
+    for (const BlockTree &bt : t)
+        for (uint32_t b = 0; b < bt.nb; ++b) w += c.ncand[bt.rep[b]] * (1 + bt.members[b].size());
+    return w;
+}
+
+constexpr uint64_t kTreeChunkWords = 1ull << 28;  // 2 GiB of weights per launch group
+
+// ---------------------------------------------------------------------------
+// Overflow proofs.
+//
+// A count at or above 2^64 cannot be reported, only flagged (ASDM_ERR_OVERFLOW);
+// enumerating that many matches to see the counter wrap is out of reach.  A
+// lower bound settles it instead: for a query Q,
+//   1. every label's query vertices get classes, a proper colouring of their
+//      conflict graph (same label, not adjacent), and query vertex u may only
+//      take candidates of its class (class = a hash of the vertex id modulo
+//      the label's class count).  Conflicting vertices then have disjoint
+//      candidate sets, so every homomorphism that respects the classes is an
+//      embedding;
+//   2. a feedback vertex set F of Q (greedy: peel leaves, take the vertex of
+//      highest remaining degree, repeat) is fixed to one candidate each: the
+//      candidate of its class with the largest data degree.  Each vertex f of
+//      F becomes a leaf copy under each of its other neighbours, whose weight
+//      is 1 at f's fixed candidate and 0 elsewhere; edges inside F are checked
+//      between the fixed candidates;
+//   3. Q minus F is a forest; each component's homomorphism count (with the
+//      copies) is the tree program's bottom-up product of sums.
+// The product over components counts a subset of Q's embeddings (those with
+// the fixed images and the classes), so it is a lower bound of the count.  It
+// is computed in doubles with every sum and product rounded toward zero
+// (__dadd_rz, __dmul_rz): all operands are non-negative, so every stored value
+// is at most the exact one, and a final bound of at least 2^64 proves
+// count >= 2^64.
+// (No counterpart in the reference, whose ALL_LEVEL count is a size_t that
+// wraps silently: matching/join.cpp:1017-1097.)
+
+constexpr uint32_t kMaxFixed = 6;  // largest feedback vertex set tried
+
+// Class of data vertex v among k classes (a multiplicative hash of its id).
+__device__ __forceinline__ uint32_t vertex_class(uint32_t v, uint32_t k) {
+    return (uint32_t)((((unsigned long long)v * 0x9E3779B97F4A7C15ull) >> 32) % k);
+}
+
+// A query vertex of a lower-bound program: its weights over C(u).
+struct BoundSeg {
+    double *w;
+    const uint32_t *cand;       // C(u), for the class test
+    uint32_t ncand, cls_k, cls_c;
+    uint32_t child_first, nchild, pad;
+    unsigned long long start;   // first item of this segment in the launch
+};
+
+struct BoundChild {
+    const uint32_t *off, *list;  // candidate edges u -> c
+    const double *w;             // c's weights, or null (every candidate of c weighs 1)
+};
+
+// One thread per candidate of the level's segments:
+//   w_u(i) = [C(u)[i] has u's class] * prod over children c of
+//            sum over j in list_{u->c}(i) of w_c(j),
+// rounded toward zero; lists longer than 32 entries are summed by the warp.
+__global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, unsigned long long total,
+                            const BoundChild *__restrict__ kids) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total;
+         base += stride) {
+        const unsigned long long t = base + lane;
+        const bool valid = t < total;
+        BoundSeg sg{};
+        uint32_t i = 0;
+        bool alive = valid;
+        if (valid) {
+            uint32_t lo = 0, hi = nseg;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (segs[mid].start <= t) lo = mid; else hi = mid;
+            }
+            sg = segs[lo];
+            i = (uint32_t)(t - sg.start);
+            if (sg.cls_k > 1) alive = vertex_class(sg.cand[i], sg.cls_k) == sg.cls_c;
+        }
+        double acc = alive ? 1.0 : 0.0;
+        uint32_t maxk = alive ? sg.nchild : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) maxk = max(maxk, __shfl_xor_sync(0xffffffffu, maxk, o));
+        for (uint32_t k = 0; k < maxk; ++k) {
+            const bool mine = alive && k < sg.nchild;
+            uint32_t b = 0, e = 0;
+            const double *w = nullptr;
+            const uint32_t *list = nullptr;
+            if (mine) {
+                const BoundChild ch = kids[sg.child_first + k];
+                b = ch.off[i];
+                e = ch.off[i + 1];
+                w = ch.w;
+                list = ch.list;
+            }
+            double sum = (mine && !w) ? (double)(e - b) : 0.0;
+            const bool coop = mine && w && (e - b) > 32;
+            uint32_t todo = __ballot_sync(0xffffffffu, coop);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+                const double *ww = (const double *)__shfl_sync(0xffffffffu, (unsigned long long)w, src);
+                const uint32_t *ll = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)list, src);
+                double part = 0.0;
+                for (uint32_t x = bb + lane; x < ee; x += 32) part = __dadd_rz(part, ww[ll[x]]);
+#pragma unroll
+                for (int o = 16; o; o >>= 1) part = __dadd_rz(part, __shfl_xor_sync(0xffffffffu, part, o));
+                if ((int)lane == src) sum = part;
+            }
+            if (mine && w && !coop)
+                for (uint32_t x = b; x < e; ++x) sum = __dadd_rz(sum, w[list[x]]);
+            if (mine) acc = __dmul_rz(acc, sum);
+        }
+        if (valid) sg.w[i] = acc;
+    }
+}
+
+// A query's bound: for each component, the sum of its root's weights; the
+// product over components; 0 when a fixed vertex has no candidate of its
+// class or an edge between fixed vertices is missing.  One block per query.
+struct BoundQuery {
+    const double *const *roots;  // root weight arrays of the components
+    const uint32_t *nroot;       // their lengths
+    uint32_t ncomp, nhub, nedge, pad;
+    const uint32_t *hub;         // chosen hub indices of the fixed vertices
+    const uint32_t *edge_ok;     // checks of the edges inside F
+    double *out;
+};
+
+__global__ void bound_queries(const BoundQuery *__restrict__ qs) {
+    const BoundQuery bq = qs[blockIdx.x];
+    __shared__ double red[32];
+    __shared__ double prod;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) / 32;
+    if (threadIdx.x == 0) {
+        prod = 1.0;
+        for (uint32_t k = 0; k < bq.nhub; ++k) prod = bq.hub[k] == kNone ? 0.0 : prod;
+        for (uint32_t k = 0; k < bq.nedge; ++k) prod = bq.edge_ok[k] ? prod : 0.0;
+    }
+    __syncthreads();
+    for (uint32_t c = 0; c < bq.ncomp; ++c) {
+        double part = 0.0;
+        const double *w = bq.roots[c];
+        for (uint32_t i = threadIdx.x; i < bq.nroot[c]; i += blockDim.x) part = __dadd_rz(part, w[i]);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) part = __dadd_rz(part, __shfl_xor_sync(0xffffffffu, part, o));
+        if (lane == 0) red[warp] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (uint32_t k = 0; k < nw; ++k) tot = __dadd_rz(tot, red[k]);
+            prod = __dmul_rz(prod, tot);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *bq.out = prod;
+}
+
+struct HubSeg {
+    const uint32_t *cand;
+    uint32_t ncand, cls_k, cls_c, pad;
+    uint32_t *out;  // index in C(f) of the chosen candidate, or kNone
+};
+
+// One block per segment: the candidate of the segment's class with the
+// largest data degree (ties: the smaller index).
+__global__ void pick_hubs(const HubSeg *__restrict__ segs, const uint32_t *__restrict__ goff) {
+    const HubSeg sg = segs[blockIdx.x];
+    unsigned long long best = 0;
+    for (uint32_t i = threadIdx.x; i < sg.ncand; i += blockDim.x) {
+        const uint32_t v = sg.cand[i];
+        if (sg.cls_k > 1 && vertex_class(v, sg.cls_k) != sg.cls_c) continue;
+        const unsigned long long key =
+            (1ull << 63) | ((unsigned long long)(goff[v + 1] - goff[v]) << 32) | (0xFFFFFFFFu - i);
+        best = max(best, key);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    __shared__ unsigned long long red[32];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < (blockDim.x + 31) / 32 ? red[lane] : 0ull;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) *sg.out = best ? 0xFFFFFFFFu - (uint32_t)(best & 0xFFFFFFFFull) : kNone;
+    }
+}
+
+// Indicator weights of the fixed vertices (w[hub] = 1; the arrays are zeroed
+// before), and the checks of edges between fixed vertices: ok = 1 when fixed
+// candidate b of the edge's head lies in the edge's list of fixed candidate a.
+struct FixEdge {
+    const uint32_t *off, *list;
+    const uint32_t *ha, *hb;  // chosen indices of the two fixed vertices
+    uint32_t *ok;
+};
+
+__global__ void fix_weights(double *const *__restrict__ w, const uint32_t *const *__restrict__ hub, uint32_t nw,
+                            const FixEdge *__restrict__ edges, uint32_t ne) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nw) {
+        const uint32_t h = *hub[t];
+        if (h != kNone) w[t][h] = 1.0;
+    } else if (t < nw + ne) {
+        const FixEdge e = edges[t - nw];
+        const uint32_t a = *e.ha, b = *e.hb;
+        uint32_t ok = 0;
+        if (a != kNone && b != kNone) {
+            const uint32_t lo = e.off[a], hi = e.off[a + 1];
+            const uint32_t q = lo + lower_bound_u32(e.list + lo, hi - lo, b);
+            ok = q < hi && e.list[q] == b;
+        }
+        *e.ok = ok;
+    }
+}
+
+}  // namespace
+
+// proven[i] = 1 when query i's count is shown to be at least 2^64 (see the
+// overflow proofs above); lower (optional) receives each lower bound, capped
+// at 2^64 - 1 (0 where no bound was formed).  Queries are processed in chunks
+// of at most kTreeChunkWords weight words.
+int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<char> &proven,
+                    std::vector<uint64_t> *lower) {
+    cudaStream_t s = G->stream;
+    const size_t Q = cs.size();
+    proven.assign(Q, 0);
+    if (lower) lower->assign(Q, 0);
+    struct Prep {
+        std::vector<char> fixed;                // u in F
+        std::vector<uint32_t> fvs;              // F
+        std::vector<uint32_t> cls_k, cls_c;     // classes
+        std::vector<uint32_t> parent, height;   // forest over Q - F (kNone: component root)
+        std::vector<uint32_t> comp;             // component of each vertex outside F
+        std::vector<uint32_t> croot;            // root of each component
+        std::vector<char> seg;                  // u needs a weight array
+        uint64_t words = 0;
+    };
+    std::vector<Prep> prep(Q);
+    std::vector<char> ok(Q, 0);
+    for (size_t i = 0; i < Q; ++i) {
+        const asdm_cs &c = *cs[i];
+        const QueryGraph &q = c.q;
+        if (!c.nonempty || q.n < 2) continue;
+        Prep &P = prep[i];
+        const uint32_t n = q.n;
+        // feedback vertex set: peel vertices of degree <= 1, fix the busiest
+        P.fixed.assign(n, 0);
+        std::vector<char> gone(n, 0);
+        std::vector<uint32_t> deg(n);
+        for (uint32_t u = 0; u < n; ++u) deg[u] = q.deg(u);
+        for (;;) {
+            bool changed = true;
+            while (changed) {
+                changed = false;
+                for (uint32_t u = 0; u < n; ++u)
+                    if (!gone[u] && deg[u] <= 1) {
+                        gone[u] = 1;
+                        changed = true;
+                        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e)
+                            if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+                    }
+            }
+            uint32_t best = kNone;
+            for (uint32_t u = 0; u < n; ++u)
+                if (!gone[u] && (best == kNone || deg[u] > deg[best])) best = u;
+            if (best == kNone) break;
+            P.fixed[best] = 1;
+            P.fvs.push_back(best);
+            gone[best] = 1;
+            for (uint32_t e = q.off[best]; e < q.off[best + 1]; ++e)
+                if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+        }
+        if (P.fvs.size() > kMaxFixed || P.fvs.size() == n) continue;
+        // classes: greedy colouring of each label's conflict graph
+        P.cls_k.assign(n, 1);
+        P.cls_c.assign(n, 0);
+        for (uint32_t u = 0; u < n; ++u) {
+            uint64_t used = 0;
+            for (uint32_t w = 0; w < u; ++w)
+                if (q.lab[w] == q.lab[u] && q.slot(u, w) < 0) used |= 1ull << P.cls_c[w];
+            uint32_t c0 = 0;
+            while (used >> c0 & 1ull) ++c0;
+            P.cls_c[u] = c0;
+        }
+        for (uint32_t u = 0; u < n; ++u) {
+            uint32_t k = 0;
+            for (uint32_t w = 0; w < n; ++w)
+                if (q.lab[w] == q.lab[u]) k = std::max(k, P.cls_c[w] + 1);
+            P.cls_k[u] = k;
+        }
+        // forest over Q - F: components, parents, heights
+        P.parent.assign(n, kNone);
+        P.height.assign(n, 0);
+        P.comp.assign(n, kNone);
+        std::vector<uint32_t> order;
+        for (uint32_t r = 0; r < n; ++r) {
+            if (P.fixed[r] || P.comp[r] != kNone) continue;
+            const size_t first = order.size();
+            P.comp[r] = (uint32_t)P.croot.size();
+            P.croot.push_back(r);
+            order.push_back(r);
+            for (size_t k = first; k < order.size(); ++k) {
+                const uint32_t u = order[k];
+                for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                    const uint32_t w = q.nbr[e];
+                    if (P.fixed[w] || P.comp[w] != kNone) continue;
+                    P.comp[w] = P.comp[r];
+                    P.parent[w] = u;
+                    order.push_back(w);
+                }
+            }
+        }
+        for (size_t k = order.size(); k-- > 0;) {
+            const uint32_t u = order[k];
+            if (P.parent[u] != kNone) P.height[P.parent[u]] = std::max(P.height[P.parent[u]], P.height[u] + 1);
+        }
+        // a vertex needs its own weights unless it is an unrestricted leaf
+        // with no fixed neighbour (its parent then takes the list length)
+        P.seg.assign(n, 0);
+        for (uint32_t u = 0; u < n; ++u) {
+            if (P.fixed[u]) continue;
+            bool fixed_nbr = false, child = false;
+            for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                fixed_nbr |= P.fixed[q.nbr[e]] != 0;
+                child |= P.parent[q.nbr[e]] == u;
+            }
+            P.seg[u] = child || fixed_nbr || P.cls_k[u] > 1 || P.parent[u] == kNone;
+            if (P.seg[u]) P.words += c.ncand[u];
+        }
+        for (uint32_t f : P.fvs) P.words += c.ncand[f];  // the indicator arrays
+        ok[i] = 1;
+    }
+    size_t at = 0;
+    int rc = ASDM_OK;
+    while (at < Q && rc == ASDM_OK) {
+        std::vector<size_t> ids;
+        uint64_t words = 0;
+        for (; at < Q; ++at) {
+            if (!ok[at]) continue;
+            if (!ids.empty() && words + prep[at].words > kTreeChunkWords) break;
+            words += prep[at].words;
+            ids.push_back(at);
+        }
+        if (ids.empty()) break;
+        // descriptor uploads go through the graph's pinned stage: nothing is in flight after this sync
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "overflow-bound sync failed");
+            break;
+        }
+        G->stage.reset();
+        std::vector<uint32_t> hub0(ids.size());
+        uint32_t nhub = 0;
+        for (size_t k = 0; k < ids.size(); ++k) {
+            hub0[k] = nhub;
+            nhub += (uint32_t)prep[ids[k]].fvs.size();
+        }
+        double *wbuf = nullptr, *d_out = nullptr;
+        uint32_t *d_hub = nullptr, *d_eok = nullptr, *d_nroot = nullptr;
+        BoundSeg *d_segs = nullptr;
+        BoundChild *d_kids = nullptr;
+        HubSeg *d_hsegs = nullptr;
+        FixEdge *d_fe = nullptr;
+        BoundQuery *d_bq = nullptr;
+        double **d_fw = nullptr;
+        const uint32_t **d_fh = nullptr;
+        const double **d_roots = nullptr;
+        do {
+            if ((rc = dalloc(&wbuf, std::max<uint64_t>(words, 1), s)) || (rc = dalloc(&d_out, ids.size(), s)) ||
+                (rc = dalloc(&d_hub, std::max<uint32_t>(nhub, 1), s)))
+                break;
+            if (cudaMemsetAsync(wbuf, 0, std::max<uint64_t>(words, 1) * sizeof(double), s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "overflow-bound reset failed");
+                break;
+            }
+            // weight arrays: vertices with segments and the fixed vertices' indicators
+            std::vector<std::vector<double *>> wptr(ids.size());
+            std::vector<HubSeg> hsegs;
+            std::vector<double *> fw;
+            std::vector<const uint32_t *> fh;
+            std::vector<FixEdge> fedges;
+            std::vector<uint32_t> fe0(ids.size() + 1, 0);
+            uint64_t wo = 0;
+            for (size_t k = 0; k < ids.size(); ++k) {
+                const asdm_cs &c = *cs[ids[k]];
+                const Prep &P = prep[ids[k]];
+                wptr[k].assign(c.q.n, nullptr);
+                for (uint32_t u = 0; u < c.q.n; ++u)
+                    if (P.seg[u] || P.fixed[u]) {
+                        wptr[k][u] = wbuf + wo;
+                        wo += c.ncand[u];
+                    }
+                for (size_t j = 0; j < P.fvs.size(); ++j) {
+                    const uint32_t f = P.fvs[j];
+                    hsegs.push_back(HubSeg{c.d_cand + c.cand_base[f], c.ncand[f], P.cls_k[f], P.cls_c[f], 0,
+                                           d_hub + hub0[k] + j});
+                    fw.push_back(wptr[k][f]);
+                    fh.push_back(d_hub + hub0[k] + j);
+                }
+                fe0[k] = (uint32_t)fedges.size();
+                for (size_t j = 0; j < P.fvs.size(); ++j)
+                    for (size_t j2 = j + 1; j2 < P.fvs.size(); ++j2) {
+                        const uint32_t f = P.fvs[j], f2 = P.fvs[j2];
+                        const int sl = c.q.slot(f, f2);
+                        if (sl < 0) continue;
+                        const uint32_t e = c.q.off[f] + (uint32_t)sl;
+                        fedges.push_back(FixEdge{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                                 d_hub + hub0[k] + j, d_hub + hub0[k] + j2, nullptr});
+                    }
+            }
+            fe0[ids.size()] = (uint32_t)fedges.size();
+            const uint32_t ne = (uint32_t)fedges.size();
+            if ((rc = dalloc(&d_eok, std::max<uint32_t>(ne, 1), s))) break;
+            for (uint32_t e = 0; e < ne; ++e) fedges[e].ok = d_eok + e;
+            if (!hsegs.empty()) {
+                if ((rc = dalloc(&d_hsegs, hsegs.size(), s)) || (rc = dalloc(&d_fw, fw.size(), s)) ||
+                    (rc = dalloc(&d_fh, fh.size(), s)) || (rc = dalloc(&d_fe, std::max<uint32_t>(ne, 1), s)))
+                    break;
+                if (upload_async(G, d_hsegs, hsegs.data(), hsegs.size() * sizeof(HubSeg)) != cudaSuccess ||
+                    upload_async(G, d_fw, fw.data(), fw.size() * sizeof(void *)) != cudaSuccess ||
+                    upload_async(G, d_fh, fh.data(), fh.size() * sizeof(void *)) != cudaSuccess ||
+                    (ne && upload_async(G, d_fe, fedges.data(), ne * sizeof(FixEdge)) != cudaSuccess)) {
+                    rc = fail(ASDM_ERR_CUDA, "overflow-bound upload failed");
+                    break;
+                }
+                pick_hubs<<<(unsigned)hsegs.size(), 256, 0, s>>>(d_hsegs, G->d.off);
+                ::asdm::count_launch();
+                const uint32_t nfix = (uint32_t)fw.size() + ne;
+                fix_weights<<<(nfix + 255) / 256, 256, 0, s>>>(d_fw, d_fh, (uint32_t)fw.size(), d_fe, ne);
+                ::asdm::count_launch();
+                if (cudaGetLastError() != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "overflow-bound hub kernels failed");
+                    break;
+                }
+            }
+            // segments by height; children: forest children, then fixed copies
+            std::vector<std::vector<BoundSeg>> lv;
+            std::vector<BoundChild> kids;
+            std::vector<const double *> roots;
+            std::vector<uint32_t> nroot;
+            std::vector<BoundQuery> bqs(ids.size());
+            for (size_t k = 0; k < ids.size(); ++k) {
+                const asdm_cs &c = *cs[ids[k]];
+                const QueryGraph &q = c.q;
+                const Prep &P = prep[ids[k]];
+                for (uint32_t u = 0; u < q.n; ++u) {
+                    if (!P.seg[u]) continue;
+                    BoundSeg sg{};
+                    sg.w = wptr[k][u];
+                    sg.cand = c.d_cand + c.cand_base[u];
+                    sg.ncand = c.ncand[u];
+                    sg.cls_k = P.cls_k[u];
+                    sg.cls_c = P.cls_c[u];
+                    sg.child_first = (uint32_t)kids.size();
+                    for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                        const uint32_t w = q.nbr[e];
+                        if (P.parent[w] == u || P.fixed[w])
+                            kids.push_back(BoundChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                                      wptr[k][w]});
+                    }
+                    sg.nchild = (uint32_t)kids.size() - sg.child_first;
+                    if (lv.size() <= P.height[u]) lv.resize(P.height[u] + 1);
+                    lv[P.height[u]].push_back(sg);
+                }
+                BoundQuery &bq = bqs[k];
+                bq.ncomp = (uint32_t)P.croot.size();
+                bq.nhub = (uint32_t)P.fvs.size();
+                bq.nedge = fe0[k + 1] - fe0[k];
+                bq.out = d_out + k;
+                // pointer fields are set once the device arrays exist
+                for (uint32_t r : P.croot) {
+                    roots.push_back(wptr[k][r]);
+                    nroot.push_back(c.ncand[r]);
+                }
+            }
+            std::vector<BoundSeg> segs;
+            std::vector<size_t> first{0};
+            std::vector<unsigned long long> totals;
+            for (auto &l : lv) {
+                unsigned long long t = 0;
+                for (BoundSeg &sg : l) {
+                    sg.start = t;
+                    t += sg.ncand;
+                    segs.push_back(sg);
+                }
+                first.push_back(segs.size());
+                totals.push_back(t);
+            }
+            if (kids.empty()) kids.push_back(BoundChild{});
+            if (segs.empty()) segs.push_back(BoundSeg{});
+            if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s)) ||
+                (rc = dalloc(&d_roots, std::max<size_t>(roots.size(), 1), s)) ||
+                (rc = dalloc(&d_nroot, std::max<size_t>(nroot.size(), 1), s)) || (rc = dalloc(&d_bq, ids.size(), s)))
+                break;
+            uint32_t r0 = 0;
+            for (size_t k = 0; k < ids.size(); ++k) {
+                bqs[k].roots = d_roots + r0;
+                bqs[k].nroot = d_nroot + r0;
+                bqs[k].hub = d_hub + hub0[k];
+                bqs[k].edge_ok = d_eok + fe0[k];
+                r0 += bqs[k].ncomp;
+            }
+            if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
+                upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
+                upload_async(G, d_roots, roots.data(), roots.size() * sizeof(void *)) != cudaSuccess ||
+                upload_async(G, d_nroot, nroot.data(), nroot.size() * sizeof(uint32_t)) != cudaSuccess ||
+                upload_async(G, d_bq, bqs.data(), bqs.size() * sizeof(BoundQuery)) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "overflow-bound upload failed");
+                break;
+            }
+            for (size_t h = 0; h < totals.size() && rc == ASDM_OK; ++h) {
+                if (!totals[h]) continue;
+                const unsigned grid =
+                    (unsigned)std::min<unsigned long long>((totals[h] + 255) / 256, (unsigned long long)G->num_sms * 32);
+                bound_level<<<grid, 256, 0, s>>>(d_segs + first[h], (uint32_t)(first[h + 1] - first[h]), totals[h],
+                                                 d_kids);
+                ::asdm::count_launch();
+                if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "overflow-bound kernel failed");
+            }
+            if (rc != ASDM_OK) break;
+            bound_queries<<<(unsigned)ids.size(), 256, 0, s>>>(d_bq);
+            ::asdm::count_launch();
+            std::vector<double> out(ids.size());
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "overflow-bound readback failed");
+                break;
+            }
+            const double two64 = 18446744073709551616.0;  // exactly 2^64
+            for (size_t k = 0; k < ids.size(); ++k) {
+                proven[ids[k]] = out[k] >= two64;
+                if (lower) (*lower)[ids[k]] = out[k] >= two64 ? ~0ull : (uint64_t)out[k];
+            }
+        } while (false);
+        dfree(wbuf, s);
+        dfree(d_out, s);
+        dfree(d_hub, s);
+        dfree(d_eok, s);
+        dfree(d_nroot, s);
+        dfree(d_segs, s);
+        dfree(d_kids, s);
+        dfree(d_hsegs, s);
+        dfree(d_fe, s);
+        dfree(d_bq, s);
+        dfree(d_fw, s);
+        dfree(d_fh, s);
+        dfree(d_roots, s);
+        cudaStreamSynchronize(s);
+    }
+    if (rc != ASDM_OK) {
+        proven.assign(Q, 0);
+        if (lower) lower->assign(Q, 0);
+    }
+    return rc;
+}
+
+// Counts every countable query of `cs` (non-empty candidate spaces on graph
+// G); done[i] = 1 and counts[i] set for the queries it settled.  With local
+// counts only queries without conflicts are taken.  Queries run in chunks of
+// at most kTreeChunkWords device words (one query alone may exceed it).
+int tree_counts(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<uint64_t> &counts,
+                std::vector<char> &done, const std::vector<unsigned long long *> *local) {
+    const size_t Q = cs.size();
+    counts.assign(Q, 0);
+    done.assign(Q, 0);
+    size_t at = 0;
+    while (at < Q) {
+        std::vector<asdm_cs *> part;
+        std::vector<unsigned long long *> lpart;
+        std::vector<size_t> ids;
+        uint64_t words = 0;
+        for (; at < Q; ++at) {
+            const uint64_t w = tree_words(*cs[at]);
+            if (!ids.empty() && words + w > kTreeChunkWords) break;
+            words += w;
+            part.push_back(cs[at]);
+            if (local) lpart.push_back((*local)[at]);
+            ids.push_back(at);
+        }
+        std::vector<uint64_t> pc;
+        std::vector<char> pd;
+        const int rc = tree_counts_chunk(G, part, pc, pd, local ? &lpart : nullptr);
+        if (rc != ASDM_OK) {
+            done.assign(Q, 0);
+            return rc;
+        }
+        for (size_t k = 0; k < ids.size(); ++k) {
+            counts[ids[k]] = pc[k];
+            done[ids[k]] = pd[k];
+        }
+    }
+    return ASDM_OK;
 }
 
 }  // namespace asdm

@@ -247,10 +247,25 @@ int asdm_run_plan(asdm_cs *cs, const asdm_plan *plan, const asdm_run_opts *opts,
  * make it before any stream capture.  Calls share the array and must not
  * overlap on the GPU; each call resets the parts that must start at zero.
  * Queries up to 32 vertices (a plan of at most 16 KiB); larger plans are
- * rejected with ASDM_ERR_INVALID.  No counterpart in the reference, which
- * allocates with new[] throughout. */
+ * rejected with ASDM_ERR_INVALID.  Each call is synchronous: it returns after
+ * the kernel has finished and its counters are read back.  It fills count,
+ * intersections, list_bytes and tasks of `stats`; kernel_ms, tails_lane,
+ * tails_warp, emb_rows, build_ms and build_bytes stay 0.  No counterpart in
+ * the reference, which allocates with new[] throughout. */
 int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, double time_limit_s,
                                 uint64_t count_limit, asdm_run_stats *stats);
+
+/* A lower bound of the query's embedding count, formed on the device without
+ * enumeration: query vertices of one label that may not share a data vertex
+ * take candidates of distinct hash classes, a feedback vertex set is fixed to
+ * its highest-degree candidates, and the remaining forest is counted by a
+ * bottom-up program with sums and products saturating at 2^64 - 1.  *lower
+ * receives the bound (2^64 - 1 when it reaches that), *exceeds 1 when the
+ * bound shows the count is at least 2^64 — the case the counting entry points
+ * report as ASDM_ERR_OVERFLOW without enumerating.  No counterpart in the
+ * reference, whose ALL_LEVEL count is a size_t that wraps silently
+ * (matching/join.cpp:1017-1097). */
+int asdm_cs_count_lower_bound(asdm_cs *cs, uint64_t *lower, int *exceeds);
 
 /* One call for a query end to end on a resident graph: candidate space, plan
  * and count (the whole of ASDMatch.out's main(), main.cpp:11-147, without I/O). */
@@ -278,6 +293,10 @@ typedef struct asdm_batch_opts {
     const asdm_card *const *cards;  /* per query cardinality cache for its plan, or NULL    */
     asdm_estimator *estimator;      /* learned estimates for the planner, or NULL           */
     uint32_t learned_max_subset;    /* largest prefix the estimator is asked about (0 = 6) */
+    double query_time_limit_s;      /* 0 = none; else each query may use this much GPU time
+                                       (its warp-time over all resident warps: the time it
+                                       would run alone on the GPU) in the enumeration kernel,
+                                       past which it alone stops with ASDM_ERR_TIMEOUT      */
 } asdm_batch_opts;
 /* asdm_run_batch with per-query count limits and plan caches (the learned
  * estimator's predictions reach the planner this way); local_counts as in
