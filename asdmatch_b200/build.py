@@ -81,6 +81,12 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         if _stale(exe, [src, LIB] + hdrs):
             log.append(_run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src,
                              "-L", PKG, "-lasdm_b200", "-Wl,-rpath,$ORIGIN/..", "-o", exe]))
+    # the workload generator alone, from its host sources: no CUDA, no library
+    gen_src = [os.path.join(PKG, "cli", "gen_main.cpp"), os.path.join(CSRC, "host_graph.cpp")]
+    gen = os.path.join(BIN, "asdm_gen.out")
+    if all(os.path.exists(x) for x in gen_src) and _stale(gen, gen_src + hdrs):
+        log.append(_run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC] + gen_src +
+                        ["-o", gen]))
     text = "".join(log)
     if verbose:
         print(text)

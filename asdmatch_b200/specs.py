@@ -1,0 +1,38 @@
+"""Workload specifications (graph parameters, query seeds and sizes) as plain
+data, with no dependency on the compiled library: a process that only writes
+input files for another implementation (bench.py's reference arm) loads this
+file by path and runs the host-only generator asdmatch_b200/bin/asdm_gen.out.
+
+* C0  — N=3,112, M=12,519, degree exponent 2.5, 71 labels Zipf(1.0), 8-vertex
+        random-walk queries (the shape of the Yeast benchmark).
+* C0D — the same graph shape with 8 labels (heavier enumeration for tests).
+* C1  — N=3.77M, M=16.5M, exponent 2.1, 20 labels Zipf(1.2) (the shape of US
+        Patents), resident in HBM.
+* C2  — the C1 graph with the mixed batch: query i has seed C2_QUERY_SEED + i
+        and a size uniform in 4..32 (c2_size).
+* C4  — local subgraph counting: N=1.0M, M=10M, exponent 2.3, 32 labels
+        Zipf(1.0), 10-vertex queries.
+"""
+
+C0 = dict(n=3112, m=12519, gamma=2.5, nlabels=71, zipf_s=1.0, seed=1)
+C0_QUERY_SEED = 1000
+C0D = dict(n=3112, m=12519, gamma=2.5, nlabels=8, zipf_s=1.0, seed=2)
+C0D_QUERY_SEED = 3000
+C1 = dict(n=3_770_000, m=16_500_000, gamma=2.1, nlabels=20, zipf_s=1.2, seed=11)
+C2_QUERY_SEED = 50_000
+C2_QUERIES = 1000
+C4 = dict(n=1_000_000, m=10_000_000, gamma=2.3, nlabels=32, zipf_s=1.0, seed=41)
+C4_QUERY_SEED = 90_000
+
+
+def c2_seed_size(i):
+    """(seed, size) of the i-th query of the C2 mixed batch: sizes uniform in
+    4..32, decorrelated from the walk seed."""
+    seed = C2_QUERY_SEED + i
+    return seed, 4 + (seed * 2654435761 % 2 ** 32) % 29
+
+
+def generator_args(spec):
+    """The graph arguments of asdm_gen.out for a spec."""
+    return [str(spec["n"]), str(spec["m"]), repr(float(spec["gamma"])), str(spec["nlabels"]),
+            repr(float(spec["zipf_s"])), str(spec["seed"])]

@@ -8,10 +8,8 @@ machine rebuilds identical graphs and queries from the seeds.
         matches (heavier enumeration for parity tests).
 * C1  — N=3.77M, M=16.5M, exponent 2.1, 20 labels Zipf(1.2) (the shape of US
         Patents), resident in HBM.
-* C2  — the C1 graph with a mixed batch of random-walk queries whose sizes are
-        uniform in 4..32.  ``screen`` keeps the first queries (in seed order)
-        whose exact match count is at most ``count_limit``; the kept seeds and
-        counts are stored in ``c2_screened.json`` beside this module.
+* C2  — the C1 graph with the mixed batch: the first 1,000 random-walk queries
+        in seed order, sizes uniform in 4..32 (``c2_batch``), none screened out.
 * C4  — local subgraph counting: N=1.0M, M=10M, exponent 2.3, 32 labels
         Zipf(1.0).  No 10-vertex random-walk query of 1,500 tried has <= 10^9
         matches, so ``screen_c4`` keeps 8-vertex ones (``c4_screened.json``).
@@ -23,17 +21,10 @@ import os
 
 import asdmatch_b200 as A
 
-C0 = dict(n=3112, m=12519, gamma=2.5, nlabels=71, zipf_s=1.0, seed=1)
-C0_QUERY_SEED = 1000
-C0D = dict(n=3112, m=12519, gamma=2.5, nlabels=8, zipf_s=1.0, seed=2)
-C0D_QUERY_SEED = 3000
-C1 = dict(n=3_770_000, m=16_500_000, gamma=2.1, nlabels=20, zipf_s=1.2, seed=11)
-C2_QUERY_SEED = 50_000
+from asdmatch_b200.specs import (C0, C0_QUERY_SEED, C0D, C0D_QUERY_SEED, C1, C2_QUERIES, C2_QUERY_SEED, C4,  # noqa: F401
+                                  C4_QUERY_SEED, c2_seed_size)
+
 C2_COUNT_LIMIT = 10 ** 9
-C2_SCREEN_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c2_screened.json")
-# config 4: local subgraph counting; N=1.0M, M=10M, exponent 2.3, 32 labels Zipf(1.0), 10-vertex queries
-C4 = dict(n=1_000_000, m=10_000_000, gamma=2.3, nlabels=32, zipf_s=1.0, seed=41)
-C4_QUERY_SEED = 90_000
 C4_SCREEN_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c4_screened.json")
 
 
@@ -59,30 +50,15 @@ def write_workload(dirpath, g, qs, prefix="q"):
 
 
 def c2_candidate(g, i):
-    """The i-th candidate query of the C2 mixed batch: (seed, size, query)."""
-    seed = C2_QUERY_SEED + i
-    size = 4 + (seed * 2654435761 % 2 ** 32) % 29  # uniform in 4..32, decorrelated from the walk seed
+    """The i-th query of the C2 mixed batch: (seed, size, query)."""
+    seed, size = c2_seed_size(i)
     return seed, size, g.random_walk_query(size, seed, 0)
 
 
-def screen(dg, g, keep=1000, count_limit=C2_COUNT_LIMIT, time_limit_s=5.0, max_candidates=20000, log=None):
-    """Exact counts of C2 candidates in seed order; keeps those <= count_limit."""
-    kept, rejected = [], 0
-    for i in range(max_candidates):
-        if len(kept) >= keep:
-            break
-        seed, size, q = c2_candidate(g, i)
-        try:
-            r = A.count_query(dg, q, time_limit_s=time_limit_s, count_limit=count_limit)
-            kept.append(dict(index=i, seed=seed, size=size, edges=q.m2 // 2, count=r.count))
-        except A.AsdmError as e:
-            if e.code not in (A.ERR_LIMIT, A.ERR_TIMEOUT, A.ERR_OVERFLOW):
-                raise
-            rejected += 1
-        if log and (i + 1) % 100 == 0:
-            log("screened %d kept %d" % (i + 1, len(kept)))
-    return dict(spec=C1, query_seed=C2_QUERY_SEED, count_limit=count_limit, time_limit_s=time_limit_s,
-                candidates=len(kept) + rejected, rejected=rejected, queries=kept)
+def c2_batch(g, count=C2_QUERIES):
+    """The C2 mixed batch as specified: the first `count` queries in seed order,
+    sizes uniform in 4..32, none screened out."""
+    return [c2_candidate(g, i)[2] for i in range(count)]
 
 
 def c4_candidate(g, i, size=10):
@@ -125,39 +101,17 @@ def c4_queries(g, screen_data):
     return out
 
 
-def load_c2_screen():
-    with open(C2_SCREEN_FILE) as fh:
-        return json.load(fh)
-
-
-def c2_queries(g, screen_data):
-    """Regenerates the screened C2 queries from their indices."""
-    out = []
-    for rec in screen_data["queries"]:
-        seed, size, q = c2_candidate(g, rec["index"])
-        assert seed == rec["seed"] and size == rec["size"]
-        out.append(q)
-    return out
-
-
 if __name__ == "__main__":
-    # python -m asdmatch_b200.workloads c2 [keep] [out]   |   ... c4 [keep] [out] [size]
+    # python -m asdmatch_b200.workloads c4 [keep] [out] [size]: the config-4 local-counting screen
     import sys
     import time
     t = time.time()
-    which = sys.argv[1] if len(sys.argv) > 1 else "c2"
-    keep = int(sys.argv[2]) if len(sys.argv) > 2 else (1000 if which == "c2" else 50)
-    if which == "c2":
-        g = graph(C1)
-        dg = A.DeviceGraph(g)
-        data = screen(dg, g, keep=keep, log=print)
-        out = sys.argv[3] if len(sys.argv) > 3 else C2_SCREEN_FILE
-    else:
-        g = graph(C4)
-        dg = A.DeviceGraph(g)
-        size = int(sys.argv[4]) if len(sys.argv) > 4 else 8
-        data = screen_c4(dg, g, keep=keep, size=size, log=print)
-        out = sys.argv[3] if len(sys.argv) > 3 else C4_SCREEN_FILE
+    keep = int(sys.argv[2]) if len(sys.argv) > 2 else 50
+    g = graph(C4)
+    dg = A.DeviceGraph(g)
+    size = int(sys.argv[4]) if len(sys.argv) > 4 else 8
+    data = screen_c4(dg, g, keep=keep, size=size, log=print)
+    out = sys.argv[3] if len(sys.argv) > 3 else C4_SCREEN_FILE
     with open(out, "w") as fh:
         json.dump(data, fh, indent=0)
     print("screen done in %.1f s: kept %d of %d" % (time.time() - t, len(data["queries"]), data["candidates"]))

@@ -42,6 +42,14 @@
 //    storeMatches format (matching/join.cpp:1099-1107).  Counted here by plain
 //    backtracking over the candidate space, which is exact because the CFL
 //    filter only removes vertices that cannot be in any embedding.
+//  * For tree queries whose counts are too large to enumerate: the same count
+//    by inclusion-exclusion over same-label blocks (tree_count below), a
+//    restatement of the identity count = sum over partitions pi of mu(pi) *
+//    hom(Q/pi) that the product's tree program evaluates on the device
+//    (the identity itself is checked against brute-force embedding counts in
+//    tests/test_cpu_inclusion_exclusion.py).  Written independently of the
+//    device code: set partitions by recursion, quotient homomorphisms by a
+//    bottom-up product of sums over data adjacency, in 128-bit integers.
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -427,6 +435,130 @@ struct Enumerator {
     }
 };
 
+// hom(Q/pi) for the quotient of tree query q by the blocks `block` (block of
+// each vertex): a block's candidates are the data vertices that are candidates
+// of all its members; an edge between two blocks needs data adjacency.
+// Returns false when the quotient is not a tree.
+bool quotient_hom(const OGraph &q, const OGraph &g, const CandSpace &cs, const std::vector<uint32_t> &block,
+                  uint32_t nb, unsigned __int128 &out) {
+    std::vector<std::vector<uint32_t>> adj(nb), members(nb);
+    for (uint32_t u = 0; u < q.n; ++u) members[block[u]].push_back(u);
+    uint64_t nedges = 0;
+    for (uint32_t u = 0; u < q.n; ++u)
+        for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            const uint32_t a = block[u], b = block[q.nbr[e]];
+            if (a == b) return false;
+            if (std::find(adj[a].begin(), adj[a].end(), b) == adj[a].end()) {
+                adj[a].push_back(b);
+                ++nedges;
+            }
+        }
+    if (nedges != 2ull * (nb - 1)) return false;
+    // candidates of each block: intersection of its members' candidate sets
+    std::vector<std::vector<uint32_t>> cand(nb);
+    for (uint32_t b = 0; b < nb; ++b) {
+        cand[b] = cs.C[members[b][0]];
+        for (size_t k = 1; k < members[b].size(); ++k) {
+            std::vector<uint32_t> t;
+            const auto &o = cs.C[members[b][k]];
+            std::set_intersection(cand[b].begin(), cand[b].end(), o.begin(), o.end(), std::back_inserter(t));
+            cand[b].swap(t);
+        }
+    }
+    // rooted at block 0: BFS order, then weights bottom-up
+    std::vector<uint32_t> order{0}, parent(nb, UINT32_MAX);
+    std::vector<char> seen(nb, 0);
+    seen[0] = 1;
+    for (size_t k = 0; k < order.size(); ++k)
+        for (uint32_t c : adj[order[k]])
+            if (!seen[c]) {
+                seen[c] = 1;
+                parent[c] = order[k];
+                order.push_back(c);
+            }
+    if (order.size() != nb) return false;
+    std::vector<std::vector<unsigned __int128>> w(nb);
+    for (size_t k = order.size(); k-- > 0;) {
+        const uint32_t b = order[k];
+        const uint32_t lb = q.lab[members[b][0]];
+        w[b].assign(cand[b].size(), 1);
+        for (uint32_t c : adj[b]) {
+            if (parent[c] != b) continue;
+            const uint32_t lc = q.lab[members[c][0]];
+            for (size_t i = 0; i < cand[b].size(); ++i) {
+                if (w[b][i] == 0) continue;
+                uint64_t s0, s1;
+                g.run(cand[b][i], lc, s0, s1);
+                unsigned __int128 sum = 0;
+                for (uint64_t j = s0; j < s1; ++j) {
+                    const auto it = std::lower_bound(cand[c].begin(), cand[c].end(), g.nbr[j]);
+                    if (it != cand[c].end() && *it == g.nbr[j]) sum += w[c][it - cand[c].begin()];
+                }
+                w[b][i] *= sum;
+            }
+        }
+        (void)lb;
+    }
+    out = 0;
+    for (auto x : w[0]) out += x;
+    return true;
+}
+
+// Exact count of tree query q: sum over the partitions pi of the query
+// vertices into blocks of one label whose members are pairwise non-adjacent
+// of mu(pi) * hom(Q/pi), mu(pi) = prod over blocks of (-1)^(|B|-1) (|B|-1)!.
+// status: 0 exact (count set), 1 the count is >= 2^64, 2 not countable this
+// way (a quotient with a cycle, too many partitions, or a term too large).
+int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &count) {
+    count = 0;
+    if (q.n < 2 || q.m2 != 2ull * (q.n - 1)) return 2;
+    std::vector<uint32_t> block(q.n, 0);
+    std::vector<std::vector<uint32_t>> members;
+    __int128 total = 0;
+    size_t partitions = 0;
+    bool ok = true;
+    const __int128 limit = (__int128)1 << 120;
+    std::function<void(uint32_t)> place = [&](uint32_t u) {
+        if (!ok) return;
+        if (u == q.n) {
+            if (++partitions > (1u << 14)) { ok = false; return; }
+            __int128 mu = 1;
+            for (auto &m : members) {
+                __int128 f = 1;
+                for (size_t k = 2; k < m.size(); ++k) f *= (__int128)k;
+                mu *= (m.size() % 2 == 0) ? -f : f;
+            }
+            unsigned __int128 h = 0;
+            if (!quotient_hom(q, g, cs, block, (uint32_t)members.size(), h) || h >= (unsigned __int128)limit) {
+                ok = false;
+                return;
+            }
+            total += mu * (__int128)h;
+            return;
+        }
+        for (size_t b = 0; b < members.size() && ok; ++b) {
+            if (q.lab[members[b][0]] != q.lab[u]) continue;
+            bool adj = false;
+            for (uint32_t w : members[b]) adj = adj || q.adjacent(u, w);
+            if (adj) continue;
+            members[b].push_back(u);
+            block[u] = (uint32_t)b;
+            place(u + 1);
+            members[b].pop_back();
+        }
+        if (!ok) return;
+        block[u] = (uint32_t)members.size();
+        members.push_back({u});
+        place(u + 1);
+        members.pop_back();
+    };
+    place(0);
+    if (!ok || total < 0) return 2;
+    if (total >= ((__int128)1 << 64)) return 1;
+    count = (uint64_t)total;
+    return 0;
+}
+
 struct RunResult {
     uint64_t count = 0;
     bool overflow = false;
@@ -496,21 +628,51 @@ int orc_run(const char *qpath, const char *dpath, int mode, uint64_t *count, uin
     return rc;
 }
 
+// Tree queries of a list file (one path per line) against one data graph,
+// loaded once: one line per query on stdout, "T <k> ok <count>",
+// "T <k> overflow", "T <k> empty" (a candidate set is empty: count 0) or
+// "T <k> skip" (not a tree countable this way).
+int orc_tree_list(const char *dpath, const char *list) {
+    OGraph g;
+    if (!load_graph(dpath, g)) return 2;
+    std::ifstream in(list);
+    std::string qp;
+    for (uint32_t k = 0; std::getline(in, qp); ++k) {
+        if (qp.empty()) continue;
+        OGraph q;
+        if (!load_graph(qp, q)) return 2;
+        CandSpace cs = build_cfl(q, g);
+        if (!cs.ok) {
+            std::cout << "T " << k << " empty" << std::endl;
+            continue;
+        }
+        uint64_t c = 0;
+        const int st = tree_count(q, g, cs, c);
+        if (st == 0) std::cout << "T " << k << " ok " << c << std::endl;
+        else if (st == 1) std::cout << "T " << k << " overflow" << std::endl;
+        else std::cout << "T " << k << " skip" << std::endl;
+    }
+    return 0;
+}
+
 }  // extern "C"
 
 #ifdef ORACLE_MAIN
 // CLI: asdm_oracle -q Q -d D [-c csv] [-e emb] [-w csdump]; prints the
-// reference's "Number of matches:" line.
+// reference's "Number of matches:" line.  asdm_oracle -d D -t LIST: the tree
+// counts of the queries listed in LIST (orc_tree_list).
 int main(int argc, char **argv) {
-    std::string qp, dp, csv, emb, csd;
+    std::string qp, dp, csv, emb, csd, tl;
     for (int i = 1; i + 1 < argc; ++i) {
         std::string a = argv[i];
+        if (a == "-t") tl = argv[i + 1];
         if (a == "-q") qp = argv[i + 1];
         else if (a == "-d") dp = argv[i + 1];
         else if (a == "-c") csv = argv[i + 1];
         else if (a == "-e") emb = argv[i + 1];
         else if (a == "-w") csd = argv[i + 1];
     }
+    if (!tl.empty()) return orc_tree_list(dp.c_str(), tl.c_str()) == 0 ? 0 : 1;
     int mode = !emb.empty() ? MODE_EMBED : (!csv.empty() ? MODE_LOCAL : MODE_COUNT);
     uint64_t c = 0;
     uint32_t fl = 0;

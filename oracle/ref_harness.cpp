@@ -21,16 +21,30 @@
 //                   reference's storeMatches format (matching/join.cpp:1099-1107);
 //        -b <file>  the data graph in the reference's binary cache format
 //                   (Graph::writeToStream, relation/graph.cpp:316-332), then exit.
+//   3. many queries against one data graph (-Q <list> -O <dir> [-T s] [-J n]):
+//      the data graph is read once; each query of the list file (one path
+//      per line) runs in a child process forked from that state, with its
+//      report in <dir>/q<k>.out (k = line number, from 0), at most n children
+//      at a time, each killed after s seconds.  One line per query on
+//      stdout: "Q <k> ok|timeout|signal <n>|exit <n> <wall seconds>".  Every
+//      child starts from the same untouched state, as a fresh process would.
 // Build variants select the reference's compile-time modes (config/config.h:38-40):
 //   ref_count : ALL_LEVEL                          (exact counts)
 //   ref_local : ALL_LEVEL + LOCAL_COUNT            (+ |Vg|x|Vq| CSV via -c)
 //   ref_embed : ALL_LEVEL + LOCAL_COUNT + COLLECT_RESULT (+ -e dump)
+#include <signal.h>
+#include <sys/wait.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "adaptive.h"
@@ -50,10 +64,9 @@ static double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-int main(int argc, char **argv) {
-    Command cmd(argc, argv);
-    const std::string qpath = cmd.getQueryGraphPath();
-    const std::string dpath = cmd.getDataGraphPath();
+// One query against the loaded data graph g: the reference's ASDMatch.out
+// sequence after its graph loads (main.cpp:27-147).
+static int run_query(int argc, char **argv, Command &cmd, const std::string &qpath, Graph &g) {
     const std::string cardPath = cmd.getDPStructPath();
     const std::string csDump = option_after(argc, argv, "-w");
     const std::string embDump = option_after(argc, argv, "-e");
@@ -61,16 +74,8 @@ int main(int argc, char **argv) {
     if (memKB == 0) memKB = 16e5;
     const size_t budget = (size_t)1024 * memKB;
 
-    Graph q, g;
-    const std::string binOut = option_after(argc, argv, "-b");
-    if (!binOut.empty()) {
-        g.loadGraphFromTextFile(dpath);
-        std::ofstream os(binOut, std::ios::binary);
-        g.writeToStream(os);
-        return 0;
-    }
+    Graph q;
     q.loadGraphFromTextFile(qpath);
-    g.loadGraphFromTextFile(dpath);
     CandidateSpace cs(q, g);
 
     auto t0 = std::chrono::steady_clock::now();
@@ -191,4 +196,87 @@ int main(int argc, char **argv) {
     }
 #endif
     return 0;
+}
+
+// Harness difference 3: the queries of a list file, one forked child each.
+static int run_list(int argc, char **argv, Command &cmd, Graph &g, const std::string &list) {
+    const std::string outDir = option_after(argc, argv, "-O");
+    const std::string tArg = option_after(argc, argv, "-T"), jArg = option_after(argc, argv, "-J");
+    const double limit = tArg.empty() ? 0.0 : std::stod(tArg);
+    const int jobs = std::max(1, jArg.empty() ? 1 : std::stoi(jArg));
+    if (outDir.empty()) {
+        std::cerr << "-Q needs -O <dir>" << std::endl;
+        return 2;
+    }
+    std::vector<std::string> queries;
+    {
+        std::ifstream is(list);
+        std::string line;
+        while (std::getline(is, line))
+            if (!line.empty()) queries.push_back(line);
+    }
+    struct Child { size_t k; std::chrono::steady_clock::time_point t0; bool killed; };
+    std::map<pid_t, Child> running;
+    size_t next = 0;
+    std::cout.setf(std::ios::fixed);
+    while (next < queries.size() || !running.empty()) {
+        while (next < queries.size() && (int)running.size() < jobs) {
+            std::cout.flush();
+            const pid_t pid = fork();
+            if (pid == 0) {
+                const std::string out = outDir + "/q" + std::to_string(next) + ".out";
+                if (!std::freopen(out.c_str(), "w", stdout)) _exit(3);
+                const int rc = run_query(argc, argv, cmd, queries[next], g);
+                std::cout.flush();
+                std::fflush(stdout);
+                _exit(rc);
+            }
+            if (pid < 0) {
+                std::cerr << "fork failed" << std::endl;
+                return 2;
+            }
+            running[pid] = Child{next, std::chrono::steady_clock::now(), false};
+            ++next;
+        }
+        int wst = 0;
+        const pid_t done = waitpid(-1, &wst, WNOHANG);
+        if (done > 0) {
+            auto it = running.find(done);
+            if (it == running.end()) continue;
+            const double wall = seconds_since(it->second.t0);
+            std::cout << "Q " << it->second.k << " ";
+            if (it->second.killed) std::cout << "timeout";
+            else if (WIFSIGNALED(wst)) std::cout << "signal " << WTERMSIG(wst);
+            else if (WEXITSTATUS(wst) != 0) std::cout << "exit " << WEXITSTATUS(wst);
+            else std::cout << "ok";
+            std::cout << " " << wall << std::endl;
+            running.erase(it);
+            continue;
+        }
+        for (auto &kv : running)
+            if (limit > 0 && !kv.second.killed && seconds_since(kv.second.t0) > limit) {
+                kill(kv.first, SIGKILL);
+                kv.second.killed = true;
+            }
+        std::this_thread::sleep_for(std::chrono::milliseconds(5));
+    }
+    return 0;
+}
+
+int main(int argc, char **argv) {
+    Command cmd(argc, argv);
+    const std::string qpath = cmd.getQueryGraphPath();
+    const std::string dpath = cmd.getDataGraphPath();
+    Graph g;
+    const std::string binOut = option_after(argc, argv, "-b");
+    if (!binOut.empty()) {
+        g.loadGraphFromTextFile(dpath);
+        std::ofstream os(binOut, std::ios::binary);
+        g.writeToStream(os);
+        return 0;
+    }
+    const std::string list = option_after(argc, argv, "-Q");
+    g.loadGraphFromTextFile(dpath);
+    if (!list.empty()) return run_list(argc, argv, cmd, g, list);
+    return run_query(argc, argv, cmd, qpath, g);
 }

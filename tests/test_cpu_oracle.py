@@ -6,7 +6,7 @@ import pytest
 
 import oracle_util as O
 
-YEAST = "/root/reference/dataset/yeast.tar.gz"
+YEAST = O.reference_file("dataset", "yeast.tar.gz")
 
 
 def _check(rec, qpath, dpath, tmp_path, full):
@@ -43,7 +43,7 @@ def test_oracle_edge_cases(golden, c0_files, edge_files, tmp_path):
         _check(rec, edge_files[rec["name"]][1], dpath, tmp_path, "csv_sha" in rec)
 
 
-@pytest.mark.skipif(not (os.path.exists(YEAST) and O.ref_available()), reason="needs the reference tree and oracle/_ref")
+@pytest.mark.skipif(not (YEAST and O.ref_available()), reason="needs the reference tree and oracle/_ref")
 def test_oracle_matches_reference_on_yeast(tmp_path):
     import tarfile
     with tarfile.open(YEAST) as t:
@@ -58,3 +58,25 @@ def test_oracle_matches_reference_on_yeast(tmp_path):
             c, _ = O.oracle_run(q, dpath, O.MODE_COUNT, cs=ocs)
             assert c == r, q
             assert O.sha256_file(rcs) == O.sha256_file(ocs), q
+
+
+def test_oracle_tree_count_matches_golden_counts(golden, c0_files, tmp_path):
+    """The oracle's inclusion-exclusion tree count (asdm_oracle -t) equals the
+    reference's count on every config-0 tree query it can count this way."""
+    import subprocess
+    g, dpath, qs, qpaths = c0_files
+    O.build_oracle()
+    recs = [r for r in golden["sets"]["c0"] if qs[r["index"]].m2 // 2 == qs[r["index"]].n - 1]
+    lst = tmp_path / "trees.txt"
+    lst.write_text("\n".join(qpaths[r["index"]] for r in recs) + "\n")
+    out = subprocess.run([O.ORACLE_BIN, "-d", dpath, "-t", str(lst)], capture_output=True, text=True, check=True)
+    counted = 0
+    for line in out.stdout.splitlines():
+        _, k, st, *rest = line.split()
+        rec = recs[int(k)]
+        if st == "ok":
+            assert int(rest[0]) == rec["count"], rec["index"]
+            counted += 1
+        else:
+            assert st in ("skip", "empty") and (st == "skip" or rec["count"] == 0), (rec["index"], st)
+    assert counted >= 30
