@@ -102,7 +102,7 @@ _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_
                                                   C.POINTER(RunStats)])
 class Tuning(C.Structure):
     _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32), ("planner", C.c_uint32),
-                ("root_block_min", C.c_uint32)]
+                ("root_block_min", C.c_uint32), ("padded_cap_log2", C.c_uint32)]
 
 
 PLANNER_DP = 0
@@ -134,6 +134,8 @@ _run_batch_ex = _sig("asdm_run_batch_ex", C.c_int,
                       C.POINTER(C.c_int), C.POINTER(_u64p), C.POINTER(RunStats)])
 _cs_edge_totals = _sig("asdm_cs_edge_totals", C.c_int, [_vp, _u64p])
 _cs_lower_bound = _sig("asdm_cs_count_lower_bound", C.c_int, [_vp, _u64p, C.POINTER(C.c_int)])
+_cs_digest = _sig("asdm_cs_digest", C.c_int, [_vp, _u64p, _u32p])
+CS_TWO_SCAN, CS_LABEL_RUNS = 1, 2
 _est_create = _sig("asdm_est_create", C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(_vp)])
 _est_train = _sig("asdm_est_train_step", C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_float), _u32p, _u32p, _u32p,
                                                    C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)])
@@ -299,17 +301,19 @@ class DeviceGraph:
         self._spaces = weakref.WeakSet()
 
     def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None,
-                   root_block_min: Optional[int] = None):
+                   root_block_min: Optional[int] = None, padded_cap_log2: Optional[int] = None):
         cur = self.tuning()
         planner = cur["planner"] if planner is None else planner
         root_block_min = cur["root_block_min"] if root_block_min is None else root_block_min
-        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner, root_block_min))), "tuning")
+        padded_cap_log2 = cur["padded_cap_log2"] if padded_cap_log2 is None else padded_cap_log2
+        _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner, root_block_min,
+                                                   padded_cap_log2))), "tuning")
 
     def tuning(self):
         t = Tuning()
         _check(_get_tuning(self._h, C.byref(t)))
         return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max, "planner": t.planner,
-                "root_block_min": t.root_block_min}
+                "root_block_min": t.root_block_min, "padded_cap_log2": t.padded_cap_log2}
 
     def stream(self) -> int:
         """cudaStream_t (as an int) the library uses for this graph."""
@@ -357,6 +361,14 @@ class CandidateSpace:
         out = np.zeros(max(int(self.q.offsets[-1]), 1), np.uint64)
         _check(_cs_edge_totals(self._h, _ptr(out, _u64p)))
         return out[:int(self.q.offsets[-1])]
+
+    def digest(self):
+        """(digest, flags): a device-computed 64-bit digest of C(u) and the
+        candidate-edge lists, and the CS_* bits of how they were built."""
+        d = C.c_uint64()
+        f = C.c_uint32()
+        _check(_cs_digest(self._h, C.byref(d), C.byref(f)), "digest")
+        return int(d.value), int(f.value)
 
     def count_lower_bound(self):
         """(bound, exceeds): a lower bound of the embedding count (capped at

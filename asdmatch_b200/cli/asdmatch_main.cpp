@@ -13,7 +13,8 @@
 // writes the sorted embedding set in storeMatches format
 // (matching/join.cpp:1099-1107), -t sets a device time limit.  -a and -i are
 // accepted and ignored, like the reference.  Counts are always exact (the
-// reference's ALL_LEVEL semantics).
+// reference's ALL_LEVEL semantics); a count of 2^64 or more is reported as
+// "Number of matches: overflow (at least 18446744073709551616)".
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -94,7 +95,9 @@ int main(int argc, char **argv) {
     if ((rc = cache ? asdm_plan_create_card(cs, cache, &plan) : asdm_plan_create(cs, nullptr, &plan))) die("plan", rc);
     asdm_card_free(cache);
     out << "Planning Time: " << since(t0) << std::endl;
-    out << "cost: " << 0 << std::endl;
+    double cost = 0.0;
+    asdm_plan_cost(plan, &cost);
+    out << "cost: " << cost << std::endl;
 
     asdm_run_opts o{};
     o.mode = ASDM_MODE_COUNT;
@@ -120,7 +123,21 @@ int main(int argc, char **argv) {
         o.embeddings = rows.data();
         o.emb_capacity = st.count;
     }
-    if ((rc = asdm_run_plan(cs, plan, &o, &st))) die("enumeration", rc);
+    rc = asdm_run_plan(cs, plan, &o, &st);
+    if (rc == ASDM_ERR_OVERFLOW) {
+        // the count is at least 2^64: a uint64 cannot hold it (the reference's
+        // size_t would wrap); the report says so instead of a wrapped number
+        out << "Execution Time: " << since(t0) << std::endl;
+        out << "Number of matches: overflow (at least 18446744073709551616)" << std::endl;
+        out << "Number of intersections: " << st.intersections << std::endl;
+        asdm_plan_free(plan);
+        asdm_cs_free(cs);
+        asdm_graph_free(dg);
+        asdm_host_graph_free(q);
+        asdm_host_graph_free(g);
+        return 0;
+    }
+    if (rc) die("enumeration", rc);
     out << "Execution Time: " << since(t0) << std::endl;
     out << "Number of matches: " << st.count << std::endl;
     out << "Number of fixed attributes: " << 0 << std::endl;

@@ -97,6 +97,7 @@ extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
     if (t->root_block_min < 1 || t->root_block_min > 256) return fail(ASDM_ERR_INVALID, "root_block_min must be 1..256");
     if (t->planner != ASDM_PLANNER_DP && t->planner != ASDM_PLANNER_GREEDY)
         return fail(ASDM_ERR_INVALID, "planner must be ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY");
+    if (t->padded_cap_log2 < 20 || t->padded_cap_log2 > 34) return fail(ASDM_ERR_INVALID, "padded_cap_log2 must be 20..34");
     g->tuning = *t;
     return ASDM_OK;
 }
@@ -119,6 +120,59 @@ extern "C" int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *b
     if (build_bytes) *build_bytes = cs->build_bytes;
     if (build_ms) *build_ms = cs->build_ms;
     return ASDM_OK;
+}
+
+namespace asdm {
+__device__ __forceinline__ unsigned long long digest_mix64(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Sum over i of mix(tag, i, a[i]): independent of the order threads add in.
+__global__ void digest_kernel(const uint32_t *__restrict__ a, uint64_t n, unsigned long long tag,
+                              unsigned long long *__restrict__ out) {
+    unsigned long long acc = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        acc += digest_mix64(tag * 0x9E3779B97F4A7C15ull + i * 0xD1B54A32D192ED03ull + a[i]);
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+}  // namespace asdm
+
+extern "C" int asdm_cs_digest(const asdm_cs *cs, uint64_t *digest, uint32_t *flags) {
+    clear_error();
+    if (!cs || !digest) return fail(ASDM_ERR_INVALID, "null argument");
+    *digest = 0;
+    if (flags) *flags = cs->build_flags;
+    if (!cs->nonempty) return ASDM_OK;
+    cudaStream_t s = cs->g->stream;
+    unsigned long long *d = nullptr;
+    ASDM_TRY(dalloc(&d, 1, s));
+    int rc = cudaMemsetAsync(d, 0, sizeof(unsigned long long), s) == cudaSuccess ? ASDM_OK
+                                                                                  : fail(ASDM_ERR_CUDA, "digest reset");
+    const QueryGraph &q = cs->q;
+    auto run = [&](const uint32_t *a, uint64_t n, unsigned long long tag) {
+        if (rc != ASDM_OK || n == 0) return;
+        const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+        digest_kernel<<<grid, 256, 0, s>>>(a, n, tag, d);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "digest kernel failed");
+    };
+    for (uint32_t u = 0; u < q.n; ++u) run(cs->d_cand + cs->cand_base[u], cs->ncand[u], 1 + u);
+    for (uint32_t u = 0; u < q.n; ++u)
+        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+            run(cs->d_eoff + cs->eoff_base[e], cs->ncand[u] + 1ull, 1000 + 2ull * e);
+            run(cs->d_elist + cs->elist_base[e], cs->etotal[e], 1001 + 2ull * e);
+        }
+    unsigned long long h = 0;
+    if (rc == ASDM_OK && (cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                          cudaStreamSynchronize(s) != cudaSuccess))
+        rc = fail(ASDM_ERR_CUDA, "digest readback failed");
+    dfree(d, s);
+    cudaStreamSynchronize(s);
+    *digest = h;
+    return rc;
 }
 
 extern "C" const char *asdm_version(void) { return "asdmatch-b200 0.1 (sm_100a)"; }
@@ -194,7 +248,7 @@ int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uin
 
 // Candidate-space state a group may hold at once (state words, storage and
 // candidate arrays: 12 bytes per data vertex of each query vertex's label).
-static constexpr uint64_t kGroupStateBytes = 16ull << 30;
+static constexpr uint64_t kGroupStateBytes = 32ull << 30;
 
 static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, const uint64_t *q_off_base,
                           const uint32_t *q_offsets, const uint64_t *q_nbr_base, const uint32_t *q_nbrs,

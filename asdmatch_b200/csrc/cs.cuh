@@ -41,6 +41,7 @@ struct asdm_cs {
     uint32_t *d_elist = nullptr;
     uint64_t build_bytes = 0;              // algorithmic bytes of K1-K3 (roofline)
     float build_ms = 0.f;                  // device time of K1-K3
+    uint32_t build_flags = 0;              // ASDM_CS_* bits: which K3 form built the edges, label-run table
     std::shared_ptr<CsArena> arena;        // owns d_cand / d_eoff / d_elist
 };
 

@@ -34,9 +34,6 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr uint32_t kLongRun = 32;
-// K3b pads candidate-edge lists to their label-run lengths up to this many
-// entries in total (4 GiB), and counts first beyond it.
-constexpr uint64_t kPaddedEdgeCap = 1ull << 30;
 
 __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ prefix, uint32_t nseg, uint64_t item) {
     // last s with prefix[s] <= item (prefix has nseg + 1 entries, non-decreasing)
@@ -1130,6 +1127,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     const uint32_t ne = (uint32_t)edges.size();
     const uint64_t nitems = item_base.back();
     std::vector<uint64_t> estart(ne, 0);
+    bool two_scan = false;
     uint64_t total = 0;
     if (ne) {
         EdgeDesc *d_edges = nullptr;
@@ -1161,7 +1159,11 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
         ASDM_CUDA(cudaMemcpyAsync(&bound, d_upos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         ASDM_CUDA(cudaStreamSynchronize(s));
-        if (bound <= kPaddedEdgeCap) {
+        // padded lists up to 2^padded_cap_log2 entries in total (default 2^32:
+        // 16 GiB), the exact two-scan form beyond
+        const uint64_t padded_cap = 1ull << G->tuning.padded_cap_log2;
+        two_scan = bound > padded_cap;
+        if (bound <= padded_cap) {
             uint32_t *padded = nullptr;
             ASDM_TRY(scr.alloc(&padded, bound));
             k3_flat<<<egrid, kBlock, 0, s>>>(g, d_edges, d_ib, ne, arena->d_eoff, d_upos, rstart, padded, d_elems + 1);
@@ -1216,6 +1218,7 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         asdm_cs &cs = *qp.cs;
         cs.build_ms = ms / Q;
         cs.build_bytes = bytes / Q;
+        cs.build_flags = (two_scan ? ASDM_CS_TWO_SCAN : 0u) | (g.lab_pos ? ASDM_CS_LABEL_RUNS : 0u);
         cs.arena = arena;
         cs.d_cand = arena->d_cand;
         cs.d_eoff = arena->d_eoff;

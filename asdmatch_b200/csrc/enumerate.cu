@@ -1815,8 +1815,9 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
             return ASDM_OK;
         }
     }
-    if (mode == ASDM_MODE_COUNT && plan.order.size() == n) {
+    if (plan.order.size() == n) {
         // a lower bound at or above 2^64 settles the query without enumeration
+        // (in every mode: local counts or embeddings of such a query do not fit)
         std::vector<char> proven;
         ASDM_TRY(overflow_bounds(G, {&cs}, proven));
         if (proven[0]) return fail(ASDM_ERR_OVERFLOW, "match count exceeds 2^64-1 (shown by a lower bound)");
@@ -2127,7 +2128,11 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             if (agg) agg->kernel_ms += tree_ms;
             if (live.empty()) return ASDM_OK;
         }
-        // queries whose count a lower bound shows to be at least 2^64 are settled as overflows
+    }
+    {
+        // queries whose count a lower bound shows to be at least 2^64 are
+        // settled as overflows (in LOCAL mode too: their matrices would have
+        // a column summing past 2^64 - 1)
         std::vector<asdm_cs *> ocs;
         std::vector<uint32_t> oid;
         for (uint32_t i : live)

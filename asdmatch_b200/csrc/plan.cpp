@@ -267,11 +267,34 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
     const uint32_t n = q.n;
     if (!cs.nonempty) return fail(ASDM_ERR_INVALID, "cannot plan over an empty candidate space");
     if (user_order) {
-        p.order.assign(user_order, user_order + n);
+        std::vector<uint32_t> given(user_order, user_order + n);
         std::vector<char> seen(n, 0);
         for (uint32_t k = 0; k < n; ++k) {
-            if (p.order[k] >= n || seen[p.order[k]]) return fail(ASDM_ERR_INVALID, "order is not a permutation");
-            seen[p.order[k]] = 1;
+            if (given[k] >= n || seen[given[k]]) return fail(ASDM_ERR_INVALID, "order is not a permutation");
+            seen[given[k]] = 1;
+        }
+        // An order whose vertex has no earlier neighbour is the reference's
+        // Cartesian attribute (cartesianParent, plan/decomposition.cpp:7-88,
+        // enumerated by optimizedCartesianProduct, plan/estimator.cpp:41-171).
+        // Counts do not depend on the order, so such a vertex is deferred to
+        // the first position where an earlier neighbour exists: the order
+        // stays the caller's wherever it is connected.
+        p.order.clear();
+        std::vector<char> in(n, 0), taken(n, 0);
+        while (p.order.size() < n) {
+            bool placed = false;
+            for (uint32_t k = 0; k < n && !placed; ++k) {
+                const uint32_t u = given[k];
+                if (taken[k]) continue;
+                bool linked = p.order.empty();
+                for (uint32_t e = q.off[u]; e < q.off[u + 1] && !linked; ++e) linked = in[q.nbr[e]] != 0;
+                if (!linked) continue;
+                p.order.push_back(u);
+                in[u] = 1;
+                taken[k] = 1;
+                placed = true;
+            }
+            if (!placed) return fail(ASDM_ERR_INVALID, "query is not connected");
         }
         p.cost = 0;
     } else if (cs.g->tuning.planner == ASDM_PLANNER_DP &&
@@ -367,6 +390,12 @@ extern "C" int asdm_plan_create_card(const asdm_cs *cs, const asdm_card *card, a
 extern "C" int asdm_plan_order(const asdm_plan *p, uint32_t *order) {
     if (!p || !order) return fail(ASDM_ERR_INVALID, "null argument");
     std::copy(p->order.begin(), p->order.end(), order);
+    return ASDM_OK;
+}
+
+extern "C" int asdm_plan_cost(const asdm_plan *p, double *cost) {
+    if (!p || !cost) return fail(ASDM_ERR_INVALID, "null argument");
+    *cost = p->cost;
     return ASDM_OK;
 }
 

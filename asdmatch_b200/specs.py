@@ -10,8 +10,10 @@ file by path and runs the host-only generator asdmatch_b200/bin/asdm_gen.out.
         Patents), resident in HBM.
 * C2  — the C1 graph with the mixed batch: query i has seed C2_QUERY_SEED + i
         and a size uniform in 4..32 (c2_size).
+* C1 queries — 100 queries each of 12 and 16 vertices on the C1 graph, half
+        dense (average query degree >= 3) and half sparse (< 3): c1_query_specs.
 * C4  — local subgraph counting: N=1.0M, M=10M, exponent 2.3, 32 labels
-        Zipf(1.0), 10-vertex queries.
+        Zipf(1.0), 50 random-walk queries of 10 vertices: c4_query_specs.
 """
 
 C0 = dict(n=3112, m=12519, gamma=2.5, nlabels=71, zipf_s=1.0, seed=1)
@@ -21,8 +23,12 @@ C0D_QUERY_SEED = 3000
 C1 = dict(n=3_770_000, m=16_500_000, gamma=2.1, nlabels=20, zipf_s=1.2, seed=11)
 C2_QUERY_SEED = 50_000
 C2_QUERIES = 1000
+C1_QUERY_SEED = 70_000
 C4 = dict(n=1_000_000, m=10_000_000, gamma=2.3, nlabels=32, zipf_s=1.0, seed=41)
 C4_QUERY_SEED = 90_000
+C4_QUERIES = 50
+C4_QUERY_SIZE = 10
+DENSE, SPARSE = 1, 2  # density argument of the query generator
 
 
 def c2_seed_size(i):
@@ -30,6 +36,22 @@ def c2_seed_size(i):
     4..32, decorrelated from the walk seed."""
     seed = C2_QUERY_SEED + i
     return seed, 4 + (seed * 2654435761 % 2 ** 32) % 29
+
+
+def c1_query_specs():
+    """(size, seed, density) of the config-1 queries: for 12 and 16 vertices,
+    50 dense then 50 sparse."""
+    out = []
+    for size in (12, 16):
+        for density in (DENSE, SPARSE):
+            for i in range(50):
+                out.append((size, C1_QUERY_SEED + 1000 * size + 100 * density + i, density))
+    return out
+
+
+def c4_query_specs():
+    """(size, seed, density) of the config-4 queries."""
+    return [(C4_QUERY_SIZE, C4_QUERY_SEED + i, 0) for i in range(C4_QUERIES)]
 
 
 def generator_args(spec):

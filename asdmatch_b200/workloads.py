@@ -22,7 +22,7 @@ import os
 import asdmatch_b200 as A
 
 from asdmatch_b200.specs import (C0, C0_QUERY_SEED, C0D, C0D_QUERY_SEED, C1, C2_QUERIES, C2_QUERY_SEED, C4,  # noqa: F401
-                                  C4_QUERY_SEED, c2_seed_size)
+                                  C4_QUERY_SEED, c1_query_specs, c2_seed_size, c4_query_specs)
 
 C2_COUNT_LIMIT = 10 ** 9
 C4_SCREEN_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c4_screened.json")
@@ -59,6 +59,21 @@ def c2_batch(g, count=C2_QUERIES):
     """The C2 mixed batch as specified: the first `count` queries in seed order,
     sizes uniform in 4..32, none screened out."""
     return [c2_candidate(g, i)[2] for i in range(count)]
+
+
+def from_specs(g, specs):
+    """Queries of (size, seed, density) specs."""
+    return [g.random_walk_query(size, seed, density) for size, seed, density in specs]
+
+
+def c1_batch(g):
+    """The config-1 queries: 100 each of 12 and 16 vertices, half dense, half sparse."""
+    return from_specs(g, c1_query_specs())
+
+
+def c4_batch(g):
+    """The config-4 queries: 50 random-walk queries of 10 vertices."""
+    return from_specs(g, c4_query_specs())
 
 
 def c4_candidate(g, i, size=10):

@@ -123,6 +123,9 @@ typedef struct asdm_tuning {
     uint32_t planner;          /* ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY */
     uint32_t root_block_min;   /* batches: fewest (level-0, level-1) pairs per root task of plans of at
                                   most 4 levels with a closed-form tail, 1..256 (default 64) */
+    uint32_t padded_cap_log2;  /* candidate edges of a group are filled into lists padded to their
+                                  label-run lengths when those total at most 2^this entries, else
+                                  counted first and filled exactly (20..34, default 32) */
 } asdm_tuning;
 /* Order search: exhaustive over connected prefixes where the query is small
  * enough (at most 24 vertices and 4096 connected vertex subsets), else
@@ -160,6 +163,15 @@ int asdm_cs_edge_totals(const asdm_cs *cs, uint64_t *totals);
 /* Algorithmic bytes and device milliseconds of the K1-K3 build (the
  * reference's "Filtering time", main.cpp:38). */
 int asdm_cs_stats(const asdm_cs *cs, uint64_t *build_bytes, double *build_ms);
+/* A 64-bit digest of the candidate space (every C(u) and every candidate-edge
+ * list with its offsets, position-sensitive), computed on the device, so that
+ * two builds can be compared without reading them back; *flags receives the
+ * ASDM_CS_* bits of its build.  For tests at scale; no reference counterpart
+ * (the reference compares CandidateSpace::writeToStream text,
+ * relation/candidate_space.cpp:489-505). */
+#define ASDM_CS_TWO_SCAN 1u   /* K3 counted, then filled (its group passed the padded-entry cap) */
+#define ASDM_CS_LABEL_RUNS 2u /* the graph's dense label-run table was used                      */
+int asdm_cs_digest(const asdm_cs *cs, uint64_t *digest, uint32_t *flags);
 int asdm_cs_free(asdm_cs *cs);
 
 /* ---- sorted-set intersection (K4) --------------------------------------- */
@@ -181,6 +193,10 @@ int asdm_intersect_batch(const uint32_t *values, const uint64_t *list_off, uint6
  * connected permutation of the query vertices. */
 int asdm_plan_create(const asdm_cs *cs, const uint32_t *order, asdm_plan **out);
 int asdm_plan_order(const asdm_plan *p, uint32_t *order);
+/* The planner's estimated cost of the plan (partial matches times work per
+ * extension), the figure the reference prints as "cost:" (minCost of
+ * optCostPlan/simplePlan, main.cpp:100-114). */
+int asdm_plan_cost(const asdm_plan *p, double *cost);
 /* Planner guided by a cardinality cache: prefixes whose vertex set is in the
  * cache use the cached cardinality (ASDMatch.out -s; the reference loads the
  * same map with loadSubsetToCard, plan/estimator.cpp:994-1008). */
@@ -277,7 +293,7 @@ int asdm_count_query(asdm_graph *g, const uint32_t *q_offsets, const uint32_t *q
  * counterpart; the reference runs one query per process).  Query i is the CSR
  * slice q_offsets[q_off_base[i] ..], q_nbrs[q_nbr_base[i] ..],
  * q_labels[q_lab_base[i] ..] with q_sizes[i] vertices.  Queries are grouped
- * (up to 16 GiB of candidate-space state per group); each group builds its
+ * (up to 32 GiB of candidate-space state per group); each group builds its
  * candidate spaces with one launch per CFL phase and counts with one
  * persistent kernel over all (query, root task) pairs.  counts[i] and
  * status[i] receive each query's result; stats (nullable) the totals; the

@@ -559,6 +559,124 @@ int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &
     return 0;
 }
 
+// The device's overflow lower bound, restated from its definition (the set
+// of embeddings it counts), not from the kernels: same-label query vertices
+// that are not adjacent get distinct classes (greedy colouring in vertex
+// order), a query vertex may only take candidates whose hashed class is its
+// own; a feedback vertex set (peel vertices of degree <= 1, then take the
+// vertex of highest remaining degree, lowest id first) is fixed to the
+// highest-degree candidate of its class (lowest id on ties); the forest left
+// is counted exactly.  Returns 0 and lb (saturated at 2^127) when a bound is
+// formed, 1 when the rules form none (more than 6 fixed vertices).
+uint32_t vertex_class(uint32_t v, uint32_t k) {
+    return (uint32_t)((((unsigned __int128)v * 0x9E3779B97F4A7C15ull) >> 32) % k);
+}
+
+int lower_bound(const OGraph &q, const OGraph &g, const CandSpace &cs, unsigned __int128 &lb) {
+    const uint32_t n = q.n;
+    const unsigned __int128 kSat = (unsigned __int128)1 << 127;
+    auto sat_mul = [&](unsigned __int128 a, unsigned __int128 b) -> unsigned __int128 {
+        if (a == 0 || b == 0) return 0;
+        if (a >= kSat || b >= kSat || a > kSat / b) return kSat;
+        return a * b;
+    };
+    auto sat_add = [&](unsigned __int128 a, unsigned __int128 b) -> unsigned __int128 {
+        return (a >= kSat || b >= kSat || a + b >= kSat) ? kSat : a + b;
+    };
+    lb = 0;
+    std::vector<char> fixed(n, 0), gone(n, 0);
+    std::vector<uint32_t> fvs, deg(n);
+    for (uint32_t u = 0; u < n; ++u) deg[u] = q.deg(u);
+    auto drop = [&](uint32_t u) {
+        gone[u] = 1;
+        for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e)
+            if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+    };
+    for (;;) {
+        for (bool changed = true; changed;) {
+            changed = false;
+            for (uint32_t u = 0; u < n; ++u)
+                if (!gone[u] && deg[u] <= 1) { drop(u); changed = true; }
+        }
+        int best = -1;
+        for (uint32_t u = 0; u < n; ++u)
+            if (!gone[u] && (best < 0 || deg[u] > deg[best])) best = (int)u;
+        if (best < 0) break;
+        fixed[best] = 1;
+        fvs.push_back((uint32_t)best);
+        drop((uint32_t)best);
+    }
+    if (fvs.size() > 6 || fvs.size() == n) return 1;
+    std::vector<uint32_t> cls(n, 0), ncls(n, 1);
+    for (uint32_t u = 0; u < n; ++u) {
+        std::vector<char> used(n + 1, 0);
+        for (uint32_t w = 0; w < u; ++w)
+            if (q.lab[w] == q.lab[u] && !q.adjacent(u, w)) used[cls[w]] = 1;
+        while (used[cls[u]]) ++cls[u];
+    }
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t w = 0; w < n; ++w)
+            if (q.lab[w] == q.lab[u]) ncls[u] = std::max(ncls[u], cls[w] + 1);
+    auto allowed = [&](uint32_t u, uint32_t v) { return ncls[u] <= 1 || vertex_class(v, ncls[u]) == cls[u]; };
+    std::vector<uint32_t> hub(n, UINT32_MAX);
+    for (uint32_t f : fvs) {
+        for (uint32_t v : cs.C[f])
+            if (allowed(f, v) && (hub[f] == UINT32_MAX || g.deg(v) > g.deg(hub[f]))) hub[f] = v;
+        if (hub[f] == UINT32_MAX) return 0;  // lb = 0
+    }
+    for (uint32_t f : fvs)
+        for (uint32_t f2 : fvs)
+            if (f < f2 && q.adjacent(f, f2) && !g.adjacent(hub[f], hub[f2])) return 0;
+    // forest components, rooted at their lowest vertex; weights bottom-up
+    std::vector<uint32_t> comp(n, UINT32_MAX), parent(n, UINT32_MAX), order;
+    unsigned __int128 prod = 1;
+    for (uint32_t r = 0; r < n; ++r) {
+        if (fixed[r] || comp[r] != UINT32_MAX) continue;
+        const size_t first = order.size();
+        comp[r] = r;
+        order.push_back(r);
+        for (size_t k = first; k < order.size(); ++k)
+            for (uint64_t e = q.off[order[k]]; e < q.off[order[k] + 1]; ++e) {
+                const uint32_t w = q.nbr[e];
+                if (fixed[w] || comp[w] != UINT32_MAX) continue;
+                comp[w] = r;
+                parent[w] = order[k];
+                order.push_back(w);
+            }
+        std::vector<std::vector<unsigned __int128>> wt(n);
+        for (size_t k = order.size(); k-- > first;) {
+            const uint32_t u = order[k];
+            const auto &C = cs.C[u];
+            wt[u].assign(C.size(), 0);
+            for (size_t i = 0; i < C.size(); ++i) {
+                if (!allowed(u, C[i])) continue;
+                unsigned __int128 acc = 1;
+                for (uint64_t e = q.off[u]; e < q.off[u + 1] && acc; ++e) {
+                    const uint32_t c = q.nbr[e];
+                    if (fixed[c]) {
+                        acc = g.adjacent(C[i], hub[c]) ? acc : 0;
+                    } else if (parent[c] == u) {
+                        uint64_t s0, s1;
+                        g.run(C[i], q.lab[c], s0, s1);
+                        unsigned __int128 sum = 0;
+                        for (uint64_t j = s0; j < s1; ++j) {
+                            const auto it = std::lower_bound(cs.C[c].begin(), cs.C[c].end(), g.nbr[j]);
+                            if (it != cs.C[c].end() && *it == g.nbr[j]) sum = sat_add(sum, wt[c][it - cs.C[c].begin()]);
+                        }
+                        acc = sat_mul(acc, sum);
+                    }
+                }
+                wt[u][i] = acc;
+            }
+        }
+        unsigned __int128 tot = 0;
+        for (auto x : wt[r]) tot = sat_add(tot, x);
+        prod = sat_mul(prod, tot);
+    }
+    lb = prod;
+    return 0;
+}
+
 struct RunResult {
     uint64_t count = 0;
     bool overflow = false;
@@ -655,17 +773,53 @@ int orc_tree_list(const char *dpath, const char *list) {
     return 0;
 }
 
+// The lower bounds of the queries of a list file against one data graph:
+// "B <k> <bound>" (decimal, saturated at 2^127), "B <k> none" when the rules
+// form no bound, "B <k> empty" for an empty candidate set.
+int orc_bound_list(const char *dpath, const char *list) {
+    OGraph g;
+    if (!load_graph(dpath, g)) return 2;
+    std::ifstream in(list);
+    std::string qp;
+    for (uint32_t k = 0; std::getline(in, qp); ++k) {
+        if (qp.empty()) continue;
+        OGraph q;
+        if (!load_graph(qp, q)) return 2;
+        CandSpace cs = build_cfl(q, g);
+        if (!cs.ok) {
+            std::cout << "B " << k << " empty" << std::endl;
+            continue;
+        }
+        unsigned __int128 lb = 0;
+        if (lower_bound(q, g, cs, lb) != 0) {
+            std::cout << "B " << k << " none" << std::endl;
+            continue;
+        }
+        char buf[64];
+        int p = 63;
+        buf[p] = 0;
+        do {
+            buf[--p] = (char)('0' + (int)(lb % 10));
+            lb /= 10;
+        } while (lb);
+        std::cout << "B " << k << " " << (buf + p) << std::endl;
+    }
+    return 0;
+}
+
 }  // extern "C"
 
 #ifdef ORACLE_MAIN
 // CLI: asdm_oracle -q Q -d D [-c csv] [-e emb] [-w csdump]; prints the
 // reference's "Number of matches:" line.  asdm_oracle -d D -t LIST: the tree
-// counts of the queries listed in LIST (orc_tree_list).
+// counts of the queries listed in LIST (orc_tree_list); -b LIST: their
+// overflow lower bounds (orc_bound_list).
 int main(int argc, char **argv) {
-    std::string qp, dp, csv, emb, csd, tl;
+    std::string qp, dp, csv, emb, csd, tl, bl;
     for (int i = 1; i + 1 < argc; ++i) {
         std::string a = argv[i];
         if (a == "-t") tl = argv[i + 1];
+        if (a == "-b") bl = argv[i + 1];
         if (a == "-q") qp = argv[i + 1];
         else if (a == "-d") dp = argv[i + 1];
         else if (a == "-c") csv = argv[i + 1];
@@ -673,6 +827,7 @@ int main(int argc, char **argv) {
         else if (a == "-w") csd = argv[i + 1];
     }
     if (!tl.empty()) return orc_tree_list(dp.c_str(), tl.c_str()) == 0 ? 0 : 1;
+    if (!bl.empty()) return orc_bound_list(dp.c_str(), bl.c_str()) == 0 ? 0 : 1;
     int mode = !emb.empty() ? MODE_EMBED : (!csv.empty() ? MODE_LOCAL : MODE_COUNT);
     uint64_t c = 0;
     uint32_t fl = 0;

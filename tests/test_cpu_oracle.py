@@ -80,3 +80,25 @@ def test_oracle_tree_count_matches_golden_counts(golden, c0_files, tmp_path):
         else:
             assert st in ("skip", "empty") and (st == "skip" or rec["count"] == 0), (rec["index"], st)
     assert counted >= 30
+
+
+def test_oracle_lower_bound_never_exceeds_golden_counts(golden, c0_files, tmp_path):
+    """The oracle's restatement of the device's overflow lower bound (asdm_oracle
+    -b) counts a subset of the embeddings: never more than the reference's count."""
+    import subprocess
+    g, dpath, qs, qpaths = c0_files
+    O.build_oracle()
+    recs = golden["sets"]["c0"]
+    lst = tmp_path / "all.txt"
+    lst.write_text("\n".join(qpaths[r["index"]] for r in recs) + "\n")
+    out = subprocess.run([O.ORACLE_BIN, "-d", dpath, "-b", str(lst)], capture_output=True, text=True, check=True)
+    formed = positive = 0
+    for line in out.stdout.splitlines():
+        _, k, v = line.split()
+        rec = recs[int(k)]
+        if v in ("none", "empty"):
+            continue
+        formed += 1
+        assert int(v) <= rec["count"], (rec["index"], v, rec["count"])
+        positive += int(v) > 0
+    assert formed >= 150 and positive >= 20

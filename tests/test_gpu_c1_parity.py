@@ -1,0 +1,117 @@
+"""Parity on the config-1 graph (N=3.77M, M=16.5M, 20 labels): 52 queries of
+the config-2 batch, two of every size from 7 to 32 (the set is fixed in
+tests/golden/c2_batch.json, "parity").
+
+Every outcome is checked against a CPU result made by the committed scripts:
+* an exact count against the reference's own count where the reference
+  finished (oracle/_ref/ref_count), and against the oracle's
+  inclusion-exclusion tree count where the oracle could count the query;
+* an overflow (count >= 2^64) against the oracle's tree count, which must not
+  be an exact count below 2^64;
+* the device's lower bound against the oracle's restatement of the same bound
+  (asdm_oracle -b), which must agree to within rounding toward zero;
+* candidate spaces built for the whole set in one group, in both forms of the
+  candidate-edge build (padded lists, and counting then filling), against the
+  same queries built one by one (device digests of every C(u) and
+  candidate-edge list), on a graph whose dense label-run table is used.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import asdmatch_b200 as A
+from asdmatch_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_batch.json")
+TWO64 = 1 << 64
+
+
+@pytest.fixture(scope="module")
+def c1():
+    with open(GOLDEN) as fh:
+        data = json.load(fh)
+    if "parity" not in data:
+        pytest.skip("no parity set in c2_batch.json")
+    recs = {r["index"]: r for r in data["queries"]}
+    g = W.graph(W.C1)
+    dg = A.DeviceGraph(g)
+    qs = {i: W.c2_candidate(g, i)[2] for i in data["parity"]}
+    yield dg, data["parity"], qs, recs
+    dg.close()
+
+
+def test_counts_overflows_and_timeouts_against_reference_and_oracle(c1):
+    dg, parity, qs, recs = c1
+    b = A.BatchInput([qs[i] for i in parity])
+    A.run_batch_ex(dg, b, query_time_limit_s=0.1)
+    exact = overflow = 0
+    for i, c, st in zip(parity, b.counts.tolist(), b.status.tolist()):
+        r = recs[i]
+        ref = r.get("count")
+        tree = r.get("oracle_tree")
+        assert st in (A.OK, A.ERR_OVERFLOW, A.ERR_TIMEOUT), (i, st)
+        if ref is not None:
+            assert st == A.OK and c == ref, (i, st, c, ref)
+        if isinstance(tree, int):
+            assert st == A.OK and c == tree, (i, st, c, tree)
+        if tree == "overflow":
+            assert st != A.OK, i
+        if st == A.OK:
+            exact += 1
+            assert ref is not None or isinstance(tree, int), ("exact count without a CPU confirmation", i, c)
+        overflow += st == A.ERR_OVERFLOW
+    assert exact >= 3 and overflow >= 30, (exact, overflow)
+
+
+def test_lower_bounds_against_the_oracle(c1):
+    dg, parity, qs, recs = c1
+    compared = 0
+    for i in parity:
+        ob = recs[i].get("oracle_bound")
+        if ob is None:
+            continue
+        cs = A.CandidateSpace(dg, qs[i])
+        lb, exceeds = cs.count_lower_bound()
+        cs.close()
+        if ob in ("none", "empty"):
+            assert lb == 0 and not exceeds, (i, lb)
+            continue
+        want = int(ob)
+        if want >= TWO64 * (1 + 1e-9):
+            assert exceeds and lb == TWO64 - 1, (i, lb, want)
+        elif want < TWO64 * (1 - 1e-9):
+            # the device rounds toward zero in doubles: at most the exact bound, within rounding
+            assert not exceeds and lb <= want and lb >= want * (1 - 1e-9), (i, lb, want)
+        compared += 1
+    assert compared >= 40
+
+
+def test_grouped_and_single_candidate_spaces_agree(c1):
+    """One group build (padded candidate-edge lists), the same group with the
+    padded-entry cap lowered to 2^20 (the counting two-scan form) and one build
+    per query give identical candidate spaces."""
+    dg, parity, qs, recs = c1
+    queries = [qs[i] for i in parity]
+    padded = A.candidate_spaces(dg, queries)
+    cap = dg.tuning()["padded_cap_log2"]
+    dg.set_tuning(dg.tuning()["enum_min_blocks"], dg.tuning()["lane_leaf_max"], padded_cap_log2=20)
+    try:
+        two_scan = A.candidate_spaces(dg, queries)
+    finally:
+        dg.set_tuning(dg.tuning()["enum_min_blocks"], dg.tuning()["lane_leaf_max"], padded_cap_log2=cap)
+    for i, a, b in zip(parity, padded, two_scan):
+        assert a is not None and b is not None
+        da, fa = a.digest()
+        db, fb = b.digest()
+        assert fa & A.CS_LABEL_RUNS and fb & A.CS_LABEL_RUNS
+        assert fb & A.CS_TWO_SCAN and not fa & A.CS_TWO_SCAN
+        one = A.CandidateSpace(dg, qs[i])
+        d1, _ = one.digest()
+        assert one.nonempty == a.nonempty == b.nonempty and da == db == d1, i
+        assert np.array_equal(one.sizes(), a.sizes()) and np.array_equal(one.edge_totals(), a.edge_totals())
+        for c in (one, a, b):
+            c.close()

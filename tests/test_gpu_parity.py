@@ -276,3 +276,21 @@ def test_batched_local_counts_agree_with_single_query_mode(golden, c0d_files, dg
         assert c == r["count"] == single.count
         assert np.array_equal(m, single.local_counts)
         assert all(int(x) == r["count"] for x in m.sum(axis=0, dtype=np.uint64))
+
+
+def test_orders_with_cartesian_vertices_give_the_golden_counts(golden, c0_files, dg_c0):
+    """Orders in which a vertex has no earlier neighbour (the reference planner's
+    Cartesian attributes) are accepted; the count does not depend on the order."""
+    _, _, qs, _ = c0_files
+    checked = 0
+    for rec in golden["sets"]["c0"][:60]:
+        q = qs[rec["index"]]
+        adj = [set(q.nbrs[q.offsets[u]:q.offsets[u + 1]].tolist()) for u in range(q.n)]
+        # start with two vertices that are not adjacent, the rest in reverse id order
+        pair = next(((a, b) for a in range(q.n) for b in range(q.n) if a != b and b not in adj[a]), None)
+        if pair is None:
+            continue
+        order = list(pair) + [u for u in reversed(range(q.n)) if u not in pair]
+        assert A.match(dg_c0, q, order=order).count == rec["count"], rec["index"]
+        checked += 1
+    assert checked >= 30
