@@ -122,6 +122,7 @@ _card_info = _sig("asdm_card_info", C.c_int, [_vp, _u32p, _u64p, C.POINTER(C.c_d
 _card_write = _sig("asdm_card_write", C.c_int, [_vp, C.c_char_p, C.c_double])
 _card_free = _sig("asdm_card_free", None, [_vp])
 _plan_create_card = _sig("asdm_plan_create_card", C.c_int, [_vp, _vp, C.POINTER(_vp)])
+_card_sample = _sig("asdm_card_sample", C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(_vp)])
 _gemm = _sig("asdm_gemm_bf16", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
                                          C.POINTER(C.c_float)])
 class BatchOpts(C.Structure):
@@ -494,6 +495,16 @@ class Card:
     def write(self, path: str, plan_seconds: float = 0.0):
         _check(_card_write(self._h, path.encode(), plan_seconds), path)
 
+    @classmethod
+    def sample(cls, cs: "CandidateSpace", max_subset: int = 0, walks: int = 0, seed: int = 0) -> "Card":
+        """Sampling estimates of the query's connected sub-queries of 3..max_subset
+        vertices, made on the device (asdm_card_sample)."""
+        h = _vp()
+        _check(_card_sample(cs._h, max_subset, walks, seed, C.byref(h)), "sample")
+        c = cls.__new__(cls)
+        c._h = h
+        return c
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value and _card_free is not None:  # module globals are gone at interpreter exit
@@ -695,6 +706,26 @@ def run_batch_ex(dg: DeviceGraph, b: BatchInput, time_limit_s: float = 0.0, coun
     if rc == ERR_CUDA:
         _check(rc, "batch")
     return st
+
+
+def run_batch_local_ex(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float = 0.0,
+                       query_time_limit_s: float = 0.0):
+    """Batched LOCAL_COUNT with per-query GPU-time budgets: (counts, status,
+    [|Vg| x |Vq_i| uint64 matrices], RunStats); a query's matrix is valid when
+    its status is OK."""
+    b = BatchInput(queries)
+    mats = [np.zeros((dg.n, q.n), np.uint64) for q in queries]
+    ptrs = (_u64p * max(1, len(mats)))(*[_ptr(m, _u64p) for m in mats])
+    opts = BatchOpts()
+    opts.time_limit_s = time_limit_s
+    opts.query_time_limit_s = query_time_limit_s
+    st = RunStats()
+    rc = _run_batch_ex(dg._h, b.nq, _ptr(b.sizes), _ptr(b.ob, _u64p), _ptr(b.offs), _ptr(b.nb, _u64p), _ptr(b.nbrs),
+                       _ptr(b.lb, _u64p), _ptr(b.labs), C.byref(opts), _ptr(b.counts, _u64p),
+                       b.status.ctypes.data_as(C.POINTER(C.c_int)), ptrs, C.byref(st))
+    if rc == ERR_CUDA:
+        _check(rc, "batch")
+    return b.counts.copy(), b.status.copy(), mats, st
 
 
 def candidate_spaces(dg: DeviceGraph, queries: Sequence[HostGraph], b: Optional[BatchInput] = None):

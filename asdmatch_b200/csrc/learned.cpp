@@ -22,8 +22,13 @@
 namespace asdm {
 
 int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, const asdm_card *card = nullptr);
+int sample_subsets(asdm_cs &cs, const std::vector<uint64_t> &subsets, uint32_t walks, uint64_t seed,
+                   std::vector<double> &est);
 
 namespace {
+
+// Walks per subset when the sampling estimator stands in for a dropped prediction.
+constexpr uint32_t kFallbackWalks = 256;
 
 constexpr uint32_t kF = ASDM_EST_FEATURES;
 constexpr uint32_t kLabelBuckets = 32;
@@ -264,10 +269,18 @@ int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uin
     for (uint32_t i : dp_ids) {
         // a prediction outside the possible range (more partial matches than
         // the product of the subset's candidate-set sizes, or not finite) is
-        // dropped: the planner's own estimate stands in for it
+        // dropped: the sampling estimator's estimate stands in for it
         std::unordered_map<uint64_t, double> known;
-        for (size_t r = range[i].first; r < range[i].second; ++r)
+        std::vector<uint64_t> dropped;
+        for (size_t r = range[i].first; r < range[i].second; ++r) {
             if (in_range(*css[i], rm[r], est[r])) known.emplace(rm[r], est[r]);
+            else dropped.push_back(rm[r]);
+        }
+        if (!dropped.empty()) {
+            std::vector<double> sampled;
+            ASDM_TRY(sample_subsets(*css[i], dropped, kFallbackWalks, i, sampled));
+            for (size_t k = 0; k < dropped.size(); ++k) known.emplace(dropped[k], sampled[k]);
+        }
         std::vector<uint32_t> order;
         double cost = 0;
         const bool ok = plan_dp(*css[i], [&](uint64_t S, double &c) {

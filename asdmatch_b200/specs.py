@@ -11,7 +11,7 @@ file by path and runs the host-only generator asdmatch_b200/bin/asdm_gen.out.
 * C2  — the C1 graph with the mixed batch: query i has seed C2_QUERY_SEED + i
         and a size uniform in 4..32 (c2_size).
 * C1 queries — 100 queries each of 12 and 16 vertices on the C1 graph, half
-        dense (average query degree >= 3) and half sparse (< 3): c1_query_specs.
+        dense (average query degree >= 3) and half sparse (< 3): c1_seed_base.
 * C4  — local subgraph counting: N=1.0M, M=10M, exponent 2.3, 32 labels
         Zipf(1.0), 50 random-walk queries of 10 vertices: c4_query_specs.
 """
@@ -38,15 +38,15 @@ def c2_seed_size(i):
     return seed, 4 + (seed * 2654435761 % 2 ** 32) % 29
 
 
-def c1_query_specs():
-    """(size, seed, density) of the config-1 queries: for 12 and 16 vertices,
-    50 dense then 50 sparse."""
-    out = []
-    for size in (12, 16):
-        for density in (DENSE, SPARSE):
-            for i in range(50):
-                out.append((size, C1_QUERY_SEED + 1000 * size + 100 * density + i, density))
-    return out
+def c1_seed_base(size, density):
+    """First walk seed tried for the config-1 queries of one size and density;
+    the queries are the first 50 seeds from there whose walk yields a query of
+    that density (a dense walk is not found from every seed)."""
+    return C1_QUERY_SEED + 10_000 * size + 1_000 * density
+
+
+C1_SIZES = (12, 16)
+C1_PER_CLASS = 50
 
 
 def c4_query_specs():

@@ -10,9 +10,10 @@ machine rebuilds identical graphs and queries from the seeds.
         Patents), resident in HBM.
 * C2  — the C1 graph with the mixed batch: the first 1,000 random-walk queries
         in seed order, sizes uniform in 4..32 (``c2_batch``), none screened out.
+* C1 queries — 100 each of 12 and 16 vertices, half dense, half sparse
+        (``c1_batch``).
 * C4  — local subgraph counting: N=1.0M, M=10M, exponent 2.3, 32 labels
-        Zipf(1.0).  No 10-vertex random-walk query of 1,500 tried has <= 10^9
-        matches, so ``screen_c4`` keeps 8-vertex ones (``c4_screened.json``).
+        Zipf(1.0), 50 random-walk queries of 10 vertices (``c4_batch``).
 """
 from __future__ import annotations
 
@@ -21,11 +22,10 @@ import os
 
 import asdmatch_b200 as A
 
-from asdmatch_b200.specs import (C0, C0_QUERY_SEED, C0D, C0D_QUERY_SEED, C1, C2_QUERIES, C2_QUERY_SEED, C4,  # noqa: F401
-                                  C4_QUERY_SEED, c1_query_specs, c2_seed_size, c4_query_specs)
+from asdmatch_b200.specs import (C0, C0_QUERY_SEED, C0D, C0D_QUERY_SEED, C1, C1_PER_CLASS, C1_SIZES,  # noqa: F401
+                                  C2_QUERIES, C2_QUERY_SEED, C4, C4_QUERY_SEED, DENSE, SPARSE, c1_seed_base,
+                                  c2_seed_size, c4_query_specs)
 
-C2_COUNT_LIMIT = 10 ** 9
-C4_SCREEN_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "c4_screened.json")
 
 
 def graph(spec):
@@ -67,66 +67,25 @@ def from_specs(g, specs):
 
 
 def c1_batch(g):
-    """The config-1 queries: 100 each of 12 and 16 vertices, half dense, half sparse."""
-    return from_specs(g, c1_query_specs())
+    """The config-1 queries: 100 each of 12 and 16 vertices, half dense, half
+    sparse, as (size, density, seed, query) in that order."""
+    out = []
+    for size in C1_SIZES:
+        for density in (DENSE, SPARSE):
+            seed = c1_seed_base(size, density)
+            found = 0
+            while found < C1_PER_CLASS:
+                try:
+                    q = g.random_walk_query(size, seed, density)
+                    out.append((size, density, seed, q))
+                    found += 1
+                except A.AsdmError as e:
+                    if e.code != A.ERR_INVALID:
+                        raise
+                seed += 1
+    return out
 
 
 def c4_batch(g):
     """The config-4 queries: 50 random-walk queries of 10 vertices."""
     return from_specs(g, c4_query_specs())
-
-
-def c4_candidate(g, i, size=10):
-    """The i-th candidate query of the config-4 set: (seed, size, query)."""
-    seed = C4_QUERY_SEED + i
-    return seed, size, g.random_walk_query(size, seed, 0)
-
-
-def screen_c4(dg, g, keep=50, size=8, count_limit=C2_COUNT_LIMIT, time_limit_s=2.0, max_candidates=4000, log=None):
-    """Config-4 queries in seed order whose exact count is <= count_limit."""
-    kept, rejected = [], 0
-    for i in range(max_candidates):
-        if len(kept) >= keep:
-            break
-        seed, sz, q = c4_candidate(g, i, size)
-        try:
-            r = A.count_query(dg, q, time_limit_s=time_limit_s, count_limit=count_limit)
-            kept.append(dict(index=i, seed=seed, size=sz, edges=q.m2 // 2, count=r.count))
-        except A.AsdmError as e:
-            if e.code not in (A.ERR_LIMIT, A.ERR_TIMEOUT, A.ERR_OVERFLOW):
-                raise
-            rejected += 1
-        if log and (i + 1) % 250 == 0:
-            log("c4 screened %d kept %d" % (i + 1, len(kept)))
-    return dict(spec=C4, query_seed=C4_QUERY_SEED, size=size, count_limit=count_limit, time_limit_s=time_limit_s,
-                candidates=len(kept) + rejected, rejected=rejected, queries=kept)
-
-
-def load_c4_screen():
-    with open(C4_SCREEN_FILE) as fh:
-        return json.load(fh)
-
-
-def c4_queries(g, screen_data):
-    out = []
-    for rec in screen_data["queries"]:
-        seed, size, q = c4_candidate(g, rec["index"], screen_data["size"])
-        assert seed == rec["seed"]
-        out.append(q)
-    return out
-
-
-if __name__ == "__main__":
-    # python -m asdmatch_b200.workloads c4 [keep] [out] [size]: the config-4 local-counting screen
-    import sys
-    import time
-    t = time.time()
-    keep = int(sys.argv[2]) if len(sys.argv) > 2 else 50
-    g = graph(C4)
-    dg = A.DeviceGraph(g)
-    size = int(sys.argv[4]) if len(sys.argv) > 4 else 8
-    data = screen_c4(dg, g, keep=keep, size=size, log=print)
-    out = sys.argv[3] if len(sys.argv) > 3 else C4_SCREEN_FILE
-    with open(out, "w") as fh:
-        json.dump(data, fh, indent=0)
-    print("screen done in %.1f s: kept %d of %d" % (time.time() - t, len(data["queries"]), data["candidates"]))

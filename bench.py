@@ -64,13 +64,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c0"])
-    ap.add_argument("--query-cap", type=float, default=0.05,
+    ap.add_argument("--query-cap", type=float, default=0.02,
                     help="GPU seconds of enumeration one query may use (its time alone on the GPU)")
     ap.add_argument("--ref-cap", type=float, default=10.0, help="seconds one reference process may run")
     ap.add_argument("--cpu-sample", type=int, default=0, help="queries in the CPU-baseline sample (0: the host's cores)")
     ap.add_argument("--queries", type=int, default=0, help="use only the first K queries (profiling runs)")
     ap.add_argument("--profile", action="store_true", help="timed steps only: no other forms, no CPU baseline")
-    ap.add_argument("--no-c4", action="store_true", help="skip the config-4 local-counting measurement")
+    ap.add_argument("--no-c4", action="store_true", help="skip the config-1 and config-4 measurements")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel knobs (profiling runs)")
     ap.add_argument("--estimator", default="", help="learned-estimator parameters (.npy); default: the trained "
                                                     "config-1 model shipped with the package, when present")
@@ -192,9 +192,9 @@ class Checker:
         self.overflow = set()
         self.confirmed = set()          # answered and equal to a reference count
 
-    def check(self, what, counts, status):
+    def check(self, what, counts, status, positions=None):
         for pos, (c, st) in enumerate(zip(counts, status)):
-            i = self.indices[pos]
+            i = self.indices[pos if positions is None else positions[pos]]
             g = self.golden.get(i)
             st = int(st)
             if st == OK:
@@ -414,19 +414,22 @@ def main():
                 "cs_bytes": st.build_bytes, "matches": int(batch.counts[batch.status == OK].sum(dtype=np.uint64)),
                 "inter": st.intersections, "status": histogram(int(x) for x in batch.status)}
 
-    def plain_step():
-        """The plain form: one query per launch sequence (candidate space, plan, count), same cap."""
-        counts = np.zeros(Q, np.uint64)
-        status = np.zeros(Q, np.int32)
+    def plain_step(positions=None):
+        """The plain form: one query per launch sequence (candidate space, sampling
+        estimates, plan, count), same cap; over the batch positions given (all)."""
+        positions = list(range(Q)) if positions is None else positions
+        counts = np.zeros(len(positions), np.uint64)
+        status = np.zeros(len(positions), np.int32)
         agg = {"kernel_ms": 0.0, "list_bytes": 0, "cs_ms": 0.0, "cs_bytes": 0, "inter": 0}
-        for k, q in enumerate(qs):
+        for k, q in enumerate(qs[p] for p in positions):
             cs = A.CandidateSpace(dg, q)
             b, ms_ = cs.build_stats()
             agg["cs_bytes"] += b
             agg["cs_ms"] += ms_
             if cs.nonempty:
                 try:
-                    r = A.adaptive_share_join(cs, time_limit_s=cap)
+                    plan = A.Plan(cs, card=A.Card.sample(cs, seed=k))
+                    r = A.adaptive_share_join(cs, plan, time_limit_s=cap)
                     counts[k] = r.count
                     agg["kernel_ms"] += r.kernel_ms
                     agg["list_bytes"] += r.list_bytes
@@ -436,7 +439,7 @@ def main():
                         raise
                     status[k] = e.code
             cs.close()
-        checker.check("plain", counts, status)
+        checker.check("plain", counts, status, positions)
         agg["matches"] = int(counts[status == OK].sum(dtype=np.uint64))
         agg["status"] = histogram(int(x) for x in status)
         return agg
@@ -460,7 +463,8 @@ def main():
 
     # warm-up (first step also picks the queries the tuner times: those counted exactly)
     first = batched_step()
-    exact = [q for q, s in zip(qs, packed.status.tolist()) if s == OK]
+    first_status = packed.status.tolist()
+    exact = [q for q, s in zip(qs, first_status) if s == OK]
     if args.no_tune or not exact:
         tune_best, tune_table = dg.tuning(), []
     else:
@@ -478,6 +482,8 @@ def main():
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": ms, "queries": Q, "status": agg["status"],
+                              "enum_kernel_ms_per_step": agg["kernel_ms"] / args.steps,
+                              "cs_build_ms_per_step": agg["cs_ms"] / args.steps,
                               "launches": launches // args.steps}))
         if world > 1:
             dist.destroy_process_group()
@@ -507,6 +513,29 @@ def main():
                    "what": "asdm_run_batch_ex with the learned estimator: candidate spaces, learned plans (one "
                            "forward pass per planner step for the whole group), one persistent launch; planning is "
                            "inside the timed region"}
+    # the same forms on the queries the first step decided (exact count or proven overflow): timeouts,
+    # which cost their cap in every form, left out
+    decided_pos = [p for p, s in enumerate(first_status) if s in (OK, OVERFLOW)]
+    decided = None
+    if decided_pos:
+        dbatch = A.BatchInput([qs[p] for p in decided_pos])
+
+        def decided_batched(estimator=None, what="batched-decided"):
+            st = A.run_batch_ex(dg, dbatch, estimator=estimator, learned_max_subset=args.learned_max,
+                                query_time_limit_s=cap)
+            checker.check(what, dbatch.counts, dbatch.status, decided_pos)
+            return {"status": histogram(int(x) for x in dbatch.status)}
+
+        decided_batched()
+        d_ms, d_agg = timed(decided_batched, args.steps)
+        d_plain_ms, _ = timed(lambda: plain_step(decided_pos), args.steps)
+        decided = {"queries": len(decided_pos), "batched_ms": d_ms, "plain_ms": d_plain_ms,
+                   "batched_queries_per_s": world * len(decided_pos) / (d_ms / 1e3),
+                   "batched_over_plain": d_plain_ms / d_ms,
+                   "status": {STATUS_NAME.get(k, k): v for k, v in d_agg["status"].items()}}
+        if est is not None:
+            d_learned_ms, _ = timed(lambda: decided_batched(est, "learned-decided"), args.steps)
+            decided.update(learned_ms=d_learned_ms, learned_over_plain=d_plain_ms / d_learned_ms)
     # end to end through the C ABI (asdm_run_batch_ex) from host arrays, same cold-L2 protocol
     e2e_times = []
     h2d = packed.nbytes()
@@ -572,9 +601,11 @@ def main():
                                    "status": {STATUS_NAME.get(k, k): v for k, v in plain_agg["status"].items()},
                                    "enum_kernel_ms_per_step": plain_agg["kernel_ms"] / steps,
                                    "cs_build_ms_per_step": plain_agg["cs_ms"] / steps,
-                                   "what": "one query per launch sequence (asdm_candidate_space, asdm_plan_create, "
-                                           "asdm_run_plan with the same cap as a time limit)"},
+                                   "what": "one query per launch sequence (asdm_candidate_space, asdm_card_sample: "
+                                           "the sampling estimator, asdm_plan_create_card, asdm_run_plan with the "
+                                           "same cap as a time limit)"},
                        batched_over_plain=plain_ms / ms,
+                       decided_subset=decided,
                        cs_build_roofline={"kernels": "K1-K3 (k1_filter, k2_pull, compaction, k3_bound/flat/pack)",
                                           "bound": "hbm", "achieved": cs_achieved, "peak": peak, "unit": "GB/s",
                                           "frac": cs_achieved / peak, "algorithmic_bytes_per_step": cs_bytes,
@@ -591,8 +622,9 @@ def main():
         "gpu_launches": launches // steps,
         "clocks": clocks,
     }
-    if world == 1 and not args.no_c4 and os.path.exists(W.C4_SCREEN_FILE):
-        line["config"]["local_counting_c4"] = measure_c4(A, W, torch, dev, args.steps)
+    if world == 1 and not args.no_c4 and args.workload == "c2":
+        line["config"]["config1"] = measure_c1(A, W, g, dg, torch, dev, args.steps, cap)
+        line["config"]["local_counting_c4"] = measure_c4(A, W, torch, dev, args.steps, cap)
     if world == 1 and args.workload == "c2":
         tmp = tempfile.mkdtemp(prefix="asdm_cpu_")
         n = args.cpu_sample or (os.cpu_count() or 1)
@@ -604,40 +636,119 @@ def main():
         dist.destroy_process_group()
 
 
-def measure_c4(A, W, torch, dev, steps):
-    """Config 4: the screened 8-vertex queries on the 1M/10M graph, batched LOCAL_COUNT
-    (asdm_run_batch_local); checked every step (counts, and every local-count column sums
-    to the count)."""
+def csv_sha256(mat):
+    """SHA-256 of a local-count matrix written the way the reference writes its
+    CSV (main.cpp:135-146): one row per data vertex, ',' between columns."""
+    import hashlib
+    h = hashlib.sha256()
+    for r0 in range(0, mat.shape[0], 65536):
+        block = mat[r0:r0 + 65536]
+        h.update(("\n".join(",".join(map(str, row)) for row in block.tolist()) + "\n").encode())
+    return h.hexdigest()
+
+
+def measure_c1(A, W, g, dg, torch, dev, steps, cap):
+    """Config 1: 100 queries each of 12 and 16 vertices (half dense, half sparse)
+    on the resident config-1 graph, batched with the per-query cap; per-query
+    wall times from the plain form (one query per launch sequence)."""
     import numpy as np
-    g = W.graph(W.C4)
-    sc = W.load_c4_screen()
-    qs = W.c4_queries(g, sc)
-    want = [r["count"] for r in sc["queries"]]
-    dg = A.DeviceGraph(g)
+    batch = W.c1_batch(g)
+    qs = [q for _, _, _, q in batch]
+    classes = ["%d-%s" % (size, "dense" if d == W.DENSE else "sparse") for size, d, _, _ in batch]
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
-    A.run_batch_local(dg, qs)  # warm
+    b = A.BatchInput(qs)
+    A.run_batch_ex(dg, b, query_time_limit_s=cap)  # warm
     times = []
     for _ in range(steps):
         flush_l2(torch, dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        counts, status, mats = A.run_batch_local(dg, qs)
+        A.run_batch_ex(dg, b, query_time_limit_s=cap)
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
-        if counts.tolist() != want or status.any():
-            raise SystemExit("config-4 counts differ from the screened counts")
-        for c, m in zip(want, mats):
+    by_class = {}
+    for c, st in zip(classes, b.status.tolist()):
+        by_class.setdefault(c, {})
+        k = STATUS_NAME.get(st, st)
+        by_class[c][k] = by_class[c].get(k, 0) + 1
+    walls = []
+    for q, st in zip(qs, b.status.tolist()):
+        t0 = time.perf_counter()
+        cs = A.CandidateSpace(dg, q)
+        try:
+            if cs.nonempty:
+                A.adaptive_share_join(cs, time_limit_s=cap)
+        except A.AsdmError as e:
+            if e.code not in (OVERFLOW, TIMEOUT):
+                raise
+        cs.close()
+        walls.append(time.perf_counter() - t0)
+    walls.sort()
+    ms = statistics.mean(times)
+    return {"workload": "config 1: config-1 graph; 100 random-walk queries each of 12 and 16 vertices, half dense "
+                        "(average degree >= 3), half sparse; per-query cap %.3g s of GPU time (the reference's is "
+                        "300 s of CPU)" % cap,
+            "queries_per_s": len(qs) / (ms / 1e3), "ms_per_step": ms, "status_by_class": by_class,
+            "plain_per_query_wall_s": {"median": walls[len(walls) // 2], "p90": walls[int(0.9 * len(walls))],
+                                       "max": walls[-1]},
+            "via": "asdm_run_batch_ex (batched); per-query walls: asdm_candidate_space + asdm_run_plan with the cap "
+                   "as time limit"}
+
+
+def measure_c4(A, W, torch, dev, steps, cap):
+    """Config 4: 50 random-walk queries of 10 vertices on the 1M/10M graph,
+    batched LOCAL_COUNT with the per-query cap; every finished query's
+    |Vg| x |Vq| matrix sums to its count in every column, and its CSV digest
+    equals the reference's where the reference finished
+    (tests/golden/c4_batch.json)."""
+    import numpy as np
+    g = W.graph(W.C4)
+    qs = W.c4_batch(g)
+    golden = {}
+    gp = os.path.join(ROOT, "tests", "golden", "c4_batch.json")
+    if os.path.exists(gp):
+        with open(gp) as fh:
+            golden = {r["index"]: r for r in json.load(fh)["queries"]}
+    dg = A.DeviceGraph(g)
+    stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
+    counts, status, mats, _ = A.run_batch_local_ex(dg, qs, query_time_limit_s=cap)  # warm
+    first = (counts.copy(), status.copy())
+    confirmed = 0
+    for k, (c, st, m) in enumerate(zip(counts.tolist(), status.tolist(), mats)):
+        r = golden.get(k)
+        if st == OK:
             if any(int(x) != c for x in m.sum(axis=0, dtype=np.uint64)):
-                raise SystemExit("config-4 local counts do not sum to the count")
+                raise SystemExit("config-4 query %d: local counts do not sum to the count" % k)
+            if r is not None and r.get("count") is not None:
+                if r["count"] != c or r.get("csv_sha256") != csv_sha256(m):
+                    raise SystemExit("config-4 query %d differs from the reference" % k)
+                confirmed += 1
+        elif st not in (OVERFLOW, TIMEOUT):
+            raise SystemExit("config-4 query %d failed with status %d" % (k, st))
+        elif r is not None and r.get("count") is not None and st == OVERFLOW:
+            raise SystemExit("config-4 query %d: overflow, but the reference finished" % k)
+    times = []
+    for _ in range(steps):
+        flush_l2(torch, dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        counts, status, mats, _ = A.run_batch_local_ex(dg, qs, query_time_limit_s=cap)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        ok = (status == OK) & (first[1] == OK)
+        if not np.array_equal(counts[ok], first[0][ok]):
+            raise SystemExit("config-4 counts changed between steps")
     ms = statistics.mean(times)
     dg.close()
-    return {"workload": "c4-screened: Chung-Lu N=1.0M M=10M gamma=2.3, 32 labels Zipf(1.0); %d random-walk queries "
-                        "of %d vertices with <= 1e9 matches (%d of %d candidates; no 10-vertex query qualified)"
-                        % (len(qs), sc["size"], len(qs), sc["candidates"]),
-            "queries_per_s": len(qs) / (ms / 1e3), "ms_per_step": ms, "matches_per_step": int(sum(want)),
-            "local_count_bytes_per_step": 8 * g.n * sum(q.n for q in qs),
-            "via": "asdm_run_batch_local, |Vg| x |Vq| uint64 matrices copied to host every step"}
+    return {"workload": "config 4: Chung-Lu N=1.0M M=10M gamma=2.3, 32 labels Zipf(1.0); 50 random-walk queries of "
+                        "10 vertices, LOCAL_COUNT; per-query cap %.3g s of GPU time" % cap,
+            "queries_per_s": len(qs) / (ms / 1e3), "ms_per_step": ms,
+            "status": {STATUS_NAME.get(k, k): v for k, v in histogram(int(x) for x in status).items()},
+            "csv_equal_to_reference": confirmed,
+            "local_count_bytes_per_step": 8 * g.n * sum(q.n for q, st in zip(qs, status.tolist()) if st == OK),
+            "via": "asdm_run_batch_ex with local-count matrices (|Vg| x |Vq| uint64, copied to host every step)"}
 
 
 if __name__ == "__main__":

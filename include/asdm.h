@@ -217,6 +217,15 @@ int asdm_card_info(const asdm_card *c, uint32_t *bags, uint64_t *entries, double
 /* Writes the map (values truncated to two decimals like saveSubsetToCard) and
  * the planning time, with no bag records. */
 int asdm_card_write(const asdm_card *c, const char *path, double plan_seconds);
+/* A cache filled with sampling estimates, made on the device: for every
+ * connected induced sub-query of 3..max_subset vertices (0 = 6; fewer when
+ * there are more than 4,096 such subsets), the mean weight of `walks` random
+ * walks (0 = 512) through the candidate space along a connected order, each
+ * walk multiplying the sizes of the candidate sets it meets and moving to a
+ * uniformly drawn member (an unbiased estimate of the partial-match count).
+ * Replaces cardEstimateLabeled (plan/estimator.cpp:173-291), the reference's
+ * sampling estimator, as the input of the card-guided planner. */
+int asdm_card_sample(asdm_cs *cs, uint32_t max_subset, uint32_t walks, uint64_t seed, asdm_card **out);
 void asdm_card_free(asdm_card *c);
 int asdm_plan_free(asdm_plan *p);
 

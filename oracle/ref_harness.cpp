@@ -28,6 +28,7 @@
 //      at a time, each killed after s seconds.  One line per query on
 //      stdout: "Q <k> ok|timeout|signal <n>|exit <n> <wall seconds>".  Every
 //      child starts from the same untouched state, as a fresh process would.
+//      With -c (LOCAL_COUNT builds) each child writes its CSV to <dir>/q<k>.csv.
 // Build variants select the reference's compile-time modes (config/config.h:38-40):
 //   ref_count : ALL_LEVEL                          (exact counts)
 //   ref_local : ALL_LEVEL + LOCAL_COUNT            (+ |Vg|x|Vq| CSV via -c)
@@ -63,6 +64,9 @@ static std::string option_after(int argc, char **argv, const char *flag) {
 static double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// In list mode with -c, each child's CSV path (<dir>/q<k>.csv).
+static std::string g_csv_path;
 
 // One query against the loaded data graph g: the reference's ASDMatch.out
 // sequence after its graph loads (main.cpp:27-147).
@@ -176,7 +180,7 @@ static int run_query(int argc, char **argv, Command &cmd, const std::string &qpa
     std::cout << "Number of intersections: " << gNumInterSection << std::endl;
 
 #ifdef LOCAL_COUNT
-    const std::string csvPath = cmd.getCountPath();
+    const std::string csvPath = g_csv_path.empty() ? cmd.getCountPath() : g_csv_path;
     if (!csvPath.empty()) {
         std::ofstream os(csvPath);
         for (VertexID v = 0; v < g.getNumVertices(); ++v) {
@@ -226,6 +230,7 @@ static int run_list(int argc, char **argv, Command &cmd, Graph &g, const std::st
             if (pid == 0) {
                 const std::string out = outDir + "/q" + std::to_string(next) + ".out";
                 if (!std::freopen(out.c_str(), "w", stdout)) _exit(3);
+                if (!cmd.getCountPath().empty()) g_csv_path = outDir + "/q" + std::to_string(next) + ".csv";
                 const int rc = run_query(argc, argv, cmd, queries[next], g);
                 std::cout.flush();
                 std::fflush(stdout);

@@ -34,8 +34,6 @@ TWO64 = 1 << 64
 def c1():
     with open(GOLDEN) as fh:
         data = json.load(fh)
-    if "parity" not in data:
-        pytest.skip("no parity set in c2_batch.json")
     recs = {r["index"]: r for r in data["queries"]}
     g = W.graph(W.C1)
     dg = A.DeviceGraph(g)
