@@ -123,6 +123,8 @@ _card_write = _sig("asdm_card_write", C.c_int, [_vp, C.c_char_p, C.c_double])
 _card_free = _sig("asdm_card_free", None, [_vp])
 _plan_create_card = _sig("asdm_plan_create_card", C.c_int, [_vp, _vp, C.POINTER(_vp)])
 _card_sample = _sig("asdm_card_sample", C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(_vp)])
+_sample_subsets = _sig("asdm_sample_subsets", C.c_int, [_vp, C.c_uint32, _u64p, C.c_uint32, C.c_uint64,
+                                                        C.POINTER(C.c_double)])
 _gemm = _sig("asdm_gemm_bf16", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
                                          C.POINTER(C.c_float)])
 class BatchOpts(C.Structure):
@@ -370,6 +372,15 @@ class CandidateSpace:
         f = C.c_uint32()
         _check(_cs_digest(self._h, C.byref(d), C.byref(f)), "digest")
         return int(d.value), int(f.value)
+
+    def sample_cardinalities(self, masks: Sequence[int], walks: int = 0, seed: int = 0) -> np.ndarray:
+        """Sampling estimates of the partial-match counts of connected vertex
+        subsets (asdm_sample_subsets)."""
+        m = np.ascontiguousarray(masks, dtype=np.uint64)
+        out = np.zeros(max(len(m), 1), np.float64)
+        _check(_sample_subsets(self._h, len(m), _ptr(m, _u64p), walks, seed,
+                               out.ctypes.data_as(C.POINTER(C.c_double))), "sample")
+        return out[:len(m)]
 
     def count_lower_bound(self):
         """(bound, exceeds): a lower bound of the embedding count (capped at

@@ -261,6 +261,22 @@ int sample_subsets(asdm_cs &cs, const std::vector<uint64_t> &subsets, uint32_t w
 
 using namespace asdm;
 
+extern "C" int asdm_sample_subsets(asdm_cs *cs, uint32_t nsub, const uint64_t *masks, uint32_t walks, uint64_t seed,
+                                   double *est) {
+    clear_error();
+    if (!cs || (nsub && (!masks || !est))) return fail(ASDM_ERR_INVALID, "null argument");
+    for (uint32_t i = 0; i < nsub; ++i) {
+        est[i] = 0.0;
+        if (masks[i] == 0 || (cs->q.n < 64 && (masks[i] >> cs->q.n) != 0))
+            return fail(ASDM_ERR_INVALID, "subset %u names a vertex outside the query", i);
+    }
+    if (!cs->nonempty || nsub == 0) return ASDM_OK;
+    std::vector<double> out;
+    ASDM_TRY(sample_subsets(*cs, std::vector<uint64_t>(masks, masks + nsub), walks ? walks : 512, seed, out));
+    std::copy(out.begin(), out.end(), est);
+    return ASDM_OK;
+}
+
 extern "C" int asdm_card_sample(asdm_cs *cs, uint32_t max_subset, uint32_t walks, uint64_t seed, asdm_card **out) {
     clear_error();
     if (!cs || !out) return fail(ASDM_ERR_INVALID, "null argument");

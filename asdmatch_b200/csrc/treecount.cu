@@ -360,8 +360,11 @@ uint64_t term_cost(const BlockTree &t, const asdm_cs &c) {
 // Every term of a tree query's count; false when the query does not qualify
 // (not a tree, a quotient with a cycle, too many partitions).  With a built
 // candidate space each term is rooted where its program reads the fewest
-// list entries.
-bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out, const asdm_cs *cs = nullptr) {
+// list entries.  With classes (cls[u]: u's class, or kNone when u may take
+// any candidate), vertices of different classes never share a block: they
+// can never share a data vertex.
+bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out, const asdm_cs *cs = nullptr,
+                 const std::vector<uint32_t> *cls = nullptr) {
     out.clear();
     if (q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) return false;
     std::vector<uint32_t> block(q.n, kNone);
@@ -402,7 +405,9 @@ bool block_trees(const QueryGraph &q, std::vector<BlockTree> &out, const asdm_cs
         for (uint32_t b = 0; b < members.size() && ok; ++b) {
             if (q.lab[members[b][0]] != q.lab[u]) continue;
             bool adj = false;
-            for (uint32_t w : members[b]) adj = adj || q.slot(u, w) >= 0;
+            for (uint32_t w : members[b])
+                adj = adj || q.slot(u, w) >= 0 ||
+                      (cls && (*cls)[u] != kNone && (*cls)[w] != kNone && (*cls)[u] != (*cls)[w]);
             if (adj) continue;
             members[b].push_back(u);
             block[u] = b;
@@ -793,26 +798,33 @@ __device__ __forceinline__ uint32_t vertex_class(uint32_t v, uint32_t k) {
     return (uint32_t)((((unsigned long long)v * 0x9E3779B97F4A7C15ull) >> 32) % k);
 }
 
-// A query vertex of a lower-bound program: its weights over C(u).
+// A query vertex (or block of same-label vertices) of a lower-bound program:
+// its weights over C(rep), rounded toward zero, or up (up = 1) where the
+// program's result enters a bound with a negative sign.
 struct BoundSeg {
     double *w;
-    const uint32_t *cand;       // C(u), for the class test
+    const uint32_t *cand;       // C(rep), for the class test
     uint32_t ncand, cls_k, cls_c;
-    uint32_t child_first, nchild, pad;
+    uint32_t child_first, nchild, up;
+    uint32_t val_first, nval;   // maps C(rep) -> C(member) of the block's other members
     unsigned long long start;   // first item of this segment in the launch
 };
 
 struct BoundChild {
     const uint32_t *off, *list;  // candidate edges u -> c
     const double *w;             // c's weights, or null (every candidate of c weighs 1)
+    const uint32_t *src;         // map C(rep) -> C(u) when the edge leaves another member u (else null)
 };
 
+__device__ __forceinline__ double dadd(double a, double b, bool up) { return up ? __dadd_ru(a, b) : __dadd_rz(a, b); }
+__device__ __forceinline__ double dmul(double a, double b, bool up) { return up ? __dmul_ru(a, b) : __dmul_rz(a, b); }
+
 // One thread per candidate of the level's segments:
-//   w_u(i) = [C(u)[i] has u's class] * prod over children c of
-//            sum over j in list_{u->c}(i) of w_c(j),
-// rounded toward zero; lists longer than 32 entries are summed by the warp.
+//   w_u(i) = [C(u)[i] has u's class and is a candidate of every member] *
+//            prod over children c of sum over j in list_{u->c}(i) of w_c(j),
+// rounded toward zero (or up); lists longer than 32 entries are summed by the warp.
 __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, unsigned long long total,
-                            const BoundChild *__restrict__ kids) {
+                            const BoundChild *__restrict__ kids, const uint32_t *const *__restrict__ maps) {
     const uint32_t lane = threadIdx.x & 31;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total;
@@ -831,7 +843,9 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
             sg = segs[lo];
             i = (uint32_t)(t - sg.start);
             if (sg.cls_k > 1) alive = vertex_class(sg.cand[i], sg.cls_k) == sg.cls_c;
+            for (uint32_t k = 0; k < sg.nval && alive; ++k) alive = maps[sg.val_first + k][i] != kNone;
         }
+        const bool up = sg.up != 0;
         double acc = alive ? 1.0 : 0.0;
         uint32_t maxk = alive ? sg.nchild : 0;
 #pragma unroll
@@ -843,8 +857,9 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
             const uint32_t *list = nullptr;
             if (mine) {
                 const BoundChild ch = kids[sg.child_first + k];
-                b = ch.off[i];
-                e = ch.off[i + 1];
+                const uint32_t iu = ch.src ? ch.src[i] : i;
+                b = ch.off[iu];
+                e = ch.off[iu + 1];
                 w = ch.w;
                 list = ch.list;
             }
@@ -857,15 +872,16 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
                 const uint32_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
                 const double *ww = (const double *)__shfl_sync(0xffffffffu, (unsigned long long)w, src);
                 const uint32_t *ll = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)list, src);
+                const bool uu = __shfl_sync(0xffffffffu, (uint32_t)up, src) != 0;
                 double part = 0.0;
-                for (uint32_t x = bb + lane; x < ee; x += 32) part = __dadd_rz(part, ww[ll[x]]);
+                for (uint32_t x = bb + lane; x < ee; x += 32) part = dadd(part, ww[ll[x]], uu);
 #pragma unroll
-                for (int o = 16; o; o >>= 1) part = __dadd_rz(part, __shfl_xor_sync(0xffffffffu, part, o));
+                for (int o = 16; o; o >>= 1) part = dadd(part, __shfl_xor_sync(0xffffffffu, part, o), uu);
                 if ((int)lane == src) sum = part;
             }
             if (mine && w && !coop)
-                for (uint32_t x = b; x < e; ++x) sum = __dadd_rz(sum, w[list[x]]);
-            if (mine) acc = __dmul_rz(acc, sum);
+                for (uint32_t x = b; x < e; ++x) sum = dadd(sum, w[list[x]], up);
+            if (mine) acc = dmul(acc, sum, up);
         }
         if (valid) sg.w[i] = acc;
     }
@@ -877,7 +893,7 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
 struct BoundQuery {
     const double *const *roots;  // root weight arrays of the components
     const uint32_t *nroot;       // their lengths
-    uint32_t ncomp, nhub, nedge, pad;
+    uint32_t ncomp, nhub, nedge, up;  // up = 1: sums and products rounded up (else toward zero)
     const uint32_t *hub;         // chosen hub indices of the fixed vertices
     const uint32_t *edge_ok;     // checks of the edges inside F
     double *out;
@@ -885,6 +901,7 @@ struct BoundQuery {
 
 __global__ void bound_queries(const BoundQuery *__restrict__ qs) {
     const BoundQuery bq = qs[blockIdx.x];
+    const bool up = bq.up != 0;
     __shared__ double red[32];
     __shared__ double prod;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) / 32;
@@ -897,35 +914,63 @@ __global__ void bound_queries(const BoundQuery *__restrict__ qs) {
     for (uint32_t c = 0; c < bq.ncomp; ++c) {
         double part = 0.0;
         const double *w = bq.roots[c];
-        for (uint32_t i = threadIdx.x; i < bq.nroot[c]; i += blockDim.x) part = __dadd_rz(part, w[i]);
+        for (uint32_t i = threadIdx.x; i < bq.nroot[c]; i += blockDim.x) part = dadd(part, w[i], up);
 #pragma unroll
-        for (int o = 16; o; o >>= 1) part = __dadd_rz(part, __shfl_xor_sync(0xffffffffu, part, o));
+        for (int o = 16; o; o >>= 1) part = dadd(part, __shfl_xor_sync(0xffffffffu, part, o), up);
         if (lane == 0) red[warp] = part;
         __syncthreads();
         if (threadIdx.x == 0) {
             double tot = 0.0;
-            for (uint32_t k = 0; k < nw; ++k) tot = __dadd_rz(tot, red[k]);
-            prod = __dmul_rz(prod, tot);
+            for (uint32_t k = 0; k < nw; ++k) tot = dadd(tot, red[k], up);
+            prod = dmul(prod, tot, up);
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) *bq.out = prod;
 }
 
+// The inclusion-exclusion sum of a query's terms, rounded down: terms with a
+// positive coefficient were computed rounding toward zero, the others
+// rounding up, so the result is at most the exact sum.  One thread per query.
+struct BoundSum {
+    const double *terms;
+    const double *coef;
+    uint32_t nterm, pad;
+    double *out;
+};
+
+__global__ void bound_sums(const BoundSum *__restrict__ sums, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BoundSum b = sums[i];
+    double acc = 0.0;
+    for (uint32_t t = 0; t < b.nterm; ++t) {
+        const double c = b.coef[t];
+        acc = c > 0 ? __dadd_rd(acc, __dmul_rd(c, b.terms[t])) : __dadd_rd(acc, -__dmul_ru(-c, b.terms[t]));
+    }
+    *b.out = acc;
+}
+
+constexpr uint32_t kHubRounds = 8;  // candidates tried for the first fixed vertex
+
 struct HubSeg {
     const uint32_t *cand;
-    uint32_t ncand, cls_k, cls_c, pad;
-    uint32_t *out;  // index in C(f) of the chosen candidate, or kNone
+    uint32_t ncand, cls_k, cls_c, nex;
+    uint32_t *out;                 // index in C(f) of the chosen candidate, or kNone
+    uint32_t ex[kHubRounds - 1];   // indices chosen in earlier rounds (skipped)
 };
 
 // One block per segment: the candidate of the segment's class with the
-// largest data degree (ties: the smaller index).
+// largest data degree (ties: the smaller index), other than the excluded ones.
 __global__ void pick_hubs(const HubSeg *__restrict__ segs, const uint32_t *__restrict__ goff) {
     const HubSeg sg = segs[blockIdx.x];
     unsigned long long best = 0;
     for (uint32_t i = threadIdx.x; i < sg.ncand; i += blockDim.x) {
         const uint32_t v = sg.cand[i];
         if (sg.cls_k > 1 && vertex_class(v, sg.cls_k) != sg.cls_c) continue;
+        bool skip = false;
+        for (uint32_t k = 0; k < sg.nex; ++k) skip |= sg.ex[k] == i;
+        if (skip) continue;
         const unsigned long long key =
             (1ull << 63) | ((unsigned long long)(goff[v + 1] - goff[v]) << 32) | (0xFFFFFFFFu - i);
         best = max(best, key);
@@ -972,6 +1017,299 @@ __global__ void fix_weights(double *const *__restrict__ w, const uint32_t *const
     }
 }
 
+// Tighter bounds for tree queries: classes only where a same-label pair is
+// three or more edges apart (a merge there would close a cycle), and the
+// other same-label pairs, all two edges apart, handled exactly by the tree
+// program's inclusion-exclusion over blocks (vertices of different classes
+// never share a block).  That counts exactly the embeddings whose far-apart
+// same-label vertices respect their classes, a subset of all embeddings.
+// Terms with a positive coefficient are computed rounding toward zero, the
+// others rounding up, and the signed sum rounding down (bound_sums), so the
+// result is a lower bound.  lb[i] = the bound, formed[i] = 0 where the query
+// is not a tree or has too many terms.
+int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<double> &lb, std::vector<char> &formed) {
+    cudaStream_t s = G->stream;
+    const size_t Q = cs.size();
+    lb.assign(Q, 0.0);
+    formed.assign(Q, 0);
+    struct TPrep {
+        std::vector<BlockTree> terms;
+        std::vector<uint32_t> ck, cc;  // class count and class of each vertex (ck 1: unrestricted)
+        uint64_t words = 0;
+    };
+    std::vector<TPrep> prep(Q);
+    for (size_t i = 0; i < Q; ++i) {
+        const asdm_cs &c = *cs[i];
+        const QueryGraph &q = c.q;
+        if (!c.nonempty || q.n < 2 || q.off[q.n] != 2 * (q.n - 1)) continue;
+        const uint32_t n = q.n;
+        // distances, then the classes of the far pairs' vertices
+        std::vector<std::vector<uint32_t>> dist(n, std::vector<uint32_t>(n, kNone));
+        for (uint32_t r = 0; r < n; ++r) {
+            std::vector<uint32_t> fr{r};
+            dist[r][r] = 0;
+            for (size_t k = 0; k < fr.size(); ++k)
+                for (uint32_t e = q.off[fr[k]]; e < q.off[fr[k] + 1]; ++e)
+                    if (dist[r][q.nbr[e]] == kNone) {
+                        dist[r][q.nbr[e]] = dist[r][fr[k]] + 1;
+                        fr.push_back(q.nbr[e]);
+                    }
+        }
+        auto far = [&](uint32_t u, uint32_t w) { return u != w && q.lab[u] == q.lab[w] && dist[u][w] >= 3; };
+        TPrep &P = prep[i];
+        std::vector<uint32_t> cls(n, kNone);
+        for (uint32_t u = 0; u < n; ++u) {
+            bool any = false;
+            uint64_t used = 0;
+            for (uint32_t w = 0; w < n; ++w)
+                if (far(u, w)) {
+                    any = true;
+                    if (w < u) used |= 1ull << cls[w];
+                }
+            if (!any) continue;
+            uint32_t c0 = 0;
+            while (used >> c0 & 1ull) ++c0;
+            cls[u] = c0;
+        }
+        P.ck.assign(n, 1);
+        P.cc.assign(n, 0);
+        for (uint32_t u = 0; u < n; ++u) {
+            if (cls[u] == kNone) continue;
+            uint32_t k = 0;
+            for (uint32_t w = 0; w < n; ++w)
+                if (q.lab[w] == q.lab[u] && cls[w] != kNone) k = std::max(k, cls[w] + 1);
+            P.ck[u] = k;
+            P.cc[u] = cls[u];
+        }
+        if (!block_trees(q, P.terms, &c, &cls)) continue;
+        for (const BlockTree &t : P.terms)
+            for (uint32_t b = 0; b < t.nb; ++b) P.words += c.ncand[t.rep[b]] * (1 + t.members[b].size());
+        formed[i] = 1;
+    }
+    size_t at = 0;
+    int rc = ASDM_OK;
+    while (at < Q && rc == ASDM_OK) {
+        std::vector<size_t> ids;
+        uint64_t words = 0;
+        for (; at < Q; ++at) {
+            if (!formed[at]) continue;
+            if (!ids.empty() && words + prep[at].words > kTreeChunkWords) break;
+            words += prep[at].words;
+            ids.push_back(at);
+        }
+        if (ids.empty()) break;
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "tree-bound sync failed");
+            break;
+        }
+        G->stage.reset();
+        double *wbuf = nullptr, *d_terms = nullptr, *d_coef = nullptr, *d_out = nullptr;
+        uint32_t *d_mapbuf = nullptr, *d_nroot = nullptr;
+        MapSeg *d_mseg = nullptr;
+        BoundSeg *d_segs = nullptr;
+        BoundChild *d_kids = nullptr;
+        BoundQuery *d_bq = nullptr;
+        BoundSum *d_sums = nullptr;
+        const uint32_t **d_maps = nullptr;
+        const double **d_roots = nullptr;
+        do {
+            // member maps C(rep) -> C(member) of merged blocks, one per (query, rep, member)
+            std::vector<MapSeg> msegs;
+            std::vector<std::vector<std::pair<uint64_t, uint32_t>>> mkey(ids.size());
+            uint64_t mtotal = 0, wtotal = 0;
+            std::vector<std::vector<std::vector<uint64_t>>> woff(ids.size());
+            uint32_t nterms = 0;
+            for (size_t k = 0; k < ids.size(); ++k) {
+                const asdm_cs &c = *cs[ids[k]];
+                const TPrep &P = prep[ids[k]];
+                woff[k].resize(P.terms.size());
+                nterms += (uint32_t)P.terms.size();
+                for (size_t ti = 0; ti < P.terms.size(); ++ti) {
+                    const BlockTree &t = P.terms[ti];
+                    woff[k][ti].resize(t.nb);
+                    for (uint32_t b = 0; b < t.nb; ++b) {
+                        woff[k][ti][b] = wtotal;
+                        wtotal += c.ncand[t.rep[b]];
+                        for (uint32_t u : t.members[b]) {
+                            if (u == t.rep[b]) continue;
+                            const uint64_t key = ((uint64_t)t.rep[b] << 32) | u;
+                            bool have = false;
+                            for (auto &kv : mkey[k]) have = have || kv.first == key;
+                            if (have) continue;
+                            mkey[k].emplace_back(key, (uint32_t)msegs.size());
+                            msegs.push_back(MapSeg{c.d_cand + c.cand_base[t.rep[b]], c.d_cand + c.cand_base[u],
+                                                   nullptr, c.ncand[u], 0, mtotal});
+                            mtotal += c.ncand[t.rep[b]];
+                        }
+                    }
+                }
+            }
+            if ((rc = dalloc(&wbuf, std::max<uint64_t>(wtotal, 1), s)) || (rc = dalloc(&d_terms, nterms, s)) ||
+                (rc = dalloc(&d_coef, nterms, s)) || (rc = dalloc(&d_out, ids.size(), s)))
+                break;
+            std::vector<const uint32_t *> maps;
+            if (mtotal) {
+                if ((rc = dalloc(&d_mapbuf, mtotal, s)) || (rc = dalloc(&d_mseg, msegs.size(), s))) break;
+                for (auto &m : msegs) m.out = d_mapbuf + m.start;
+                if (upload_async(G, d_mseg, msegs.data(), msegs.size() * sizeof(MapSeg)) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "tree-bound map upload failed");
+                    break;
+                }
+                const unsigned grid =
+                    (unsigned)std::min<unsigned long long>((mtotal + 255) / 256, (unsigned long long)G->num_sms * 32);
+                tree_maps<<<grid, 256, 0, s>>>(d_mseg, (uint32_t)msegs.size(), mtotal);
+                ::asdm::count_launch();
+            }
+            auto map_of = [&](size_t k, uint32_t r, uint32_t u) -> const uint32_t * {
+                const uint64_t key = ((uint64_t)r << 32) | u;
+                for (auto &kv : mkey[k])
+                    if (kv.first == key) return msegs[kv.second].out;
+                return nullptr;
+            };
+            // segments by height, children, the terms' root sums and the signed sums
+            std::vector<std::vector<BoundSeg>> lv;
+            std::vector<BoundChild> kids;
+            std::vector<BoundQuery> bqs;
+            std::vector<const double *> roots;
+            std::vector<uint32_t> nroot;
+            std::vector<double> coef;
+            std::vector<BoundSum> sums;
+            for (size_t k = 0; k < ids.size(); ++k) {
+                const asdm_cs &c = *cs[ids[k]];
+                const TPrep &P = prep[ids[k]];
+                sums.push_back(BoundSum{d_terms + coef.size(), d_coef + coef.size(), (uint32_t)P.terms.size(), 0,
+                                        d_out + k});
+                for (size_t ti = 0; ti < P.terms.size(); ++ti) {
+                    const BlockTree &t = P.terms[ti];
+                    const uint32_t up = t.coef < 0 ? 1u : 0u;
+                    auto restricted = [&](uint32_t b) {
+                        for (uint32_t u : t.members[b])
+                            if (P.ck[u] > 1) return u;
+                        return kNone;
+                    };
+                    auto leaf1 = [&](uint32_t b) {
+                        return t.height[b] == 0 && t.members[b].size() == 1 && restricted(b) == kNone;
+                    };
+                    uint32_t root = kNone;
+                    for (uint32_t b = 0; b < t.nb; ++b) {
+                        if (t.parent[b] == kNone) root = b;
+                        if (leaf1(b) && t.parent[b] != kNone) continue;
+                        const uint32_t r = t.rep[b], cu = restricted(b);
+                        BoundSeg sg{};
+                        sg.w = wbuf + woff[k][ti][b];
+                        sg.cand = c.d_cand + c.cand_base[r];
+                        sg.ncand = c.ncand[r];
+                        sg.cls_k = cu == kNone ? 1u : P.ck[cu];
+                        sg.cls_c = cu == kNone ? 0u : P.cc[cu];
+                        sg.up = up;
+                        sg.val_first = (uint32_t)maps.size();
+                        for (uint32_t u : t.members[b])
+                            if (u != r) maps.push_back(map_of(k, r, u));
+                        sg.nval = (uint32_t)maps.size() - sg.val_first;
+                        sg.child_first = (uint32_t)kids.size();
+                        for (uint32_t C = 0; C < t.nb; ++C) {
+                            if (t.parent[C] != b) continue;
+                            const uint32_t e = t.pedge[C], u = t.pfrom[C];
+                            kids.push_back(BoundChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                                      leaf1(C) ? nullptr : wbuf + woff[k][ti][C],
+                                                      u == r ? nullptr : map_of(k, r, u)});
+                        }
+                        sg.nchild = (uint32_t)kids.size() - sg.child_first;
+                        if (lv.size() <= t.height[b]) lv.resize(t.height[b] + 1);
+                        lv[t.height[b]].push_back(sg);
+                    }
+                    BoundQuery bq{};
+                    bq.ncomp = 1;
+                    bq.up = up;
+                    bq.out = d_terms + coef.size();
+                    roots.push_back(wbuf + woff[k][ti][root]);
+                    nroot.push_back(c.ncand[t.rep[root]]);
+                    bqs.push_back(bq);
+                    coef.push_back((double)t.coef);
+                }
+            }
+            std::vector<BoundSeg> segs;
+            std::vector<size_t> first{0};
+            std::vector<unsigned long long> totals;
+            for (auto &l : lv) {
+                unsigned long long tt = 0;
+                for (BoundSeg &sg : l) {
+                    sg.start = tt;
+                    tt += sg.ncand;
+                    segs.push_back(sg);
+                }
+                first.push_back(segs.size());
+                totals.push_back(tt);
+            }
+            if (kids.empty()) kids.push_back(BoundChild{});
+            if (segs.empty()) segs.push_back(BoundSeg{});
+            if (maps.empty()) maps.push_back(nullptr);
+            if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s)) ||
+                (rc = dalloc(&d_maps, maps.size(), s)) || (rc = dalloc(&d_roots, roots.size(), s)) ||
+                (rc = dalloc(&d_nroot, nroot.size(), s)) || (rc = dalloc(&d_bq, bqs.size(), s)) ||
+                (rc = dalloc(&d_sums, sums.size(), s)))
+                break;
+            for (size_t j = 0; j < bqs.size(); ++j) {
+                bqs[j].roots = d_roots + j;
+                bqs[j].nroot = d_nroot + j;
+            }
+            if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
+                upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
+                upload_async(G, d_maps, maps.data(), maps.size() * sizeof(void *)) != cudaSuccess ||
+                upload_async(G, d_roots, roots.data(), roots.size() * sizeof(void *)) != cudaSuccess ||
+                upload_async(G, d_nroot, nroot.data(), nroot.size() * sizeof(uint32_t)) != cudaSuccess ||
+                upload_async(G, d_coef, coef.data(), coef.size() * sizeof(double)) != cudaSuccess ||
+                upload_async(G, d_bq, bqs.data(), bqs.size() * sizeof(BoundQuery)) != cudaSuccess ||
+                upload_async(G, d_sums, sums.data(), sums.size() * sizeof(BoundSum)) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "tree-bound upload failed");
+                break;
+            }
+            for (size_t h = 0; h < totals.size() && rc == ASDM_OK; ++h) {
+                if (!totals[h]) continue;
+                const unsigned grid =
+                    (unsigned)std::min<unsigned long long>((totals[h] + 255) / 256, (unsigned long long)G->num_sms * 32);
+                bound_level<<<grid, 256, 0, s>>>(d_segs + first[h], (uint32_t)(first[h + 1] - first[h]), totals[h],
+                                                 d_kids, d_maps);
+                ::asdm::count_launch();
+                if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "tree-bound kernel failed");
+            }
+            if (rc != ASDM_OK) break;
+            bound_queries<<<(unsigned)bqs.size(), 256, 0, s>>>(d_bq);
+            ::asdm::count_launch();
+            bound_sums<<<(unsigned)((sums.size() + 127) / 128), 128, 0, s>>>(d_sums, (uint32_t)sums.size());
+            ::asdm::count_launch();
+            std::vector<double> out(ids.size());
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "tree-bound readback failed");
+                break;
+            }
+            for (size_t k = 0; k < ids.size(); ++k) lb[ids[k]] = std::max(0.0, out[k]);
+        } while (false);
+        dfree(wbuf, s);
+        dfree(d_terms, s);
+        dfree(d_coef, s);
+        dfree(d_out, s);
+        dfree(d_mapbuf, s);
+        dfree(d_mseg, s);
+        dfree(d_nroot, s);
+        dfree(d_segs, s);
+        dfree(d_kids, s);
+        dfree(d_bq, s);
+        dfree(d_sums, s);
+        dfree(d_maps, s);
+        dfree(d_roots, s);
+        cudaStreamSynchronize(s);
+    }
+    if (rc != ASDM_OK) {
+        lb.assign(Q, 0.0);
+        formed.assign(Q, 0);
+    }
+    return rc;
+}
+
 }  // namespace
 
 // proven[i] = 1 when query i's count is shown to be at least 2^64 (see the
@@ -984,6 +1322,16 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
     const size_t Q = cs.size();
     proven.assign(Q, 0);
     if (lower) lower->assign(Q, 0);
+    const double two64 = 18446744073709551616.0;  // exactly 2^64
+    // tree queries first: their far-class bounds are the tighter ones
+    std::vector<double> tlb;
+    std::vector<char> tformed;
+    ASDM_TRY(tree_bounds(G, cs, tlb, tformed));
+    for (size_t i = 0; i < Q; ++i) {
+        if (!tformed[i]) continue;
+        proven[i] = tlb[i] >= two64;
+        if (lower) (*lower)[i] = proven[i] ? ~0ull : (uint64_t)tlb[i];
+    }
     struct Prep {
         std::vector<char> fixed;                // u in F
         std::vector<uint32_t> fvs;              // F
@@ -999,7 +1347,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
     for (size_t i = 0; i < Q; ++i) {
         const asdm_cs &c = *cs[i];
         const QueryGraph &q = c.q;
-        if (!c.nonempty || q.n < 2) continue;
+        if (!c.nonempty || q.n < 2 || proven[i]) continue;
         Prep &P = prep[i];
         const uint32_t n = q.n;
         // feedback vertex set: peel vertices of degree <= 1, fix the busiest
@@ -1089,8 +1437,19 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
         for (uint32_t f : P.fvs) P.words += c.ncand[f];  // the indicator arrays
         ok[i] = 1;
     }
-    size_t at = 0;
+    // Round 0 fixes every vertex of F to its best candidate.  Later rounds
+    // (queries with a cycle that are not settled yet) move F's first vertex
+    // to its next-best candidates: different images of one vertex count
+    // disjoint sets of embeddings, so the rounds' bounds add up (each sum
+    // stepped down one ulp to stay a lower bound).
+    std::vector<double> acc(Q, 0.0);
+    std::vector<std::vector<uint32_t>> excl(Q);
     int rc = ASDM_OK;
+    for (uint32_t round = 0; round < kHubRounds && rc == ASDM_OK; ++round) {
+    if (round > 0)
+        for (size_t i = 0; i < Q; ++i)
+            ok[i] = ok[i] && !proven[i] && !prep[i].fvs.empty() && excl[i].size() == round;
+    size_t at = 0;
     while (at < Q && rc == ASDM_OK) {
         std::vector<size_t> ids;
         uint64_t words = 0;
@@ -1150,8 +1509,11 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                     }
                 for (size_t j = 0; j < P.fvs.size(); ++j) {
                     const uint32_t f = P.fvs[j];
-                    hsegs.push_back(HubSeg{c.d_cand + c.cand_base[f], c.ncand[f], P.cls_k[f], P.cls_c[f], 0,
-                                           d_hub + hub0[k] + j});
+                    HubSeg hs{c.d_cand + c.cand_base[f], c.ncand[f], P.cls_k[f], P.cls_c[f], 0,
+                              d_hub + hub0[k] + j, {}};
+                    if (j == 0)
+                        for (uint32_t x : excl[ids[k]]) hs.ex[hs.nex++] = x;
+                    hsegs.push_back(hs);
                     fw.push_back(wptr[k][f]);
                     fh.push_back(d_hub + hub0[k] + j);
                 }
@@ -1214,7 +1576,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                         const uint32_t w = q.nbr[e];
                         if (P.parent[w] == u || P.fixed[w])
                             kids.push_back(BoundChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
-                                                      wptr[k][w]});
+                                                      wptr[k][w], nullptr});
                     }
                     sg.nchild = (uint32_t)kids.size() - sg.child_first;
                     if (lv.size() <= P.height[u]) lv.resize(P.height[u] + 1);
@@ -1271,7 +1633,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                 const unsigned grid =
                     (unsigned)std::min<unsigned long long>((totals[h] + 255) / 256, (unsigned long long)G->num_sms * 32);
                 bound_level<<<grid, 256, 0, s>>>(d_segs + first[h], (uint32_t)(first[h + 1] - first[h]), totals[h],
-                                                 d_kids);
+                                                 d_kids, nullptr);
                 ::asdm::count_launch();
                 if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "overflow-bound kernel failed");
             }
@@ -1279,17 +1641,23 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
             bound_queries<<<(unsigned)ids.size(), 256, 0, s>>>(d_bq);
             ::asdm::count_launch();
             std::vector<double> out(ids.size());
+            std::vector<uint32_t> hubs(std::max<uint32_t>(nhub, 1));
             if (cudaGetLastError() != cudaSuccess ||
                 cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaMemcpyAsync(hubs.data(), d_hub, hubs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
                     cudaSuccess ||
                 cudaStreamSynchronize(s) != cudaSuccess) {
                 rc = fail(ASDM_ERR_CUDA, "overflow-bound readback failed");
                 break;
             }
-            const double two64 = 18446744073709551616.0;  // exactly 2^64
             for (size_t k = 0; k < ids.size(); ++k) {
-                proven[ids[k]] = out[k] >= two64;
-                if (lower) (*lower)[ids[k]] = out[k] >= two64 ? ~0ull : (uint64_t)out[k];
+                const size_t i = ids[k];
+                acc[i] = round == 0 ? out[k] : std::nextafter(acc[i] + out[k], 0.0);
+                if (!prep[i].fvs.empty() && hubs[hub0[k]] != kNone) excl[i].push_back(hubs[hub0[k]]);
+                // the larger of this bound and the tree bound (both count subsets of the embeddings)
+                proven[i] = acc[i] >= two64;
+                if (lower) (*lower)[i] = std::max<uint64_t>((*lower)[i], proven[i] ? ~0ull : (uint64_t)acc[i]);
             }
         } while (false);
         dfree(wbuf, s);
@@ -1306,6 +1674,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
         dfree(d_fh, s);
         dfree(d_roots, s);
         cudaStreamSynchronize(s);
+    }
     }
     if (rc != ASDM_OK) {
         proven.assign(Q, 0);

@@ -110,13 +110,16 @@ class Dataset:
     nbr: List[List[np.ndarray]] = field(default_factory=list)  # per sample: per node local neighbours
     y: List[float] = field(default_factory=list)             # log(1 + count)
     censored: List[bool] = field(default_factory=list)       # count reached the limit (y is a floor)
+    sampled: List[float] = field(default_factory=list)       # log(1 + sampling estimate), or nan
+    sampled_targets: bool = False                            # censored samples take the sampling estimate as y
     size: List[int] = field(default_factory=list)
     query: List[int] = field(default_factory=list)
 
     def __len__(self):
         return len(self.y)
 
-    def add_query(self, cs: A.CandidateSpace, masks: Sequence[int], counts, status, qid: int):
+    def add_query(self, cs: A.CandidateSpace, masks: Sequence[int], counts, status, qid: int,
+                  count_limit: int = COUNT_LIMIT, sampled=None):
         keep = [i for i in range(len(masks)) if status[i] in (A.OK, A.ERR_LIMIT)]
         if not keep:
             return
@@ -129,8 +132,13 @@ class Dataset:
             self.x.append(x[s:e].copy())
             self.nbr.append([adj[off[v]:off[v + 1]].astype(np.int64) - s for v in range(s, e)])
             lim = status[i] == A.ERR_LIMIT
-            self.y.append(float(np.log1p(float(COUNT_LIMIT if lim else counts[i]))))
+            y = float(np.log1p(float(count_limit if lim else counts[i])))
+            if lim and sampled is not None and self.sampled_targets:
+                # past the exact-count limit the sampling estimate is the target (never below the floor)
+                y = max(y, float(np.log1p(sampled[i])))
+            self.y.append(y)
             self.censored.append(bool(lim))
+            self.sampled.append(float(np.log1p(sampled[i])) if sampled is not None else float("nan"))
             self.size.append(e - s)
             self.query.append(qid)
 
@@ -156,10 +164,13 @@ class Dataset:
 
 def collect(dg: A.DeviceGraph, queries: Sequence[A.HostGraph], rng: np.random.Generator, per_query: int = 24,
             kmin: int = 3, kmax: int = 6, time_limit_s: float = 5.0, chunk: int = 64, qid0: int = 0,
-            log=None) -> Dataset:
+            log=None, count_limit: int = COUNT_LIMIT, walks: int = 0, sampled_targets: bool = False) -> Dataset:
     """Exact partial-match counts of sampled sub-queries inside each query's
-    candidate space (counts at or above COUNT_LIMIT are kept as censored)."""
-    ds = Dataset()
+    candidate space (counts at or above count_limit are kept as censored);
+    with walks > 0 also the sampling estimator's estimates of the same
+    sub-queries (asdm_sample_subsets), which with sampled_targets become the
+    targets of the censored samples."""
+    ds = Dataset(sampled_targets=sampled_targets)
     for at in range(0, len(queries), chunk):
         part = list(queries[at:at + chunk])
         css = A.candidate_spaces(dg, part)
@@ -171,8 +182,9 @@ def collect(dg: A.DeviceGraph, queries: Sequence[A.HostGraph], rng: np.random.Ge
                 continue
             adj = query_adjacency(q)
             orders = [connected_order(adj, m) for m in masks]
-            counts, status = cs.prefix_counts(orders, time_limit_s=time_limit_s, count_limit=COUNT_LIMIT)
-            ds.add_query(cs, masks, counts, status, qid0 + at + j)
+            counts, status = cs.prefix_counts(orders, time_limit_s=time_limit_s, count_limit=count_limit)
+            sampled = cs.sample_cardinalities(masks, walks, seed=qid0 + at + j) if walks else None
+            ds.add_query(cs, masks, counts, status, qid0 + at + j, count_limit, sampled)
         del css
         if log:
             log("collected %d queries, %d samples" % (min(at + chunk, len(queries)), len(ds)))
@@ -216,6 +228,10 @@ def q_errors(pred_log: np.ndarray, true_log: np.ndarray) -> np.ndarray:
 
 
 def evaluate(est: A.Estimator, ds: Dataset) -> dict:
+    """q-errors of the learned estimates (and of the planner's independence
+    estimate, and of the sampling estimator where the samples carry its
+    estimates) against the exact counts; for censored samples (counts past the
+    limit) the sampling estimator is the judge of the learned estimates."""
     pred = predict(est, ds)
     y = np.asarray(ds.y)
     exact = ~np.asarray(ds.censored, bool)
@@ -227,8 +243,15 @@ def evaluate(est: A.Estimator, ds: Dataset) -> dict:
         return {"p50": float(np.percentile(a, 50)), "p90": float(np.percentile(a, 90)),
                 "p99": float(np.percentile(a, 99)), "mean": float(np.mean(a))} if len(a) else {}
 
-    return {"samples": int(exact.sum()), "censored": int((~exact).sum()), "learned": pct(q),
-            "independence": pct(qi)}
+    out = {"samples": int(exact.sum()), "censored": int((~exact).sum()), "learned": pct(q),
+           "independence": pct(qi)}
+    smp = np.asarray(ds.sampled, np.float64)
+    if len(smp) and np.isfinite(smp).any():
+        have = np.isfinite(smp)
+        out["sampling"] = pct(q_errors(smp[exact & have], y[exact & have]))
+        cen = ~exact & have
+        out["censored_learned_vs_sampling"] = pct(q_errors(pred[cen], smp[cen]))
+    return out
 
 
 def queries_c3(g: A.HostGraph, count: int, seed0: int) -> List[A.HostGraph]:
@@ -257,22 +280,46 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--out", default=DEFAULT_PARAMS)
     ap.add_argument("--report", default=DEFAULT_REPORT)
+    ap.add_argument("--eval-only", default="", help="evaluate these trained parameters on the held-out queries")
+    ap.add_argument("--count-limit", type=int, default=COUNT_LIMIT, help="exact counts past this are censored")
+    ap.add_argument("--walks", type=int, default=4096, help="sampling-estimator walks per held-out sub-query")
+    ap.add_argument("--train-walks", type=int, default=1024,
+                    help="sampling-estimator walks per training sub-query (targets of the censored ones; 0: floors)")
     a = ap.parse_args(argv)
     t0 = time.time()
     g = W.graph(W.C1)
     dg = A.DeviceGraph(g)
     rng = np.random.default_rng(7)
+    if a.eval_only:
+        # the held-out set alone: learned, sampling and independence estimates against exact counts
+        est = load(a.eval_only)
+        hq = queries_c3(g, a.heldout, HELDOUT_QUERY_SEED)
+        hs = collect(dg, hq, rng, a.per_query, qid0=10 ** 6, log=print, count_limit=a.count_limit,
+                     time_limit_s=20.0, walks=a.walks)
+        rep = {"graph": W.C1, "params": os.path.basename(a.eval_only), "heldout_queries": a.heldout,
+               "per_query": a.per_query, "heldout_seed": HELDOUT_QUERY_SEED, "count_limit": a.count_limit,
+               "walks": a.walks, "collect_s": time.time() - t0, "heldout_eval": evaluate(est, hs)}
+        with open(a.report, "w") as fh:
+            json.dump(rep, fh, indent=1)
+        print(json.dumps(rep["heldout_eval"]))
+        return
     tq = queries_c3(g, a.train, TRAIN_QUERY_SEED)
     hq = queries_c3(g, a.heldout, HELDOUT_QUERY_SEED)
     t1 = time.time()
-    ds = collect(dg, tq, rng, a.per_query, log=print)
-    hs = collect(dg, hq, rng, a.per_query, qid0=10 ** 6, log=print)
+    # training targets: exact counts up to COUNT_LIMIT, sampling estimates past it; held out:
+    # exact counts up to --count-limit, with the sampling estimator's estimates beside them
+    ds = collect(dg, tq, rng, a.per_query, log=print, walks=a.train_walks, sampled_targets=a.train_walks > 0)
+    hs = collect(dg, hq, rng, a.per_query, qid0=10 ** 6, log=print, count_limit=a.count_limit,
+                 time_limit_s=20.0, walks=a.walks)
     t2 = time.time()
     est = A.Estimator(A.EST_FEATURES, 1)
     losses = train(est, ds, epochs=a.epochs, log=print)
     t3 = time.time()
     rep = {"graph": W.C1, "train_queries": a.train, "heldout_queries": a.heldout, "per_query": a.per_query,
            "train_seed": TRAIN_QUERY_SEED, "heldout_seed": HELDOUT_QUERY_SEED, "count_limit": COUNT_LIMIT,
+           "heldout_count_limit": a.count_limit, "train_walks": a.train_walks, "heldout_walks": a.walks,
+           "train_targets": "exact counts up to count_limit, sampling estimates past it" if a.train_walks else
+                            "exact counts up to count_limit, count_limit past it",
            "train_samples": len(ds), "epochs": a.epochs, "final_loss": losses[-1],
            "collect_s": t2 - t1, "train_s": t3 - t2, "setup_s": t1 - t0,
            "train_eval": evaluate(est, ds), "heldout_eval": evaluate(est, hs)}

@@ -567,7 +567,7 @@ def main():
             t = json.load(fh).get(args.workload) or {}
         traffic, traffic_cs = t.get("enum_batch_kernel"), t.get("k1_k3")
     status = {STATUS_NAME.get(k, k): v for k, v in agg["status"].items()}
-    decided = status.get("ok", 0) + status.get("overflow", 0)
+    n_decided = status.get("ok", 0) + status.get("overflow", 0)
     line = {
         "metric": "exact-count queries/sec",
         "value": Qall / (ms / 1e3),
@@ -587,7 +587,7 @@ def main():
                                      "warps, i.e. the time it would run alone on the GPU (timeouts are counted "
                                      "at the cap and reported, never dropped)",
                        status_per_step=status,
-                       decided_queries_per_s=world * decided / (ms / 1e3),
+                       decided_queries_per_s=world * n_decided / (ms / 1e3),
                        exact_counts_confirmed_by_reference=len(checker.confirmed),
                        form="batched: asdm_run_batch_ex (one launch per CFL phase for the group, tree program, "
                             "overflow lower bounds, one persistent enumeration kernel over all (query, root task) "

@@ -226,6 +226,10 @@ int asdm_card_write(const asdm_card *c, const char *path, double plan_seconds);
  * Replaces cardEstimateLabeled (plan/estimator.cpp:173-291), the reference's
  * sampling estimator, as the input of the card-guided planner. */
 int asdm_card_sample(asdm_cs *cs, uint32_t max_subset, uint32_t walks, uint64_t seed, asdm_card **out);
+/* The same sampling estimates for given connected vertex subsets (bit u =
+ * query vertex u): est[i] for masks[i], `walks` walks each (0 = 512). */
+int asdm_sample_subsets(asdm_cs *cs, uint32_t nsub, const uint64_t *masks, uint32_t walks, uint64_t seed,
+                        double *est);
 void asdm_card_free(asdm_card *c);
 int asdm_plan_free(asdm_plan *p);
 

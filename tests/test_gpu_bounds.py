@@ -101,3 +101,48 @@ def test_lower_bound_below_two64_is_exact_on_small_known_counts():
         assert A.adaptive_share_join(cs).count == exact
         cs.close()
     dg.close()
+
+
+def _far_pairs(q):
+    """Same-label pairs three or more edges apart."""
+    adj = [set(q.nbrs[q.offsets[u]:q.offsets[u + 1]].tolist()) for u in range(q.n)]
+    far = []
+    for a in range(q.n):
+        dist = {a: 0}
+        frontier = [a]
+        while frontier:
+            nxt = []
+            for x in frontier:
+                for y in adj[x]:
+                    if y not in dist:
+                        dist[y] = dist[x] + 1
+                        nxt.append(y)
+            frontier = nxt
+        far += [(a, b) for b in range(a + 1, q.n) if q.labels[a] == q.labels[b] and dist.get(b, 99) >= 3]
+    return far
+
+
+def test_tree_bound_is_the_exact_count_without_far_pairs(golden, c0_files, c0d_files):
+    """For a tree query whose same-label vertices are all two edges apart the
+    tree bound restricts nothing: it is the inclusion-exclusion count itself,
+    exact in doubles below 2^53; with far pairs it stays a lower bound."""
+    exact_checked = below = 0
+    for g, recs, qs in ((c0_files[0], golden["sets"]["c0"], c0_files[2]),
+                        (c0d_files[0], golden["sets"]["c0d"], None)):
+        dg = A.DeviceGraph(g)
+        for rec in recs:
+            q = qs[rec["index"]] if qs is not None else g.random_walk_query(rec["size"], rec["seed"], 0)
+            if q.m2 // 2 != q.n - 1 or rec["count"] == 0:
+                continue
+            cs = A.CandidateSpace(dg, q)
+            lb, exceeds = cs.count_lower_bound()
+            cs.close()
+            assert not exceeds
+            if not _far_pairs(q):
+                assert lb == rec["count"], (rec["index"], lb, rec["count"])
+                exact_checked += 1
+            else:
+                assert lb <= rec["count"]
+                below += 1
+        dg.close()
+    assert exact_checked >= 30 and below >= 1, (exact_checked, below)
