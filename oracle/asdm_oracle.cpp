@@ -435,12 +435,21 @@ struct Enumerator {
     }
 };
 
+uint32_t vertex_class(uint32_t v, uint32_t k);
+
+// Classes of query vertices for restricted counts: vertex u may only take data
+// vertices v with vertex_class(v, k[u]) == c[u] (k[u] <= 1: no restriction).
+struct Classes {
+    std::vector<uint32_t> k, c;
+};
+
 // hom(Q/pi) for the quotient of tree query q by the blocks `block` (block of
 // each vertex): a block's candidates are the data vertices that are candidates
-// of all its members; an edge between two blocks needs data adjacency.
-// Returns false when the quotient is not a tree.
+// of all its members (and of the members' classes, when given); an edge
+// between two blocks needs data adjacency.  Returns false when the quotient is
+// not a tree.
 bool quotient_hom(const OGraph &q, const OGraph &g, const CandSpace &cs, const std::vector<uint32_t> &block,
-                  uint32_t nb, unsigned __int128 &out) {
+                  uint32_t nb, unsigned __int128 &out, const Classes *cls = nullptr) {
     std::vector<std::vector<uint32_t>> adj(nb), members(nb);
     for (uint32_t u = 0; u < q.n; ++u) members[block[u]].push_back(u);
     uint64_t nedges = 0;
@@ -464,6 +473,14 @@ bool quotient_hom(const OGraph &q, const OGraph &g, const CandSpace &cs, const s
             std::set_intersection(cand[b].begin(), cand[b].end(), o.begin(), o.end(), std::back_inserter(t));
             cand[b].swap(t);
         }
+        if (cls)
+            for (uint32_t u : members[b]) {
+                if (cls->k[u] <= 1) continue;
+                std::vector<uint32_t> t;
+                for (uint32_t v : cand[b])
+                    if (vertex_class(v, cls->k[u]) == cls->c[u]) t.push_back(v);
+                cand[b].swap(t);
+            }
     }
     // rooted at block 0: BFS order, then weights bottom-up
     std::vector<uint32_t> order{0}, parent(nb, UINT32_MAX);
@@ -509,7 +526,8 @@ bool quotient_hom(const OGraph &q, const OGraph &g, const CandSpace &cs, const s
 // of mu(pi) * hom(Q/pi), mu(pi) = prod over blocks of (-1)^(|B|-1) (|B|-1)!.
 // status: 0 exact (count set), 1 the count is >= 2^64, 2 not countable this
 // way (a quotient with a cycle, too many partitions, or a term too large).
-int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &count) {
+int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &count,
+               const Classes *cls = nullptr, unsigned __int128 *wide = nullptr) {
     count = 0;
     if (q.n < 2 || q.m2 != 2ull * (q.n - 1)) return 2;
     std::vector<uint32_t> block(q.n, 0);
@@ -529,7 +547,7 @@ int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &
                 mu *= (m.size() % 2 == 0) ? -f : f;
             }
             unsigned __int128 h = 0;
-            if (!quotient_hom(q, g, cs, block, (uint32_t)members.size(), h) || h >= (unsigned __int128)limit) {
+            if (!quotient_hom(q, g, cs, block, (uint32_t)members.size(), h, cls) || h >= (unsigned __int128)limit) {
                 ok = false;
                 return;
             }
@@ -539,7 +557,9 @@ int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &
         for (size_t b = 0; b < members.size() && ok; ++b) {
             if (q.lab[members[b][0]] != q.lab[u]) continue;
             bool adj = false;
-            for (uint32_t w : members[b]) adj = adj || q.adjacent(u, w);
+            for (uint32_t w : members[b])
+                adj = adj || q.adjacent(u, w) ||
+                      (cls && cls->k[u] > 1 && cls->k[w] > 1 && cls->c[u] != cls->c[w]);
             if (adj) continue;
             members[b].push_back(u);
             block[u] = (uint32_t)b;
@@ -554,9 +574,58 @@ int tree_count(const OGraph &q, const OGraph &g, const CandSpace &cs, uint64_t &
     };
     place(0);
     if (!ok || total < 0) return 2;
+    if (wide) *wide = (unsigned __int128)total;
     if (total >= ((__int128)1 << 64)) return 1;
     count = (uint64_t)total;
     return 0;
+}
+
+// The device's tighter bound for tree queries, restated: classes (greedy in
+// vertex order) only for same-label pairs three or more edges apart, the
+// other pairs by inclusion-exclusion; the exact number of embeddings that
+// respect those classes.  false when the query is not a tree or the count
+// cannot be formed this way.
+bool tree_class_bound(const OGraph &q, const OGraph &g, const CandSpace &cs, unsigned __int128 &out) {
+    const uint32_t n = q.n;
+    if (n < 2 || q.m2 != 2ull * (n - 1)) return false;
+    std::vector<std::vector<uint32_t>> dist(n, std::vector<uint32_t>(n, UINT32_MAX));
+    for (uint32_t r = 0; r < n; ++r) {
+        std::vector<uint32_t> fr{r};
+        dist[r][r] = 0;
+        for (size_t k = 0; k < fr.size(); ++k)
+            for (uint64_t e = q.off[fr[k]]; e < q.off[fr[k] + 1]; ++e)
+                if (dist[r][q.nbr[e]] == UINT32_MAX) {
+                    dist[r][q.nbr[e]] = dist[r][fr[k]] + 1;
+                    fr.push_back(q.nbr[e]);
+                }
+    }
+    std::vector<uint32_t> col(n, UINT32_MAX);
+    for (uint32_t u = 0; u < n; ++u) {
+        std::vector<char> used(n + 1, 0);
+        bool any = false;
+        for (uint32_t w = 0; w < n; ++w)
+            if (w != u && q.lab[w] == q.lab[u] && dist[u][w] >= 3) {
+                any = true;
+                if (w < u) used[col[w]] = 1;
+            }
+        if (!any) continue;
+        uint32_t c = 0;
+        while (used[c]) ++c;
+        col[u] = c;
+    }
+    Classes cls;
+    cls.k.assign(n, 1);
+    cls.c.assign(n, 0);
+    for (uint32_t u = 0; u < n; ++u) {
+        if (col[u] == UINT32_MAX) continue;
+        uint32_t k = 0;
+        for (uint32_t w = 0; w < n; ++w)
+            if (q.lab[w] == q.lab[u] && col[w] != UINT32_MAX) k = std::max(k, col[w] + 1);
+        cls.k[u] = k;
+        cls.c[u] = col[u];
+    }
+    uint64_t c64 = 0;
+    return tree_count(q, g, cs, c64, &cls, &out) != 2;
 }
 
 // The device's overflow lower bound, restated from its definition (the set
@@ -774,8 +843,9 @@ int orc_tree_list(const char *dpath, const char *list) {
 }
 
 // The lower bounds of the queries of a list file against one data graph:
-// "B <k> <bound>" (decimal, saturated at 2^127), "B <k> none" when the rules
-// form no bound, "B <k> empty" for an empty candidate set.
+// "B <k> <bound>" (decimal, saturated at 2^127; for trees the larger of the
+// general bound and the far-class tree bound), "B <k> none" when the rules form
+// no bound, "B <k> empty" for an empty candidate set.
 int orc_bound_list(const char *dpath, const char *list) {
     OGraph g;
     if (!load_graph(dpath, g)) return 2;
@@ -790,8 +860,12 @@ int orc_bound_list(const char *dpath, const char *list) {
             std::cout << "B " << k << " empty" << std::endl;
             continue;
         }
-        unsigned __int128 lb = 0;
-        if (lower_bound(q, g, cs, lb) != 0) {
+        unsigned __int128 lb = 0, tb = 0;
+        const bool general = lower_bound(q, g, cs, lb) == 0;
+        // the device reports the larger of its two bounds
+        const bool tree = tree_class_bound(q, g, cs, tb);
+        if (tree && tb > lb) lb = tb;
+        if (!general && !tree) {
             std::cout << "B " << k << " none" << std::endl;
             continue;
         }

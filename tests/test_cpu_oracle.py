@@ -102,3 +102,44 @@ def test_oracle_lower_bound_never_exceeds_golden_counts(golden, c0_files, tmp_pa
         assert int(v) <= rec["count"], (rec["index"], v, rec["count"])
         positive += int(v) > 0
     assert formed >= 150 and positive >= 20
+
+
+def _far_same_label_pair(q):
+    """Whether tree query q has two same-label vertices three or more edges apart."""
+    off, nb, lab = q.offsets, q.nbrs, q.labels
+    for r in range(q.n):
+        dist = {r: 0}
+        front = [r]
+        for u in front:
+            for e in range(off[u], off[u + 1]):
+                w = int(nb[e])
+                if w not in dist:
+                    dist[w] = dist[u] + 1
+                    front.append(w)
+        if any(w != r and lab[w] == lab[r] and d >= 3 for w, d in dist.items()):
+            return True
+    return False
+
+
+def test_oracle_tree_bound_is_the_count_without_far_pairs(golden, c0_files, tmp_path):
+    """For a tree whose same-label vertices are all within two edges, the
+    far-class tree bound restricts nothing: asdm_oracle -b gives the exact
+    count, equal to the reference's."""
+    import subprocess
+    g, dpath, qs, qpaths = c0_files
+    O.build_oracle()
+    recs = [r for r in golden["sets"]["c0"]
+            if qs[r["index"]].m2 // 2 == qs[r["index"]].n - 1 and not _far_same_label_pair(qs[r["index"]])]
+    lst = tmp_path / "near.txt"
+    lst.write_text("\n".join(qpaths[r["index"]] for r in recs) + "\n")
+    out = subprocess.run([O.ORACLE_BIN, "-d", dpath, "-b", str(lst)], capture_output=True, text=True, check=True)
+    equal = 0
+    for line in out.stdout.splitlines():
+        _, k, v = line.split()
+        rec = recs[int(k)]
+        if v == "empty":
+            assert rec["count"] == 0
+            continue
+        assert int(v) == rec["count"], (rec["index"], v, rec["count"])
+        equal += 1
+    assert equal >= 40, (equal, len(recs))
