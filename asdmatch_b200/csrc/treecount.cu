@@ -793,6 +793,39 @@ constexpr uint64_t kTreeChunkWords = 1ull << 28;  // 2 GiB of weights per launch
 
 constexpr uint32_t kMaxFixed = 6;  // largest feedback vertex set tried
 
+// Feedback vertex set of q, greedily: peel vertices of degree <= 1, fix the
+// one of highest remaining degree (the lowest id among equals), repeat.
+void greedy_fvs(const QueryGraph &q, std::vector<char> &fixed, std::vector<uint32_t> &fvs) {
+    const uint32_t n = q.n;
+    fixed.assign(n, 0);
+    fvs.clear();
+    std::vector<char> gone(n, 0);
+    std::vector<uint32_t> deg(n);
+    for (uint32_t u = 0; u < n; ++u) deg[u] = q.deg(u);
+    for (;;) {
+        bool changed = true;
+        while (changed) {
+            changed = false;
+            for (uint32_t u = 0; u < n; ++u)
+                if (!gone[u] && deg[u] <= 1) {
+                    gone[u] = 1;
+                    changed = true;
+                    for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e)
+                        if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+                }
+        }
+        uint32_t best = kNone;
+        for (uint32_t u = 0; u < n; ++u)
+            if (!gone[u] && (best == kNone || deg[u] > deg[best])) best = u;
+        if (best == kNone) break;
+        fixed[best] = 1;
+        fvs.push_back(best);
+        gone[best] = 1;
+        for (uint32_t e = q.off[best]; e < q.off[best + 1]; ++e)
+            if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+    }
+}
+
 // Class of data vertex v among k classes (a multiplicative hash of its id).
 __device__ __forceinline__ uint32_t vertex_class(uint32_t v, uint32_t k) {
     return (uint32_t)((((unsigned long long)v * 0x9E3779B97F4A7C15ull) >> 32) % k);
@@ -808,6 +841,8 @@ struct BoundSeg {
     uint32_t child_first, nchild, up;
     uint32_t val_first, nval;   // maps C(rep) -> C(member) of the block's other members
     unsigned long long start;   // first item of this segment in the launch
+    const uint32_t *pin;        // when set: only the data vertex pin_cand[*pin] (none when *pin is kNone)
+    const uint32_t *pin_cand;
 };
 
 struct BoundChild {
@@ -820,7 +855,8 @@ __device__ __forceinline__ double dadd(double a, double b, bool up) { return up 
 __device__ __forceinline__ double dmul(double a, double b, bool up) { return up ? __dmul_ru(a, b) : __dmul_rz(a, b); }
 
 // One thread per candidate of the level's segments:
-//   w_u(i) = [C(u)[i] has u's class and is a candidate of every member] *
+//   w_u(i) = [C(u)[i] has u's class, is the pinned vertex if u is pinned, and
+//             is a candidate of every member] *
 //            prod over children c of sum over j in list_{u->c}(i) of w_c(j),
 // rounded toward zero (or up); lists longer than 32 entries are summed by the warp.
 __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, unsigned long long total,
@@ -843,6 +879,10 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
             sg = segs[lo];
             i = (uint32_t)(t - sg.start);
             if (sg.cls_k > 1) alive = vertex_class(sg.cand[i], sg.cls_k) == sg.cls_c;
+            if (sg.pin) {
+                const uint32_t h = *sg.pin;
+                alive = alive && h != kNone && sg.cand[i] == sg.pin_cand[h];
+            }
             for (uint32_t k = 0; k < sg.nval && alive; ++k) alive = maps[sg.val_first + k][i] != kNone;
         }
         const bool up = sg.up != 0;
@@ -1310,6 +1350,534 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
     return rc;
 }
 
+// First-order (Bonferroni) bounds, without classes.  With F (greedy_fvs)
+// fixed to hubs, H is the number of homomorphisms of Q into the candidate
+// space: every vertex outside F on its candidates, F on its hubs, every edge
+// kept (the forest program with indicator copies, without classes).  A
+// homomorphism that is not an embedding maps two query vertices to one data
+// vertex; the two have one label (a candidate carries its query vertex's
+// label) and are not adjacent (data graphs have no self loops).  Those that
+// map the pair {a, b} together number at most T_ab:
+//   * a in F, b not: the program with b pinned to a's hub (exact);
+//   * neither in F: the program with b merged into a (one block on the
+//     candidates of both); where the merge closes a cycle, the edge that
+//     would close it is left out of the forest (fewer constraints, so more
+//     homomorphisms: an upper bound);
+//   * both in F: none (same-label vertices of F take hubs of different
+//     classes, never one vertex).
+// So count >= H - sum of T_ab.  H is rounded toward zero, every T_ab up, and
+// the difference down (on the host: sums stepped one ulp up, the difference
+// one ulp down).  As with the class bounds, later rounds move F's first
+// vertex to its next hubs and the rounds' positive bounds add up.  Where only
+// the proof matters (no bound value asked for), a round counts its T terms
+// only for queries whose H could still carry the sum to 2^64.
+
+// One program of a pair bound: the forest over the vertices outside F, with
+// b in a's block when merged, or vertex `pin` pinned to the hub of F's
+// vertex fvs[pin_f].
+struct PairTerm {
+    uint32_t ma = kNone, mb = kNone;
+    uint32_t pin = kNone, pin_f = kNone;
+    uint32_t nb = 0;
+    std::vector<uint32_t> block;                  // by vertex (kNone in F)
+    std::vector<std::vector<uint32_t>> members;   // by block, ascending
+    std::vector<uint32_t> rep, parent, pedge, pfrom, height;
+    std::vector<char> fnbr;                       // a member has an edge into F
+    uint64_t words = 0;                           // weight words of the blocks that need them
+};
+
+// Whether block b of term t needs a weight array: all but one-vertex leaves
+// with a parent, no edge into F and no pin (the parent takes their list length).
+bool pair_needs_weights(const PairTerm &t, uint32_t b) {
+    return !(t.height[b] == 0 && t.members[b].size() == 1 && !t.fnbr[b] && t.parent[b] != kNone &&
+             t.members[b][0] != t.pin);
+}
+
+// The forest of a term: blocks in order of their lowest member; breadth-first
+// from the lowest unvisited block, each block's members in id order and
+// their neighbours in adjacency order; an edge into a visited block is left
+// out.
+void pair_forest(const QueryGraph &q, const std::vector<char> &fixed, const asdm_cs &c, PairTerm &t) {
+    const uint32_t n = q.n;
+    t.block.assign(n, kNone);
+    t.members.clear();
+    for (uint32_t u = 0; u < n; ++u) {
+        if (fixed[u] || u == t.mb) continue;
+        t.block[u] = (uint32_t)t.members.size();
+        t.members.push_back({u});
+    }
+    if (t.mb != kNone) {
+        auto &m = t.members[t.block[t.ma]];
+        t.block[t.mb] = t.block[t.ma];
+        m.push_back(t.mb);
+        std::sort(m.begin(), m.end());
+    }
+    t.nb = (uint32_t)t.members.size();
+    t.rep.assign(t.nb, kNone);
+    t.parent.assign(t.nb, kNone);
+    t.pedge.assign(t.nb, kNone);
+    t.pfrom.assign(t.nb, kNone);
+    t.height.assign(t.nb, 0);
+    t.fnbr.assign(t.nb, 0);
+    std::vector<uint32_t> order;
+    for (uint32_t r = 0; r < t.nb; ++r) {
+        if (t.rep[r] != kNone) continue;
+        t.rep[r] = t.members[r][0];
+        const size_t first = order.size();
+        order.push_back(r);
+        for (size_t k = first; k < order.size(); ++k) {
+            const uint32_t B = order[k];
+            for (uint32_t u : t.members[B])
+                for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                    const uint32_t w = q.nbr[e];
+                    if (fixed[w]) {
+                        t.fnbr[B] = 1;
+                        continue;
+                    }
+                    const uint32_t C = t.block[w];
+                    if (C == B || t.rep[C] != kNone) continue;
+                    t.rep[C] = w;
+                    t.parent[C] = B;
+                    t.pedge[C] = e;
+                    t.pfrom[C] = u;
+                    order.push_back(C);
+                }
+        }
+    }
+    for (size_t k = order.size(); k-- > 0;) {
+        const uint32_t C = order[k];
+        if (t.parent[C] != kNone) t.height[t.parent[C]] = std::max(t.height[t.parent[C]], t.height[C] + 1);
+    }
+    t.words = 0;
+    for (uint32_t b = 0; b < t.nb; ++b)
+        if (pair_needs_weights(t, b)) t.words += c.ncand[t.rep[b]];
+}
+
+struct PairPrep {
+    std::vector<char> fixed;
+    std::vector<uint32_t> fvs, fk, fc;  // F; class counts and classes among F's same-label vertices
+    std::vector<PairTerm> terms;        // terms[0]: H; then one per pair
+    uint64_t fwords = 0;                // indicator words of F
+};
+
+// Values of the programs `jobs` (query, term) of one round, one double each:
+// rounded toward zero for terms[0], up for the others.  d_hub holds the
+// round's hub indices (query i's F from hub0[i]), d_eok the checks of the
+// edges inside F (query i's from fe0[i], nfe[i] of them).  A query's jobs
+// are consecutive.
+int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<PairPrep> &prep,
+                const std::vector<std::pair<size_t, uint32_t>> &jobs, const uint32_t *d_hub,
+                const std::vector<uint32_t> &hub0, const uint32_t *d_eok, const std::vector<uint32_t> &fe0,
+                const std::vector<uint32_t> &nfe, std::vector<double> &vals) {
+    cudaStream_t s = G->stream;
+    vals.assign(jobs.size(), 0.0);
+    size_t at = 0;
+    int rc = ASDM_OK;
+    while (at < jobs.size() && rc == ASDM_OK) {
+        // a chunk: consecutive jobs whose weights and indicators fit kTreeChunkWords (one job at least)
+        const size_t j0 = at;
+        uint64_t words = 0;
+        std::vector<size_t> qs;
+        for (; at < jobs.size(); ++at) {
+            const size_t i = jobs[at].first;
+            uint64_t add = prep[i].terms[jobs[at].second].words;
+            const bool new_q = qs.empty() || qs.back() != i;
+            if (new_q) add += prep[i].fwords;
+            if (at > j0 && words + add > kTreeChunkWords) break;
+            words += add;
+            if (new_q) qs.push_back(i);
+        }
+        const size_t j1 = at;
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "pair-bound sync failed");
+            break;
+        }
+        G->stage.reset();
+        double *wbuf = nullptr, *d_out = nullptr;
+        uint32_t *d_mapbuf = nullptr, *d_nroot = nullptr;
+        MapSeg *d_mseg = nullptr;
+        BoundSeg *d_segs = nullptr;
+        BoundChild *d_kids = nullptr;
+        BoundQuery *d_bq = nullptr;
+        double **d_fw = nullptr;
+        const uint32_t **d_fh = nullptr, **d_maps = nullptr;
+        const double **d_roots = nullptr;
+        do {
+            if ((rc = dalloc(&wbuf, std::max<uint64_t>(words, 1), s)) || (rc = dalloc(&d_out, j1 - j0, s))) break;
+            if (cudaMemsetAsync(wbuf, 0, std::max<uint64_t>(words, 1) * sizeof(double), s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "pair-bound reset failed");
+                break;
+            }
+            // indicators of F, one set per query of the chunk
+            uint64_t wo = 0;
+            std::vector<std::vector<double *>> find(cs.size());
+            std::vector<double *> fw;
+            std::vector<const uint32_t *> fh;
+            for (size_t i : qs) {
+                const asdm_cs &c = *cs[i];
+                const PairPrep &P = prep[i];
+                find[i].assign(c.q.n, nullptr);
+                for (size_t j = 0; j < P.fvs.size(); ++j) {
+                    const uint32_t f = P.fvs[j];
+                    find[i][f] = wbuf + wo;
+                    wo += c.ncand[f];
+                    fw.push_back(find[i][f]);
+                    fh.push_back(d_hub + hub0[i] + j);
+                }
+            }
+            // maps C(rep) -> C(other member) of merged blocks
+            std::vector<MapSeg> msegs;
+            std::vector<std::pair<std::pair<size_t, uint64_t>, uint32_t>> mkey;
+            uint64_t mtotal = 0;
+            auto map_slot = [&](size_t i, uint32_t r, uint32_t u) -> uint32_t {
+                const auto key = std::make_pair(i, ((uint64_t)r << 32) | u);
+                for (auto &kv : mkey)
+                    if (kv.first == key) return kv.second;
+                const asdm_cs &c = *cs[i];
+                mkey.emplace_back(key, (uint32_t)msegs.size());
+                msegs.push_back(MapSeg{c.d_cand + c.cand_base[r], c.d_cand + c.cand_base[u], nullptr, c.ncand[u], 0,
+                                       mtotal});
+                mtotal += c.ncand[r];
+                return (uint32_t)msegs.size() - 1;
+            };
+            for (size_t j = j0; j < j1; ++j) {
+                const PairTerm &t = prep[jobs[j].first].terms[jobs[j].second];
+                if (t.mb == kNone) continue;
+                const uint32_t b = t.block[t.ma];
+                for (uint32_t u : t.members[b])
+                    if (u != t.rep[b]) map_slot(jobs[j].first, t.rep[b], u);
+            }
+            if (mtotal) {
+                if ((rc = dalloc(&d_mapbuf, mtotal, s)) || (rc = dalloc(&d_mseg, msegs.size(), s))) break;
+                for (auto &m : msegs) m.out = d_mapbuf + m.start;
+                if (upload_async(G, d_mseg, msegs.data(), msegs.size() * sizeof(MapSeg)) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "pair-bound map upload failed");
+                    break;
+                }
+                const unsigned grid =
+                    (unsigned)std::min<unsigned long long>((mtotal + 255) / 256, (unsigned long long)G->num_sms * 32);
+                tree_maps<<<grid, 256, 0, s>>>(d_mseg, (uint32_t)msegs.size(), mtotal);
+                ::asdm::count_launch();
+            }
+            if (!fw.empty()) {
+                if ((rc = dalloc(&d_fw, fw.size(), s)) || (rc = dalloc(&d_fh, fh.size(), s))) break;
+                if (upload_async(G, d_fw, fw.data(), fw.size() * sizeof(void *)) != cudaSuccess ||
+                    upload_async(G, d_fh, fh.data(), fh.size() * sizeof(void *)) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "pair-bound indicator upload failed");
+                    break;
+                }
+                fix_weights<<<(unsigned)((fw.size() + 255) / 256), 256, 0, s>>>(d_fw, d_fh, (uint32_t)fw.size(),
+                                                                                  nullptr, 0);
+                ::asdm::count_launch();
+            }
+            // segments by height, children (forest children, then edges into F), roots, one query per term
+            std::vector<std::vector<BoundSeg>> lv;
+            std::vector<BoundChild> kids;
+            std::vector<const uint32_t *> maps;
+            std::vector<const double *> roots;
+            std::vector<uint32_t> nroot;
+            std::vector<BoundQuery> bqs;
+            std::vector<size_t> root0;
+            for (size_t j = j0; j < j1; ++j) {
+                const size_t i = jobs[j].first;
+                const asdm_cs &c = *cs[i];
+                const QueryGraph &q = c.q;
+                const PairPrep &P = prep[i];
+                const PairTerm &t = P.terms[jobs[j].second];
+                const uint32_t up = jobs[j].second > 0 ? 1u : 0u;
+                std::vector<double *> wb(t.nb, nullptr);
+                for (uint32_t b = 0; b < t.nb; ++b)
+                    if (pair_needs_weights(t, b)) {
+                        wb[b] = wbuf + wo;
+                        wo += c.ncand[t.rep[b]];
+                    }
+                auto src_map = [&](uint32_t b, uint32_t u) -> const uint32_t * {
+                    return u == t.rep[b] ? nullptr : d_mapbuf + msegs[map_slot(i, t.rep[b], u)].start;
+                };
+                root0.push_back(roots.size());
+                for (uint32_t b = 0; b < t.nb; ++b) {
+                    if (t.parent[b] == kNone) {
+                        roots.push_back(wb[b]);
+                        nroot.push_back(c.ncand[t.rep[b]]);
+                    }
+                    if (!wb[b]) continue;
+                    const uint32_t r = t.rep[b];
+                    BoundSeg sg{};
+                    sg.w = wb[b];
+                    sg.cand = c.d_cand + c.cand_base[r];
+                    sg.ncand = c.ncand[r];
+                    sg.cls_k = 1;
+                    sg.up = up;
+                    if (t.pin != kNone && t.block[t.pin] == b) {
+                        sg.pin = d_hub + hub0[i] + t.pin_f;
+                        sg.pin_cand = c.d_cand + c.cand_base[P.fvs[t.pin_f]];
+                    }
+                    sg.val_first = (uint32_t)maps.size();
+                    for (uint32_t u : t.members[b])
+                        if (u != r) maps.push_back(src_map(b, u));
+                    sg.nval = (uint32_t)maps.size() - sg.val_first;
+                    sg.child_first = (uint32_t)kids.size();
+                    for (uint32_t C = 0; C < t.nb; ++C) {
+                        if (t.parent[C] != b) continue;
+                        const uint32_t e = t.pedge[C];
+                        kids.push_back(BoundChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e], wb[C],
+                                                  src_map(b, t.pfrom[C])});
+                    }
+                    for (uint32_t u : t.members[b])
+                        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                            const uint32_t f = q.nbr[e];
+                            if (!P.fixed[f]) continue;
+                            kids.push_back(BoundChild{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                                      find[i][f], src_map(b, u)});
+                        }
+                    sg.nchild = (uint32_t)kids.size() - sg.child_first;
+                    if (lv.size() <= t.height[b]) lv.resize(t.height[b] + 1);
+                    lv[t.height[b]].push_back(sg);
+                }
+                BoundQuery bq{};
+                bq.ncomp = (uint32_t)(roots.size() - root0.back());
+                bq.nhub = (uint32_t)P.fvs.size();
+                bq.nedge = nfe[i];
+                bq.up = up;
+                bq.out = d_out + (j - j0);
+                bqs.push_back(bq);
+            }
+            std::vector<BoundSeg> segs;
+            std::vector<size_t> first{0};
+            std::vector<unsigned long long> totals;
+            for (auto &l : lv) {
+                unsigned long long tt = 0;
+                for (BoundSeg &sg : l) {
+                    sg.start = tt;
+                    tt += sg.ncand;
+                    segs.push_back(sg);
+                }
+                first.push_back(segs.size());
+                totals.push_back(tt);
+            }
+            if (kids.empty()) kids.push_back(BoundChild{});
+            if (segs.empty()) segs.push_back(BoundSeg{});
+            if (maps.empty()) maps.push_back(nullptr);
+            if ((rc = dalloc(&d_segs, segs.size(), s)) || (rc = dalloc(&d_kids, kids.size(), s)) ||
+                (rc = dalloc(&d_maps, maps.size(), s)) || (rc = dalloc(&d_roots, roots.size(), s)) ||
+                (rc = dalloc(&d_nroot, nroot.size(), s)) || (rc = dalloc(&d_bq, bqs.size(), s)))
+                break;
+            for (size_t k = 0; k < bqs.size(); ++k) {
+                const size_t i = jobs[j0 + k].first;
+                bqs[k].roots = d_roots + root0[k];
+                bqs[k].nroot = d_nroot + root0[k];
+                bqs[k].hub = d_hub + hub0[i];
+                bqs[k].edge_ok = d_eok + fe0[i];
+            }
+            if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
+                upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
+                upload_async(G, d_maps, maps.data(), maps.size() * sizeof(void *)) != cudaSuccess ||
+                upload_async(G, d_roots, roots.data(), roots.size() * sizeof(void *)) != cudaSuccess ||
+                upload_async(G, d_nroot, nroot.data(), nroot.size() * sizeof(uint32_t)) != cudaSuccess ||
+                upload_async(G, d_bq, bqs.data(), bqs.size() * sizeof(BoundQuery)) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "pair-bound upload failed");
+                break;
+            }
+            for (size_t h = 0; h < totals.size() && rc == ASDM_OK; ++h) {
+                if (!totals[h]) continue;
+                const unsigned grid =
+                    (unsigned)std::min<unsigned long long>((totals[h] + 255) / 256, (unsigned long long)G->num_sms * 32);
+                bound_level<<<grid, 256, 0, s>>>(d_segs + first[h], (uint32_t)(first[h + 1] - first[h]), totals[h],
+                                                 d_kids, d_maps);
+                ::asdm::count_launch();
+                if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "pair-bound kernel failed");
+            }
+            if (rc != ASDM_OK) break;
+            bound_queries<<<(unsigned)bqs.size(), 256, 0, s>>>(d_bq);
+            ::asdm::count_launch();
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(vals.data() + j0, d_out, (j1 - j0) * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "pair-bound readback failed");
+                break;
+            }
+        } while (false);
+        dfree(wbuf, s);
+        dfree(d_out, s);
+        dfree(d_mapbuf, s);
+        dfree(d_mseg, s);
+        dfree(d_segs, s);
+        dfree(d_kids, s);
+        dfree(d_maps, s);
+        dfree(d_roots, s);
+        dfree(d_nroot, s);
+        dfree(d_bq, s);
+        dfree(d_fw, s);
+        dfree(d_fh, s);
+        cudaStreamSynchronize(s);
+    }
+    return rc;
+}
+
+// lb[i] = the pair bound of each query with want[i] (0 where none is formed;
+// without all_terms, also where H alone shows that it stays below 2^64).
+int pair_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<char> &want,
+                std::vector<double> &lb, bool all_terms) {
+    cudaStream_t s = G->stream;
+    const size_t Q = cs.size();
+    const double two64 = 18446744073709551616.0;
+    lb.assign(Q, 0.0);
+    std::vector<PairPrep> prep(Q);
+    std::vector<char> ok(Q, 0);
+    for (size_t i = 0; i < Q; ++i) {
+        const asdm_cs &c = *cs[i];
+        const QueryGraph &q = c.q;
+        if (!want[i] || !c.nonempty || q.n < 2) continue;
+        PairPrep &P = prep[i];
+        const uint32_t n = q.n;
+        greedy_fvs(q, P.fixed, P.fvs);
+        if (P.fvs.size() > kMaxFixed || P.fvs.size() == n) continue;
+        // classes among F: the r-th of F's k vertices with one label (in F's order) takes class r
+        P.fk.assign(P.fvs.size(), 0);
+        P.fc.assign(P.fvs.size(), 0);
+        for (size_t j = 0; j < P.fvs.size(); ++j)
+            for (size_t j2 = 0; j2 < P.fvs.size(); ++j2)
+                if (q.lab[P.fvs[j2]] == q.lab[P.fvs[j]]) {
+                    P.fc[j] += j2 < j;
+                    ++P.fk[j];
+                }
+        for (uint32_t f : P.fvs) P.fwords += c.ncand[f];
+        std::vector<uint32_t> fpos(n, kNone);
+        for (size_t j = 0; j < P.fvs.size(); ++j) fpos[P.fvs[j]] = (uint32_t)j;
+        P.terms.emplace_back();
+        for (uint32_t a = 0; a < n; ++a)
+            for (uint32_t b = a + 1; b < n; ++b) {
+                if (q.lab[a] != q.lab[b] || q.slot(a, b) >= 0 || (P.fixed[a] && P.fixed[b])) continue;
+                PairTerm t;
+                if (P.fixed[a]) {
+                    t.pin = b;
+                    t.pin_f = fpos[a];
+                } else if (P.fixed[b]) {
+                    t.pin = a;
+                    t.pin_f = fpos[b];
+                } else {
+                    t.ma = a;
+                    t.mb = b;
+                }
+                P.terms.push_back(std::move(t));
+            }
+        if (P.terms.size() == 1) continue;  // no pairs: the plain forest program counts embeddings
+        for (PairTerm &t : P.terms) pair_forest(q, P.fixed, c, t);
+        ok[i] = 1;
+    }
+    std::vector<std::vector<uint32_t>> excl(Q);
+    int rc = ASDM_OK;
+    for (uint32_t round = 0; round < kHubRounds && rc == ASDM_OK; ++round) {
+        std::vector<size_t> ids;
+        for (size_t i = 0; i < Q; ++i)
+            if (ok[i] && lb[i] < two64 && (round == 0 || (!prep[i].fvs.empty() && excl[i].size() == round)))
+                ids.push_back(i);
+        if (ids.empty()) break;
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = fail(ASDM_ERR_CUDA, "pair-bound sync failed");
+            break;
+        }
+        G->stage.reset();
+        // the round's hubs and the checks of the edges inside F
+        std::vector<uint32_t> hub0(Q, 0), fe0(Q, 0), nfe(Q, 0);
+        std::vector<HubSeg> hsegs;
+        std::vector<FixEdge> fedges;
+        uint32_t nhub = 0;
+        for (size_t i : ids) {
+            hub0[i] = nhub;
+            nhub += (uint32_t)prep[i].fvs.size();
+        }
+        uint32_t *d_hub = nullptr, *d_eok = nullptr;
+        HubSeg *d_hsegs = nullptr;
+        FixEdge *d_fe = nullptr;
+        do {
+            if ((rc = dalloc(&d_hub, std::max<uint32_t>(nhub, 1), s))) break;
+            for (size_t i : ids) {
+                const asdm_cs &c = *cs[i];
+                const PairPrep &P = prep[i];
+                for (size_t j = 0; j < P.fvs.size(); ++j) {
+                    const uint32_t f = P.fvs[j];
+                    HubSeg hs{c.d_cand + c.cand_base[f], c.ncand[f], P.fk[j], P.fc[j], 0, d_hub + hub0[i] + j, {}};
+                    if (j == 0)
+                        for (uint32_t x : excl[i]) hs.ex[hs.nex++] = x;
+                    hsegs.push_back(hs);
+                }
+                fe0[i] = (uint32_t)fedges.size();
+                for (size_t j = 0; j < P.fvs.size(); ++j)
+                    for (size_t j2 = j + 1; j2 < P.fvs.size(); ++j2) {
+                        const int sl = c.q.slot(P.fvs[j], P.fvs[j2]);
+                        if (sl < 0) continue;
+                        const uint32_t e = c.q.off[P.fvs[j]] + (uint32_t)sl;
+                        fedges.push_back(FixEdge{c.d_eoff + c.eoff_base[e], c.d_elist + c.elist_base[e],
+                                                 d_hub + hub0[i] + j, d_hub + hub0[i] + j2, nullptr});
+                    }
+                nfe[i] = (uint32_t)fedges.size() - fe0[i];
+            }
+            const uint32_t ne = (uint32_t)fedges.size();
+            if ((rc = dalloc(&d_eok, std::max<uint32_t>(ne, 1), s))) break;
+            for (uint32_t e = 0; e < ne; ++e) fedges[e].ok = d_eok + e;
+            if (!hsegs.empty()) {
+                if ((rc = dalloc(&d_hsegs, hsegs.size(), s))) break;
+                if (upload_async(G, d_hsegs, hsegs.data(), hsegs.size() * sizeof(HubSeg)) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "pair-bound hub upload failed");
+                    break;
+                }
+                pick_hubs<<<(unsigned)hsegs.size(), 256, 0, s>>>(d_hsegs, G->d.off);
+                ::asdm::count_launch();
+            }
+            if (ne) {
+                if ((rc = dalloc(&d_fe, ne, s))) break;
+                if (upload_async(G, d_fe, fedges.data(), ne * sizeof(FixEdge)) != cudaSuccess) {
+                    rc = fail(ASDM_ERR_CUDA, "pair-bound edge upload failed");
+                    break;
+                }
+                fix_weights<<<(ne + 255) / 256, 256, 0, s>>>(nullptr, nullptr, 0, d_fe, ne);
+                ::asdm::count_launch();
+            }
+            std::vector<uint32_t> hubs(std::max<uint32_t>(nhub, 1));
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(hubs.data(), d_hub, hubs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = fail(ASDM_ERR_CUDA, "pair-bound hub readback failed");
+                break;
+            }
+            // H of every query of the round, then the T terms where H could settle it
+            std::vector<std::pair<size_t, uint32_t>> jobs;
+            for (size_t i : ids) jobs.emplace_back(i, 0u);
+            std::vector<double> hv;
+            if ((rc = pair_values(G, cs, prep, jobs, d_hub, hub0, d_eok, fe0, nfe, hv))) break;
+            std::vector<double> H(Q, 0.0);
+            jobs.clear();
+            for (size_t k = 0; k < ids.size(); ++k) {
+                const size_t i = ids[k];
+                H[i] = hv[k];
+                if (!prep[i].fvs.empty() && hubs[hub0[i]] != kNone) excl[i].push_back(hubs[hub0[i]]);
+                if (H[i] > 0 && (all_terms || lb[i] + H[i] >= two64))
+                    for (uint32_t t = 1; t < prep[i].terms.size(); ++t) jobs.emplace_back(i, t);
+            }
+            std::vector<double> tv;
+            if ((rc = pair_values(G, cs, prep, jobs, d_hub, hub0, d_eok, fe0, nfe, tv))) break;
+            std::vector<double> S(Q, 0.0);
+            for (size_t k = 0; k < jobs.size(); ++k) S[jobs[k].first] = std::nextafter(S[jobs[k].first] + tv[k], HUGE_VAL);
+            for (size_t k = 0; k < jobs.size(); ++k) {
+                const size_t i = jobs[k].first;
+                if (k + 1 < jobs.size() && jobs[k + 1].first == i) continue;  // once per query, at its last term
+                const double b = std::nextafter(H[i] - S[i], -HUGE_VAL);
+                if (b > 0) lb[i] = lb[i] == 0.0 ? b : std::nextafter(lb[i] + b, 0.0);
+            }
+        } while (false);
+        dfree(d_hub, s);
+        dfree(d_eok, s);
+        dfree(d_hsegs, s);
+        dfree(d_fe, s);
+        cudaStreamSynchronize(s);
+    }
+    if (rc != ASDM_OK) lb.assign(Q, 0.0);
+    return rc;
+}
+
 }  // namespace
 
 // proven[i] = 1 when query i's count is shown to be at least 2^64 (see the
@@ -1350,33 +1918,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
         if (!c.nonempty || q.n < 2 || proven[i]) continue;
         Prep &P = prep[i];
         const uint32_t n = q.n;
-        // feedback vertex set: peel vertices of degree <= 1, fix the busiest
-        P.fixed.assign(n, 0);
-        std::vector<char> gone(n, 0);
-        std::vector<uint32_t> deg(n);
-        for (uint32_t u = 0; u < n; ++u) deg[u] = q.deg(u);
-        for (;;) {
-            bool changed = true;
-            while (changed) {
-                changed = false;
-                for (uint32_t u = 0; u < n; ++u)
-                    if (!gone[u] && deg[u] <= 1) {
-                        gone[u] = 1;
-                        changed = true;
-                        for (uint32_t e = q.off[u]; e < q.off[u + 1]; ++e)
-                            if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
-                    }
-            }
-            uint32_t best = kNone;
-            for (uint32_t u = 0; u < n; ++u)
-                if (!gone[u] && (best == kNone || deg[u] > deg[best])) best = u;
-            if (best == kNone) break;
-            P.fixed[best] = 1;
-            P.fvs.push_back(best);
-            gone[best] = 1;
-            for (uint32_t e = q.off[best]; e < q.off[best + 1]; ++e)
-                if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
-        }
+        greedy_fvs(q, P.fixed, P.fvs);
         if (P.fvs.size() > kMaxFixed || P.fvs.size() == n) continue;
         // classes: greedy colouring of each label's conflict graph
         P.cls_k.assign(n, 1);
@@ -1675,6 +2217,19 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
         dfree(d_roots, s);
         cudaStreamSynchronize(s);
     }
+    }
+    // the pair bounds for what is still open
+    if (rc == ASDM_OK) {
+        std::vector<char> want(Q, 0);
+        for (size_t i = 0; i < Q; ++i) want[i] = !proven[i];
+        std::vector<double> plb;
+        rc = pair_bounds(G, cs, want, plb, lower != nullptr);
+        if (rc == ASDM_OK)
+            for (size_t i = 0; i < Q; ++i) {
+                if (!want[i] || plb[i] <= 0) continue;
+                proven[i] = plb[i] >= two64;
+                if (lower) (*lower)[i] = std::max<uint64_t>((*lower)[i], proven[i] ? ~0ull : (uint64_t)plb[i]);
+            }
     }
     if (rc != ASDM_OK) {
         proven.assign(Q, 0);

@@ -746,6 +746,177 @@ int lower_bound(const OGraph &q, const OGraph &g, const CandSpace &cs, unsigned 
     return 0;
 }
 
+// The device's pair bound, restated for its first round of hubs: F as in
+// lower_bound, each vertex of F on the largest-degree candidate of its class,
+// classes now only among F's same-label vertices (the r-th of k in F's order
+// takes class r); H = the homomorphisms with F on its hubs; for every
+// same-label, non-adjacent pair not both in F, T = the homomorphisms with one
+// of them pinned to the other's hub (one in F) or with the two merged into one
+// block on the candidates of both, the forest of the merged query built
+// breadth-first (blocks in order of their lowest member, from the lowest
+// unvisited one, members in id order, neighbours in adjacency order, an edge
+// into a visited block left out).  bound = H - sum T when positive.  Exact
+// 128-bit integers (a saturated T sum gives no bound).  Returns false when no
+// bound is formed.
+bool pair_bound(const OGraph &q, const OGraph &g, const CandSpace &cs, unsigned __int128 &out) {
+    const uint32_t n = q.n;
+    const unsigned __int128 kSat = (unsigned __int128)1 << 127;
+    auto sat_mul = [&](unsigned __int128 a, unsigned __int128 b) -> unsigned __int128 {
+        if (a == 0 || b == 0) return 0;
+        if (a >= kSat || b >= kSat || a > kSat / b) return kSat;
+        return a * b;
+    };
+    auto sat_add = [&](unsigned __int128 a, unsigned __int128 b) -> unsigned __int128 {
+        return (a >= kSat || b >= kSat || a + b >= kSat) ? kSat : a + b;
+    };
+    out = 0;
+    // F: peel leaves, fix the vertex of highest remaining degree
+    std::vector<char> fixed(n, 0), gone(n, 0);
+    std::vector<uint32_t> fvs, deg(n);
+    for (uint32_t u = 0; u < n; ++u) deg[u] = q.deg(u);
+    auto drop = [&](uint32_t u) {
+        gone[u] = 1;
+        for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e)
+            if (!gone[q.nbr[e]]) --deg[q.nbr[e]];
+    };
+    for (;;) {
+        for (bool changed = true; changed;) {
+            changed = false;
+            for (uint32_t u = 0; u < n; ++u)
+                if (!gone[u] && deg[u] <= 1) { drop(u); changed = true; }
+        }
+        int best = -1;
+        for (uint32_t u = 0; u < n; ++u)
+            if (!gone[u] && (best < 0 || deg[u] > deg[best])) best = (int)u;
+        if (best < 0) break;
+        fixed[best] = 1;
+        fvs.push_back((uint32_t)best);
+        drop((uint32_t)best);
+    }
+    if (fvs.size() > 6 || fvs.size() == n) return false;
+    std::vector<uint32_t> hub(n, UINT32_MAX);
+    for (size_t j = 0; j < fvs.size(); ++j) {
+        uint32_t c = 0, k = 0;
+        for (size_t j2 = 0; j2 < fvs.size(); ++j2)
+            if (q.lab[fvs[j2]] == q.lab[fvs[j]]) {
+                if (j2 < j) ++c;
+                ++k;
+            }
+        const uint32_t f = fvs[j];
+        for (uint32_t v : cs.C[f])
+            if ((k <= 1 || vertex_class(v, k) == c) && (hub[f] == UINT32_MAX || g.deg(v) > g.deg(hub[f]))) hub[f] = v;
+        if (hub[f] == UINT32_MAX) return false;
+    }
+    for (uint32_t f : fvs)
+        for (uint32_t f2 : fvs)
+            if (f < f2 && q.adjacent(f, f2) && !g.adjacent(hub[f], hub[f2])) return false;
+    // the homomorphisms of one program
+    auto count = [&](uint32_t ma, uint32_t mb, uint32_t pin, uint32_t pinv) -> unsigned __int128 {
+        std::vector<uint32_t> block(n, UINT32_MAX);
+        std::vector<std::vector<uint32_t>> members;
+        for (uint32_t u = 0; u < n; ++u) {
+            if (fixed[u] || u == mb) continue;
+            block[u] = (uint32_t)members.size();
+            members.push_back({u});
+        }
+        if (mb != UINT32_MAX) {
+            block[mb] = block[ma];
+            members[block[ma]].push_back(mb);
+            std::sort(members[block[ma]].begin(), members[block[ma]].end());
+        }
+        const uint32_t nb = (uint32_t)members.size();
+        std::vector<std::vector<uint32_t>> cand(nb);
+        for (uint32_t b = 0; b < nb; ++b) {
+            cand[b] = cs.C[members[b][0]];
+            for (size_t k = 1; k < members[b].size(); ++k) {
+                std::vector<uint32_t> t;
+                const auto &o = cs.C[members[b][k]];
+                std::set_intersection(cand[b].begin(), cand[b].end(), o.begin(), o.end(), std::back_inserter(t));
+                cand[b].swap(t);
+            }
+            if (pin != UINT32_MAX && block[pin] == b) {
+                const bool has = std::binary_search(cand[b].begin(), cand[b].end(), pinv);
+                cand[b].clear();
+                if (has) cand[b].push_back(pinv);
+            }
+        }
+        // breadth-first forest; the tree edge into block C leaves member pfrom[C] for vertex crep[C]
+        std::vector<uint32_t> parent(nb, UINT32_MAX), pfrom(nb, UINT32_MAX), crep(nb, UINT32_MAX), order;
+        std::vector<char> seen(nb, 0);
+        for (uint32_t r = 0; r < nb; ++r) {
+            if (seen[r]) continue;
+            seen[r] = 1;
+            const size_t first = order.size();
+            order.push_back(r);
+            for (size_t k = first; k < order.size(); ++k) {
+                const uint32_t B = order[k];
+                for (uint32_t u : members[B])
+                    for (uint64_t e = q.off[u]; e < q.off[u + 1]; ++e) {
+                        const uint32_t w = q.nbr[e];
+                        if (fixed[w]) continue;
+                        const uint32_t C = block[w];
+                        if (C == B || seen[C]) continue;
+                        seen[C] = 1;
+                        parent[C] = B;
+                        pfrom[C] = u;
+                        crep[C] = w;
+                        order.push_back(C);
+                    }
+            }
+        }
+        std::vector<std::vector<unsigned __int128>> wt(nb);
+        for (size_t k = order.size(); k-- > 0;) {
+            const uint32_t B = order[k];
+            wt[B].assign(cand[B].size(), 0);
+            for (size_t i = 0; i < cand[B].size(); ++i) {
+                const uint32_t v = cand[B][i];
+                unsigned __int128 acc = 1;
+                for (uint32_t u : members[B])
+                    for (uint64_t e = q.off[u]; e < q.off[u + 1] && acc; ++e) {
+                        const uint32_t w = q.nbr[e];
+                        if (fixed[w]) {
+                            if (!g.adjacent(v, hub[w])) acc = 0;
+                            continue;
+                        }
+                        const uint32_t C = block[w];
+                        if (parent[C] != B || pfrom[C] != u || crep[C] != w) continue;
+                        uint64_t s0, s1;
+                        g.run(v, q.lab[w], s0, s1);
+                        unsigned __int128 sum = 0;
+                        for (uint64_t j = s0; j < s1; ++j) {
+                            const auto it = std::lower_bound(cand[C].begin(), cand[C].end(), g.nbr[j]);
+                            if (it != cand[C].end() && *it == g.nbr[j]) sum = sat_add(sum, wt[C][it - cand[C].begin()]);
+                        }
+                        acc = sat_mul(acc, sum);
+                    }
+                wt[B][i] = acc;
+            }
+        }
+        unsigned __int128 prod = 1;
+        for (uint32_t b = 0; b < nb; ++b) {
+            if (parent[b] != UINT32_MAX) continue;
+            unsigned __int128 tot = 0;
+            for (auto x : wt[b]) tot = sat_add(tot, x);
+            prod = sat_mul(prod, tot);
+        }
+        return prod;
+    };
+    const unsigned __int128 H = count(UINT32_MAX, UINT32_MAX, UINT32_MAX, 0);
+    unsigned __int128 S = 0;
+    bool pairs = false;
+    for (uint32_t a = 0; a < n; ++a)
+        for (uint32_t b = a + 1; b < n; ++b) {
+            if (q.lab[a] != q.lab[b] || q.adjacent(a, b) || (fixed[a] && fixed[b])) continue;
+            pairs = true;
+            if (fixed[a]) S = sat_add(S, count(UINT32_MAX, UINT32_MAX, b, hub[a]));
+            else if (fixed[b]) S = sat_add(S, count(UINT32_MAX, UINT32_MAX, a, hub[b]));
+            else S = sat_add(S, count(a, b, UINT32_MAX, 0));
+        }
+    if (!pairs || S >= kSat) return false;
+    out = H > S ? H - S : 0;
+    return true;
+}
+
 struct RunResult {
     uint64_t count = 0;
     bool overflow = false;
@@ -843,9 +1014,10 @@ int orc_tree_list(const char *dpath, const char *list) {
 }
 
 // The lower bounds of the queries of a list file against one data graph:
-// "B <k> <bound>" (decimal, saturated at 2^127; for trees the larger of the
-// general bound and the far-class tree bound), "B <k> none" when the rules form
-// no bound, "B <k> empty" for an empty candidate set.
+// "B <k> <bound>" (decimal, saturated at 2^127; the largest of the general
+// bound, for trees the far-class tree bound, and the first-round pair bound),
+// "B <k> none" when the rules form no bound, "B <k> empty" for an empty
+// candidate set.
 int orc_bound_list(const char *dpath, const char *list) {
     OGraph g;
     if (!load_graph(dpath, g)) return 2;
@@ -860,12 +1032,14 @@ int orc_bound_list(const char *dpath, const char *list) {
             std::cout << "B " << k << " empty" << std::endl;
             continue;
         }
-        unsigned __int128 lb = 0, tb = 0;
+        unsigned __int128 lb = 0, tb = 0, pb = 0;
         const bool general = lower_bound(q, g, cs, lb) == 0;
-        // the device reports the larger of its two bounds
+        // the device reports the largest of its bounds
         const bool tree = tree_class_bound(q, g, cs, tb);
         if (tree && tb > lb) lb = tb;
-        if (!general && !tree) {
+        const bool pair = pair_bound(q, g, cs, pb);
+        if (pair && pb > lb) lb = pb;
+        if (!general && !tree && !pair) {
             std::cout << "B " << k << " none" << std::endl;
             continue;
         }

@@ -2,6 +2,7 @@
 
     python tests/golden/make_c2_golden.py reference [--cap S] [--jobs J] [--sizes LO-HI]
     python tests/golden/make_c2_golden.py oracle [--jobs J]
+    python tests/golden/make_c2_golden.py bounds [--jobs J]
 
 The config-2 batch is the first 1,000 random-walk queries (seeds 50,000 + i,
 sizes uniform in 4..32) on the config-1 graph.  Inputs are written by the
@@ -17,6 +18,7 @@ host-only generator (asdmatch_b200/bin/asdm_gen.out) into --workdir.
   count of 2^64 or more, or "skip" where a quotient has a cycle); and on the
   parity set (two queries of every size 7..32, "parity") its restatement of
   the device's overflow lower bound ("oracle_bound").
+* bounds: the oracle's lower bounds of the parity set alone.
 
 Runs merge into the same file (a finished reference count is never replaced
 by a later timeout).  --reuse DIR merges the outputs a previous run of the
@@ -148,29 +150,40 @@ def run_oracle_lists(dpath, lists, flag, jobs):
     return [p.communicate()[0] for p in procs]
 
 
+def write_list(path, workdir, idx):
+    with open(path, "w") as fh:
+        fh.write("\n".join(os.path.join(workdir, "q%d.graph" % i) for i in idx) + "\n")
+    return path
+
+
+def run_bounds(args, S, data):
+    """asdm_oracle -b on the parity set, split over --jobs processes."""
+    par = parity_set(S)
+    dpath = write_inputs(S, args.workdir, par)
+    jobs = max(1, min(args.jobs, len(par)))
+    parts = [par[k::jobs] for k in range(jobs)]
+    lists = [write_list(os.path.join(args.workdir, "parity_list_%d.txt" % k), args.workdir, part)
+             for k, part in enumerate(parts)]
+    for part, text in zip(parts, run_oracle_lists(dpath, lists, "-b", jobs)):
+        for line in text.splitlines():
+            f = line.split()
+            if len(f) == 3 and f[0] == "B":
+                record(data, S, part[int(f[1])])["oracle_bound"] = f[2]
+
+
 def run_oracle(args, S, data):
     idx = list(range(S.C2_QUERIES))
     dpath = write_inputs(S, args.workdir, idx)
     trees = [i for i in idx if is_tree(os.path.join(args.workdir, "q%d.graph" % i))]
-    par = parity_set(S)
     jobs = max(1, args.jobs)
     if args.reuse:
         outs = [(json.load(open(os.path.join(args.reuse, "tree_list_%d.json" % k))),
                  open(os.path.join(args.reuse, "tree_out_%d.txt" % k)).read()) for k in range(jobs)]
-        bounds = (par, open(os.path.join(args.reuse, "parity_bounds.txt")).read())
     else:
         parts = [trees[k::jobs] for k in range(jobs)]
-        lists = []
-        for k, part in enumerate(parts):
-            lst = os.path.join(args.workdir, "tree_list_%d.txt" % k)
-            with open(lst, "w") as fh:
-                fh.write("\n".join(os.path.join(args.workdir, "q%d.graph" % i) for i in part) + "\n")
-            lists.append(lst)
+        lists = [write_list(os.path.join(args.workdir, "tree_list_%d.txt" % k), args.workdir, part)
+                 for k, part in enumerate(parts)]
         outs = list(zip(parts, run_oracle_lists(dpath, lists, "-t", jobs)))
-        blst = os.path.join(args.workdir, "parity_list.txt")
-        with open(blst, "w") as fh:
-            fh.write("\n".join(os.path.join(args.workdir, "q%d.graph" % i) for i in par) + "\n")
-        bounds = (par, run_oracle_lists(dpath, [blst], "-b", 1)[0])
     for part, text in outs:
         for line in text.splitlines():
             f = line.split()
@@ -179,16 +192,12 @@ def run_oracle(args, S, data):
             rec = record(data, S, part[int(f[1])])
             rec["oracle_tree"] = int(f[3]) if f[2] == "ok" else ("overflow" if f[2] == "overflow" else
                                                                   (0 if f[2] == "empty" else "skip"))
-    part, text = bounds
-    for line in text.splitlines():
-        f = line.split()
-        if len(f) == 3 and f[0] == "B":
-            record(data, S, part[int(f[1])])["oracle_bound"] = f[2]
+    run_bounds(args, S, data)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["reference", "oracle"])
+    ap.add_argument("step", choices=["reference", "oracle", "bounds"])
     ap.add_argument("--cap", type=float, default=60.0)
     ap.add_argument("--jobs", type=int, default=max(1, (os.cpu_count() or 2) - 2))
     ap.add_argument("--sizes", default="4-32")
@@ -199,6 +208,8 @@ def main():
     data = load()
     if args.step == "reference":
         run_reference(args, S, data)
+    elif args.step == "bounds":
+        run_bounds(args, S, data)
     else:
         run_oracle(args, S, data)
     save(data, S)

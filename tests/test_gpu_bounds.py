@@ -146,3 +146,51 @@ def test_tree_bound_is_the_exact_count_without_far_pairs(golden, c0_files, c0d_f
                 below += 1
         dg.close()
     assert exact_checked >= 30 and below >= 1, (exact_checked, below)
+
+
+def _broom_graph(m, p):
+    # hub 0 (label 0) joined to m vertices of label 2, each joined to p vertices of label 1 of its own
+    n = 1 + m + m * p
+    labels = [0] + [2] * m + [1] * (m * p)
+    edges = [(0, 1 + i) for i in range(m)]
+    edges += [(1 + i, 1 + m + i * p + j) for i in range(m) for j in range(p)]
+    return A.HostGraph.from_edges(n, labels, edges)
+
+
+def _broom_query(k):
+    # centre (label 0), k children (label 2), one leaf (label 1) under each: the leaves are four edges apart
+    labels = [0] + [2] * k + [1] * k
+    edges = [(0, 1 + i) for i in range(k)] + [(1 + i, 1 + k + i) for i in range(k)]
+    return A.HostGraph.from_edges(2 * k + 1, labels, edges)
+
+
+def test_pair_bound_proves_what_classes_cannot():
+    """Brooms: the exact count falling(m, 4) * p^4 = 1.55e21 is above 2^64,
+    but a bound that keeps the four far-apart leaves on four hash classes of
+    candidates keeps about 1/256 of it (6e18, below 2^64).  The first-order
+    pair bound (homomorphisms minus those that join a same-label pair) loses
+    only a few percent and proves the overflow; on a small broom it stays
+    below the exact count."""
+    m, p, k = 200, 1000, 4
+    exact = _falling(m, k) * p ** k
+    assert exact >= TWO64 and exact // 256 < TWO64
+    dg = A.DeviceGraph(_broom_graph(m, p))
+    q = _broom_query(k)
+    cs = A.CandidateSpace(dg, q)
+    lb, exceeds = cs.count_lower_bound()
+    cs.close()
+    assert exceeds and lb == TWO64 - 1
+    counts, status = A.run_batch(dg, [q])
+    assert status.tolist() == [A.ERR_OVERFLOW]
+    dg.close()
+    m, p = 40, 30
+    dg = A.DeviceGraph(_broom_graph(m, p))
+    cs = A.CandidateSpace(dg, q)
+    lb, exceeds = cs.count_lower_bound()
+    exact = _falling(m, k) * p ** k
+    # H = m^4 p^4, minus 6 merged sibling pairs (m^3 p^4 each) and 6 merged leaf pairs (m^4 p^3 each)
+    want = m ** 4 * p ** 4 - 6 * m ** 3 * p ** 4 - 6 * m ** 4 * p ** 3
+    assert not exceeds and want * (1 - 1e-12) <= lb <= exact, (lb, want, exact)
+    assert A.adaptive_share_join(cs).count == exact
+    cs.close()
+    dg.close()
