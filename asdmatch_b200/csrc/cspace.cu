@@ -1159,8 +1159,8 @@ int build_batch(const std::vector<asdm_cs *> &group) {
         ASDM_TRY(scan_exclusive_u32(arena->d_eoff, d_upos, nitems, true, s));
         ASDM_CUDA(cudaMemcpyAsync(&bound, d_upos + nitems, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         ASDM_CUDA(cudaStreamSynchronize(s));
-        // padded lists up to 2^padded_cap_log2 entries in total (default 2^32:
-        // 16 GiB), the exact two-scan form beyond
+        // padded lists up to 2^padded_cap_log2 entries in total (default 2^33:
+        // 32 GiB), the exact two-scan form beyond
         const uint64_t padded_cap = 1ull << G->tuning.padded_cap_log2;
         two_scan = bound > padded_cap;
         if (bound <= padded_cap) {

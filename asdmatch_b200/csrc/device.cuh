@@ -164,7 +164,7 @@ struct PinnedStage {
 };
 
 struct asdm_graph {
-    asdm_tuning tuning{1, 96, ASDM_PLANNER_DP, 64, 32};         // kernel knobs (asdm_graph_set_tuning)
+    asdm_tuning tuning{1, 96, ASDM_PLANNER_DP, 64, 33};         // kernel knobs (asdm_graph_set_tuning)
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;

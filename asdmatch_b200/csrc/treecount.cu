@@ -929,32 +929,34 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
 
 // A query's bound: for each component, the sum of its root's weights; the
 // product over components; 0 when a fixed vertex has no candidate of its
-// class or an edge between fixed vertices is missing.  One block per query.
+// class or an edge between fixed vertices is missing.  The sums run in two
+// steps: bound_parts sums kRootSlices slices of every root array (one block
+// per slice), bound_queries adds a query's slices in order and multiplies.
+constexpr uint32_t kRootSlices = 32;
+
 struct BoundQuery {
     const double *const *roots;  // root weight arrays of the components
     const uint32_t *nroot;       // their lengths
     uint32_t ncomp, nhub, nedge, up;  // up = 1: sums and products rounded up (else toward zero)
     const uint32_t *hub;         // chosen hub indices of the fixed vertices
     const uint32_t *edge_ok;     // checks of the edges inside F
+    double *part;                // ncomp * kRootSlices slice sums (set by attach_parts)
     double *out;
 };
 
-__global__ void bound_queries(const BoundQuery *__restrict__ qs) {
-    const BoundQuery bq = qs[blockIdx.x];
+// Block (slice, query): the slice's share of every component's root sum.
+__global__ void bound_parts(const BoundQuery *__restrict__ qs) {
+    const BoundQuery bq = qs[blockIdx.y];
     const bool up = bq.up != 0;
     __shared__ double red[32];
-    __shared__ double prod;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) / 32;
-    if (threadIdx.x == 0) {
-        prod = 1.0;
-        for (uint32_t k = 0; k < bq.nhub; ++k) prod = bq.hub[k] == kNone ? 0.0 : prod;
-        for (uint32_t k = 0; k < bq.nedge; ++k) prod = bq.edge_ok[k] ? prod : 0.0;
-    }
-    __syncthreads();
     for (uint32_t c = 0; c < bq.ncomp; ++c) {
+        const uint32_t n = bq.nroot[c];
+        const uint32_t per = (n + kRootSlices - 1) / kRootSlices;
+        const uint32_t lo = min(n, blockIdx.x * per), hi = min(n, lo + per);
         double part = 0.0;
         const double *w = bq.roots[c];
-        for (uint32_t i = threadIdx.x; i < bq.nroot[c]; i += blockDim.x) part = dadd(part, w[i], up);
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) part = dadd(part, w[i], up);
 #pragma unroll
         for (int o = 16; o; o >>= 1) part = dadd(part, __shfl_xor_sync(0xffffffffu, part, o), up);
         if (lane == 0) red[warp] = part;
@@ -962,11 +964,52 @@ __global__ void bound_queries(const BoundQuery *__restrict__ qs) {
         if (threadIdx.x == 0) {
             double tot = 0.0;
             for (uint32_t k = 0; k < nw; ++k) tot = dadd(tot, red[k], up);
-            prod = dmul(prod, tot, up);
+            bq.part[c * kRootSlices + blockIdx.x] = tot;
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) *bq.out = prod;
+}
+
+// One thread per query.
+__global__ void bound_queries(const BoundQuery *__restrict__ qs, uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const BoundQuery bq = qs[t];
+    const bool up = bq.up != 0;
+    double prod = 1.0;
+    for (uint32_t k = 0; k < bq.nhub; ++k) prod = bq.hub[k] == kNone ? 0.0 : prod;
+    for (uint32_t k = 0; k < bq.nedge; ++k) prod = bq.edge_ok[k] ? prod : 0.0;
+    for (uint32_t c = 0; c < bq.ncomp; ++c) {
+        double tot = 0.0;
+        for (uint32_t k = 0; k < kRootSlices; ++k) tot = dadd(tot, bq.part[c * kRootSlices + k], up);
+        prod = dmul(prod, tot, up);
+    }
+    *bq.out = prod;
+}
+
+// Slice-sum storage for the queries' components: one device buffer (*d_part,
+// freed by the caller) that each BoundQuery's part points into.
+int attach_parts(std::vector<BoundQuery> &bqs, double **d_part, cudaStream_t s) {
+    uint64_t total = 0;
+    for (const BoundQuery &bq : bqs) total += (uint64_t)bq.ncomp * kRootSlices;
+    ASDM_TRY(dalloc(d_part, std::max<uint64_t>(total, 1), s));
+    uint64_t at = 0;
+    for (BoundQuery &bq : bqs) {
+        bq.part = *d_part + at;
+        at += (uint64_t)bq.ncomp * kRootSlices;
+    }
+    return ASDM_OK;
+}
+
+// The two launches of a set of queries' bounds (descriptors on the device).
+void launch_bound_queries(const BoundQuery *d_bq, uint32_t n, cudaStream_t s) {
+    if (!n) return;
+    for (uint32_t at = 0; at < n; at += 65535u) {  // grid y is at most 65535
+        bound_parts<<<dim3(kRootSlices, std::min(65535u, n - at)), 256, 0, s>>>(d_bq + at);
+        ::asdm::count_launch();
+    }
+    bound_queries<<<(n + 127) / 128, 128, 0, s>>>(d_bq, n);
+    ::asdm::count_launch();
 }
 
 // The inclusion-exclusion sum of a query's terms, rounded down: terms with a
@@ -1000,12 +1043,19 @@ struct HubSeg {
     uint32_t ex[kHubRounds - 1];   // indices chosen in earlier rounds (skipped)
 };
 
-// One block per segment: the candidate of the segment's class with the
-// largest data degree (ties: the smaller index), other than the excluded ones.
-__global__ void pick_hubs(const HubSeg *__restrict__ segs, const uint32_t *__restrict__ goff) {
-    const HubSeg sg = segs[blockIdx.x];
+// The candidate of each segment's class with the largest data degree (ties:
+// the smaller index), other than the excluded ones: block (slice, segment)
+// takes the best key (set bit 63, degree, inverted index) of its slice of
+// C(f) into keys[segment] (zeroed before), hub_decode turns it into an index.
+constexpr uint32_t kHubSlices = 16;
+
+__global__ void pick_hubs(const HubSeg *__restrict__ segs, const uint32_t *__restrict__ goff,
+                          unsigned long long *__restrict__ keys) {
+    const HubSeg sg = segs[blockIdx.y];
+    const uint32_t per = (sg.ncand + kHubSlices - 1) / kHubSlices;
+    const uint32_t lo = min(sg.ncand, blockIdx.x * per), hi = min(sg.ncand, lo + per);
     unsigned long long best = 0;
-    for (uint32_t i = threadIdx.x; i < sg.ncand; i += blockDim.x) {
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const uint32_t v = sg.cand[i];
         if (sg.cls_k > 1 && vertex_class(v, sg.cls_k) != sg.cls_c) continue;
         bool skip = false;
@@ -1025,8 +1075,36 @@ __global__ void pick_hubs(const HubSeg *__restrict__ segs, const uint32_t *__res
         best = lane < (blockDim.x + 31) / 32 ? red[lane] : 0ull;
 #pragma unroll
         for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if (lane == 0) *sg.out = best ? 0xFFFFFFFFu - (uint32_t)(best & 0xFFFFFFFFull) : kNone;
+        if (lane == 0 && best) atomicMax(keys + blockIdx.y, best);
     }
+}
+
+__global__ void hub_decode(const HubSeg *__restrict__ segs, const unsigned long long *__restrict__ keys, uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const unsigned long long k = keys[t];
+    *segs[t].out = k ? 0xFFFFFFFFu - (uint32_t)(k & 0xFFFFFFFFull) : kNone;
+}
+
+// Both launches for n segments (descriptors on the device).
+int launch_pick_hubs(asdm_graph *G, const HubSeg *d_segs, uint32_t n, cudaStream_t s) {
+    if (!n) return ASDM_OK;
+    unsigned long long *keys = nullptr;
+    ASDM_TRY(dalloc(&keys, n, s));
+    int rc = ASDM_OK;
+    if (cudaMemsetAsync(keys, 0, n * sizeof(unsigned long long), s) != cudaSuccess) {
+        rc = fail(ASDM_ERR_CUDA, "hub keys reset failed");
+    } else {
+        for (uint32_t at = 0; at < n; at += 65535u) {  // grid y is at most 65535
+            pick_hubs<<<dim3(kHubSlices, std::min(65535u, n - at)), 256, 0, s>>>(d_segs + at, G->d.off, keys + at);
+            ::asdm::count_launch();
+        }
+        hub_decode<<<(n + 127) / 128, 128, 0, s>>>(d_segs, keys, n);
+        ::asdm::count_launch();
+        if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "hub kernels failed");
+    }
+    dfree(keys, s);
+    return rc;
 }
 
 // Indicator weights of the fixed vertices (w[hub] = 1; the arrays are zeroed
@@ -1143,7 +1221,7 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
             break;
         }
         G->stage.reset();
-        double *wbuf = nullptr, *d_terms = nullptr, *d_coef = nullptr, *d_out = nullptr;
+        double *wbuf = nullptr, *d_terms = nullptr, *d_coef = nullptr, *d_out = nullptr, *d_part = nullptr;
         uint32_t *d_mapbuf = nullptr, *d_nroot = nullptr;
         MapSeg *d_mseg = nullptr;
         BoundSeg *d_segs = nullptr;
@@ -1293,6 +1371,7 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
                 bqs[j].roots = d_roots + j;
                 bqs[j].nroot = d_nroot + j;
             }
+            if ((rc = attach_parts(bqs, &d_part, s))) break;
             if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
                 upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
                 upload_async(G, d_maps, maps.data(), maps.size() * sizeof(void *)) != cudaSuccess ||
@@ -1314,8 +1393,7 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
                 if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "tree-bound kernel failed");
             }
             if (rc != ASDM_OK) break;
-            bound_queries<<<(unsigned)bqs.size(), 256, 0, s>>>(d_bq);
-            ::asdm::count_launch();
+            launch_bound_queries(d_bq, (uint32_t)bqs.size(), s);
             bound_sums<<<(unsigned)((sums.size() + 127) / 128), 128, 0, s>>>(d_sums, (uint32_t)sums.size());
             ::asdm::count_launch();
             std::vector<double> out(ids.size());
@@ -1341,6 +1419,7 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
         dfree(d_sums, s);
         dfree(d_maps, s);
         dfree(d_roots, s);
+        dfree(d_part, s);
         cudaStreamSynchronize(s);
     }
     if (rc != ASDM_OK) {
@@ -1371,6 +1450,10 @@ int tree_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector<dou
 // vertex to its next hubs and the rounds' positive bounds add up.  Where only
 // the proof matters (no bound value asked for), a round counts its T terms
 // only for queries whose H could still carry the sum to 2^64.
+
+// Weight words of one launch group of pair programs (8 GiB): many small
+// programs per launch keep the level launches full.
+constexpr uint64_t kPairChunkWords = 1ull << 30;
 
 // One program of a pair bound: the forest over the vertices outside F, with
 // b in a's block when merged, or vertex `pin` pinned to the hub of F's
@@ -1474,7 +1557,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
     size_t at = 0;
     int rc = ASDM_OK;
     while (at < jobs.size() && rc == ASDM_OK) {
-        // a chunk: consecutive jobs whose weights and indicators fit kTreeChunkWords (one job at least)
+        // a chunk: consecutive jobs whose weights and indicators fit kPairChunkWords (one job at least)
         const size_t j0 = at;
         uint64_t words = 0;
         std::vector<size_t> qs;
@@ -1483,7 +1566,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
             uint64_t add = prep[i].terms[jobs[at].second].words;
             const bool new_q = qs.empty() || qs.back() != i;
             if (new_q) add += prep[i].fwords;
-            if (at > j0 && words + add > kTreeChunkWords) break;
+            if (at > j0 && words + add > kPairChunkWords) break;
             words += add;
             if (new_q) qs.push_back(i);
         }
@@ -1493,7 +1576,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
             break;
         }
         G->stage.reset();
-        double *wbuf = nullptr, *d_out = nullptr;
+        double *wbuf = nullptr, *d_out = nullptr, *d_part = nullptr;
         uint32_t *d_mapbuf = nullptr, *d_nroot = nullptr;
         MapSeg *d_mseg = nullptr;
         BoundSeg *d_segs = nullptr;
@@ -1669,6 +1752,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
                 bqs[k].hub = d_hub + hub0[i];
                 bqs[k].edge_ok = d_eok + fe0[i];
             }
+            if ((rc = attach_parts(bqs, &d_part, s))) break;
             if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
                 upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
                 upload_async(G, d_maps, maps.data(), maps.size() * sizeof(void *)) != cudaSuccess ||
@@ -1688,8 +1772,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
                 if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "pair-bound kernel failed");
             }
             if (rc != ASDM_OK) break;
-            bound_queries<<<(unsigned)bqs.size(), 256, 0, s>>>(d_bq);
-            ::asdm::count_launch();
+            launch_bound_queries(d_bq, (uint32_t)bqs.size(), s);
             if (cudaGetLastError() != cudaSuccess ||
                 cudaMemcpyAsync(vals.data() + j0, d_out, (j1 - j0) * sizeof(double), cudaMemcpyDeviceToHost, s) !=
                     cudaSuccess ||
@@ -1710,6 +1793,7 @@ int pair_values(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
         dfree(d_bq, s);
         dfree(d_fw, s);
         dfree(d_fh, s);
+        dfree(d_part, s);
         cudaStreamSynchronize(s);
     }
     return rc;
@@ -1823,8 +1907,7 @@ int pair_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
                     rc = fail(ASDM_ERR_CUDA, "pair-bound hub upload failed");
                     break;
                 }
-                pick_hubs<<<(unsigned)hsegs.size(), 256, 0, s>>>(d_hsegs, G->d.off);
-                ::asdm::count_launch();
+                if ((rc = launch_pick_hubs(G, d_hsegs, (uint32_t)hsegs.size(), s))) break;
             }
             if (ne) {
                 if ((rc = dalloc(&d_fe, ne, s))) break;
@@ -1867,6 +1950,7 @@ int pair_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vect
                 const double b = std::nextafter(H[i] - S[i], -HUGE_VAL);
                 if (b > 0) lb[i] = lb[i] == 0.0 ? b : std::nextafter(lb[i] + b, 0.0);
             }
+
         } while (false);
         dfree(d_hub, s);
         dfree(d_eok, s);
@@ -2014,7 +2098,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
             hub0[k] = nhub;
             nhub += (uint32_t)prep[ids[k]].fvs.size();
         }
-        double *wbuf = nullptr, *d_out = nullptr;
+        double *wbuf = nullptr, *d_out = nullptr, *d_part = nullptr;
         uint32_t *d_hub = nullptr, *d_eok = nullptr, *d_nroot = nullptr;
         BoundSeg *d_segs = nullptr;
         BoundChild *d_kids = nullptr;
@@ -2085,8 +2169,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                     rc = fail(ASDM_ERR_CUDA, "overflow-bound upload failed");
                     break;
                 }
-                pick_hubs<<<(unsigned)hsegs.size(), 256, 0, s>>>(d_hsegs, G->d.off);
-                ::asdm::count_launch();
+                if ((rc = launch_pick_hubs(G, d_hsegs, (uint32_t)hsegs.size(), s))) break;
                 const uint32_t nfix = (uint32_t)fw.size() + ne;
                 fix_weights<<<(nfix + 255) / 256, 256, 0, s>>>(d_fw, d_fh, (uint32_t)fw.size(), d_fe, ne);
                 ::asdm::count_launch();
@@ -2162,6 +2245,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                 bqs[k].edge_ok = d_eok + fe0[k];
                 r0 += bqs[k].ncomp;
             }
+            if ((rc = attach_parts(bqs, &d_part, s))) break;
             if (upload_async(G, d_segs, segs.data(), segs.size() * sizeof(BoundSeg)) != cudaSuccess ||
                 upload_async(G, d_kids, kids.data(), kids.size() * sizeof(BoundChild)) != cudaSuccess ||
                 upload_async(G, d_roots, roots.data(), roots.size() * sizeof(void *)) != cudaSuccess ||
@@ -2180,8 +2264,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
                 if (cudaGetLastError() != cudaSuccess) rc = fail(ASDM_ERR_CUDA, "overflow-bound kernel failed");
             }
             if (rc != ASDM_OK) break;
-            bound_queries<<<(unsigned)ids.size(), 256, 0, s>>>(d_bq);
-            ::asdm::count_launch();
+            launch_bound_queries(d_bq, (uint32_t)ids.size(), s);
             std::vector<double> out(ids.size());
             std::vector<uint32_t> hubs(std::max<uint32_t>(nhub, 1));
             if (cudaGetLastError() != cudaSuccess ||
@@ -2215,6 +2298,7 @@ int overflow_bounds(asdm_graph *G, const std::vector<asdm_cs *> &cs, std::vector
         dfree(d_fw, s);
         dfree(d_fh, s);
         dfree(d_roots, s);
+        dfree(d_part, s);
         cudaStreamSynchronize(s);
     }
     }

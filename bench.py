@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--profile", action="store_true", help="timed steps only: no other forms, no CPU baseline")
     ap.add_argument("--no-c4", action="store_true", help="skip the config-1 and config-4 measurements")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel knobs (profiling runs)")
+    ap.add_argument("--padded-cap-log2", type=int, default=0,
+                    help="candidate-edge build: padded lists up to 2^K entries, counting then filling beyond "
+                         "(0: the library default; profiling runs)")
     ap.add_argument("--estimator", default="", help="learned-estimator parameters (.npy); default: the trained "
                                                     "config-1 model shipped with the package, when present")
     ap.add_argument("--learned-max", type=int, default=0, help="largest prefix the estimator is asked about (0 = 6)")
@@ -398,6 +401,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     A, W, g, qs, indices, golden, cfg = setup_workload(args.workload, rank, world, args.queries)
     dg = A.DeviceGraph(g)
+    if args.padded_cap_log2:
+        t = dg.tuning()
+        dg.set_tuning(t["enum_min_blocks"], t["lane_leaf_max"], padded_cap_log2=args.padded_cap_log2)
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
     Qall = Q * world if world > 1 else Q

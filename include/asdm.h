@@ -125,7 +125,7 @@ typedef struct asdm_tuning {
                                   most 4 levels with a closed-form tail, 1..256 (default 64) */
     uint32_t padded_cap_log2;  /* candidate edges of a group are filled into lists padded to their
                                   label-run lengths when those total at most 2^this entries, else
-                                  counted first and filled exactly (20..34, default 32) */
+                                  counted first and filled exactly (20..34, default 33: 32 GiB) */
 } asdm_tuning;
 /* Order search: exhaustive over connected prefixes where the query is small
  * enough (at most 24 vertices and 4096 connected vertex subsets), else
