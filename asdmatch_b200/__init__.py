@@ -59,7 +59,7 @@ class RunStats(C.Structure):
     _fields_ = [("count", C.c_uint64), ("emb_rows", C.c_uint64), ("intersections", C.c_uint64),
                 ("list_bytes", C.c_uint64), ("tasks", C.c_uint64), ("kernel_ms", C.c_double),
                 ("build_ms", C.c_double), ("build_bytes", C.c_uint64), ("tails_lane", C.c_uint64),
-                ("tails_warp", C.c_uint64)]
+                ("tails_warp", C.c_uint64), ("busy_warp_ms", C.c_double), ("idle_warp_ms", C.c_double)]
 
 
 def _sig(name, res, args):

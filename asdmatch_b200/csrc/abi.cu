@@ -346,6 +346,8 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
             stats->kernel_ms += gs.kernel_ms;
             stats->tails_lane += gs.tails_lane;
             stats->tails_warp += gs.tails_warp;
+            stats->busy_warp_ms += gs.busy_warp_ms;
+            stats->idle_warp_ms += gs.idle_warp_ms;
             for (asdm_cs *gc : group) {
                 stats->build_ms += gc->build_ms;
                 stats->build_bytes += gc->build_bytes;

@@ -1211,8 +1211,10 @@ int build_batch(const std::vector<asdm_cs *> &group) {
     cudaEventDestroy(ev1);
     // K1 reads 8 bytes per vertex of the label of each distinct query-vertex
     // signature (and copies F words for the repeats); K2 and K3 read one rank
-    // per scanned neighbour; compaction reads the bitsets it ANDs
-    const uint64_t bytes = 8ull * seg.back() + 8ull * copied_words + 4ull * (elems[0] + elems[1]) + 4ull * bit_words_read;
+    // per scanned neighbour; compaction reads the bitsets it ANDs; K3 writes
+    // the candidate-edge lists and their offsets (4 bytes per entry)
+    const uint64_t bytes = 8ull * seg.back() + 8ull * copied_words + 4ull * (elems[0] + elems[1]) +
+                           4ull * bit_words_read + 4ull * total + 4ull * nitems;
     for (uint32_t qi = 0; qi < Q; ++qi) {
         QPlan &qp = P[qi];
         asdm_cs &cs = *qp.cs;

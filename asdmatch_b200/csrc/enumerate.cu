@@ -51,7 +51,7 @@ constexpr uint32_t kStopFlags = kFlagOverflow | kFlagTimeout | kFlagLimit;
 enum : int {
     kCtrTask = 0, kCtrCount = 1, kCtrFlags = 2, kCtrRows = 3, kCtrInter = 4, kCtrElems = 5,
     kCtrHead = 6, kCtrTail = 7, kCtrActive = 8, kCtrIdle = 9, kCtrDonated = 10, kCtrTailLane = 11,
-    kCtrTailWarp = 12, kCtrN = 16
+    kCtrTailWarp = 12, kCtrIdleNs = 13, kCtrN = 16
 };
 // Work-donation ring (a bounded multi-producer multi-consumer queue with a
 // sequence number per slot): a record is [query, level s, lo, hi, idx[0..s-1]].
@@ -936,6 +936,7 @@ struct Warp {
                 }
             }
             if (pos != ~0ull) atomicAdd(&a.ctr[kCtrActive], 1ull);
+            atomicAdd(&a.ctr[kCtrIdleNs], (unsigned long long)(globaltimer() - t0));
             atomicAdd(&a.ctr[kCtrIdle], ~0ull);
             __threadfence();
         }
@@ -2358,10 +2359,10 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         }
         cudaEventRecord(e1, s);
         unsigned long long ctr[kCtrN];
-        std::vector<unsigned long long> qc(L);
+        std::vector<unsigned long long> qc(2ull * L);  // counts, then warp-time charged
         std::vector<unsigned int> qf(L);
         if (cudaMemcpyAsync(ctr, d_ctr, sizeof ctr, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-            cudaMemcpyAsync(qc.data(), d_qcounts, L * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(qc.data(), d_qcounts, 2ull * L * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaMemcpyAsync(qf.data(), d_qflags, L * sizeof(unsigned int), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
             rc = fail(ASDM_ERR_CUDA, "batch readback failed");
             break;
@@ -2400,6 +2401,10 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             agg->kernel_ms += ms;
             agg->tails_lane = ctr[kCtrTailLane];
             agg->tails_warp = ctr[kCtrTailWarp];
+            double busy = 0.0;
+            for (uint32_t li = 0; li < L; ++li) busy += (double)qc[L + li];
+            agg->busy_warp_ms += busy * 1e-6;
+            agg->idle_warp_ms += (double)ctr[kCtrIdleNs] * 1e-6;
         }
         if (gflags & kFlagTimeout) rc = fail(ASDM_ERR_TIMEOUT, "time limit reached");
         if (rc == ASDM_OK && local_mode && d_lw) {

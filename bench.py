@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--profile", action="store_true", help="timed steps only: no other forms, no CPU baseline")
     ap.add_argument("--no-c4", action="store_true", help="skip the config-1 and config-4 measurements")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel knobs (profiling runs)")
+    ap.add_argument("--enum-min-blocks", type=int, default=0,
+                    help="resident blocks per SM the enumeration kernel is compiled for (0: the library default "
+                         "or the tuner's choice; profiling runs)")
     ap.add_argument("--padded-cap-log2", type=int, default=0,
                     help="candidate-edge build: padded lists up to 2^K entries, counting then filling beyond "
                          "(0: the library default; profiling runs)")
@@ -401,9 +404,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     A, W, g, qs, indices, golden, cfg = setup_workload(args.workload, rank, world, args.queries)
     dg = A.DeviceGraph(g)
-    if args.padded_cap_log2:
+    if args.padded_cap_log2 or args.enum_min_blocks:
         t = dg.tuning()
-        dg.set_tuning(t["enum_min_blocks"], t["lane_leaf_max"], padded_cap_log2=args.padded_cap_log2)
+        dg.set_tuning(args.enum_min_blocks or t["enum_min_blocks"], t["lane_leaf_max"],
+                      padded_cap_log2=args.padded_cap_log2 or t["padded_cap_log2"])
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
     Qall = Q * world if world > 1 else Q
@@ -418,7 +422,8 @@ def main():
             checker.check(what, batch.counts, batch.status)
         return {"kernel_ms": st.kernel_ms, "list_bytes": st.list_bytes, "cs_ms": st.build_ms,
                 "cs_bytes": st.build_bytes, "matches": int(batch.counts[batch.status == OK].sum(dtype=np.uint64)),
-                "inter": st.intersections, "status": histogram(int(x) for x in batch.status)}
+                "inter": st.intersections, "busy_warp_ms": st.busy_warp_ms, "idle_warp_ms": st.idle_warp_ms,
+                "status": histogram(int(x) for x in batch.status)}
 
     def plain_step(positions=None):
         """The plain form: one query per launch sequence (candidate space, sampling
@@ -490,6 +495,10 @@ def main():
             print(json.dumps({"profile_run": True, "ms_per_step": ms, "queries": Q, "status": agg["status"],
                               "enum_kernel_ms_per_step": agg["kernel_ms"] / args.steps,
                               "cs_build_ms_per_step": agg["cs_ms"] / args.steps,
+                              "enum_algorithmic_bytes_per_step": agg["list_bytes"] / args.steps,
+                              "enum_busy_warp_ms_per_step": agg["busy_warp_ms"] / args.steps,
+                              "enum_idle_warp_ms_per_step": agg["idle_warp_ms"] / args.steps,
+                              "cs_algorithmic_bytes_per_step": agg["cs_bytes"] / args.steps,
                               "launches": launches // args.steps}))
         if world > 1:
             dist.destroy_process_group()
@@ -569,9 +578,16 @@ def main():
     traffic = traffic_cs = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
+        # DRAM bytes per algorithmic byte from an ncu capture of a smaller case of the same workload,
+        # scaled to this step's algorithmic bytes
         with open(tp) as fh:
             t = json.load(fh).get(args.workload) or {}
-        traffic, traffic_cs = t.get("enum_batch_kernel"), t.get("k1_k3")
+
+        def scaled(k, alg):
+            e = t.get(k)
+            ok = isinstance(e, dict) and e.get("algorithmic_bytes") and e.get("dram_bytes") is not None
+            return round(e["dram_bytes"] / e["algorithmic_bytes"] * alg) if ok else None
+        traffic, traffic_cs = scaled("enum_batch_kernel", bytes_), scaled("k1_k3", cs_bytes)
     status = {STATUS_NAME.get(k, k): v for k, v in agg["status"].items()}
     n_decided = status.get("ok", 0) + status.get("overflow", 0)
     line = {

@@ -257,6 +257,8 @@ typedef struct asdm_run_stats {
     uint64_t build_bytes;    /* algorithmic bytes of that build                  */
     uint64_t tails_lane;     /* last-two-level closed forms evaluated one per lane */
     uint64_t tails_warp;     /* ... and warp-wide (long intersections)             */
+    double busy_warp_ms;     /* batches with per-query budgets: warp-time charged to queries */
+    double idle_warp_ms;     /* batches: warp-time spent waiting for donated work            */
 } asdm_run_stats;
 
 /* Exact enumeration of one query over its candidate space.  Replaces
