@@ -1287,11 +1287,13 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
     bool stop = false, roots_left = true;
     uint64_t deadline = 0;
     if (a.limit_ns && lane == 0) deadline = globaltimer() + a.limit_ns;
+    // a warp counts as active (kCtrActive) from its first root task until the
+    // roots run out, not per task: fewer atomics on one hot counter
+    if (lane == 0) atomicAdd(&a.ctr[kCtrActive], 1ull);
     while (!stop) {
         if (roots_left) {
             unsigned long long b = 0;
             if (lane == 0) {
-                atomicAdd(&a.ctr[kCtrActive], 1ull);
                 b = atomicAdd(&a.ctr[kCtrTask], 1ull);
                 if (b >= nblocks) atomicAdd(&a.ctr[kCtrActive], ~0ull);
             }
@@ -1308,9 +1310,13 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                 }
                 unsigned long long t = b * K;
                 unsigned long long t_end = min(t + K, P);
-                // a query past its count limit or time budget is abandoned
+                // a query past its count limit or time budget is abandoned: its remaining
+                // root tasks are skipped at once (the task counter jumps past them)
                 W.mark();
-                if (W.query_stopped()) t_end = t;
+                if (W.query_stopped()) {
+                    t_end = t;
+                    if (MULTI && lane == 0) atomicMax(&a.ctr[kCtrTask], a.task_pre[W.q + 1]);
+                }
                 if (W.n == 1) {
                     for (; t < t_end; ++t) {
                         if (lane == 0) {
@@ -1342,10 +1348,8 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
                     }
                 }
                 W.charge();
-                if (lane == 0) {
-                    if (MULTI && a.qcycles) atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
-                    atomicAdd(&a.ctr[kCtrActive], ~0ull);
-                }
+                if (lane == 0 && MULTI && a.qcycles)
+                    atomicAdd(&a.qcycles[W.q], (unsigned long long)(clock64() - c0));
                 continue;
             }
             roots_left = false;
@@ -1371,6 +1375,8 @@ __device__ void warp_loop(const EnumArgs &a, Warp<MODE, MULTI> &W, uint32_t lane
             atomicAdd(&a.ctr[kCtrActive], ~0ull);
         }
     }
+    // a warp stopped while it still had roots leaves the active count
+    if (roots_left && lane == 0) atomicAdd(&a.ctr[kCtrActive], ~0ull);
     // flush per-warp totals
     W.flush_count();
     if (lane == 0) {
@@ -1736,13 +1742,14 @@ unsigned long long root_pairs(const asdm_cs &cs, const asdm_plan &plan) {
 }
 
 // Root tasks: blocks of consecutive (level-0, level-1) candidate pairs, about
-// 64K pairs per block count, between 1 and 256 pairs per block.
-// `min_blk` raises the block size (a batch's whole launch needs only a few
-// dozen tasks per resident warp; work donation splits heavy ranges).
+// 64K blocks per query, between 1 and 65,536 pairs per block (a few dozen
+// tasks per resident warp are enough: work donation splits heavy ranges, and
+// every task costs an atomic on one shared counter).  `min_blk` raises the
+// block size.
 void root_blocks(const asdm_cs &cs, const asdm_plan &plan, unsigned long long &pairs, unsigned long long &blk,
                  unsigned long long &nblocks, unsigned long long min_blk = 1) {
     pairs = root_pairs(cs, plan);
-    blk = std::min<unsigned long long>(256, std::max<unsigned long long>(min_blk, pairs / 65536));
+    blk = std::min<unsigned long long>(65536, std::max<unsigned long long>(min_blk, pairs / 65536));
     nblocks = (pairs + blk - 1) / blk;
 }
 

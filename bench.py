@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--enum-min-blocks", type=int, default=0,
                     help="resident blocks per SM the enumeration kernel is compiled for (0: the library default "
                          "or the tuner's choice; profiling runs)")
+    ap.add_argument("--root-block-min", type=int, default=0,
+                    help="fewest level-0/1 pairs per root task of short plans (0: the library default or the "
+                         "tuner's choice; profiling runs)")
     ap.add_argument("--padded-cap-log2", type=int, default=0,
                     help="candidate-edge build: padded lists up to 2^K entries, counting then filling beyond "
                          "(0: the library default; profiling runs)")
@@ -404,9 +407,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     A, W, g, qs, indices, golden, cfg = setup_workload(args.workload, rank, world, args.queries)
     dg = A.DeviceGraph(g)
-    if args.padded_cap_log2 or args.enum_min_blocks:
+    if args.padded_cap_log2 or args.enum_min_blocks or args.root_block_min:
         t = dg.tuning()
         dg.set_tuning(args.enum_min_blocks or t["enum_min_blocks"], t["lane_leaf_max"],
+                      root_block_min=args.root_block_min or t["root_block_min"],
                       padded_cap_log2=args.padded_cap_log2 or t["padded_cap_log2"])
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
@@ -423,6 +427,7 @@ def main():
         return {"kernel_ms": st.kernel_ms, "list_bytes": st.list_bytes, "cs_ms": st.build_ms,
                 "cs_bytes": st.build_bytes, "matches": int(batch.counts[batch.status == OK].sum(dtype=np.uint64)),
                 "inter": st.intersections, "busy_warp_ms": st.busy_warp_ms, "idle_warp_ms": st.idle_warp_ms,
+                "tasks": st.tasks,
                 "status": histogram(int(x) for x in batch.status)}
 
     def plain_step(positions=None):
@@ -498,6 +503,7 @@ def main():
                               "enum_algorithmic_bytes_per_step": agg["list_bytes"] / args.steps,
                               "enum_busy_warp_ms_per_step": agg["busy_warp_ms"] / args.steps,
                               "enum_idle_warp_ms_per_step": agg["idle_warp_ms"] / args.steps,
+                              "enum_root_tasks_per_step": agg["tasks"] / args.steps,
                               "cs_algorithmic_bytes_per_step": agg["cs_bytes"] / args.steps,
                               "launches": launches // args.steps}))
         if world > 1:
