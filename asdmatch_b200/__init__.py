@@ -102,7 +102,7 @@ _count_query = _sig("asdm_count_query", C.c_int, [_vp, _u32p, _u32p, _u32p, C.c_
                                                   C.POINTER(RunStats)])
 class Tuning(C.Structure):
     _fields_ = [("enum_min_blocks", C.c_uint32), ("lane_leaf_max", C.c_uint32), ("planner", C.c_uint32),
-                ("root_block_min", C.c_uint32), ("padded_cap_log2", C.c_uint32)]
+                ("root_block_min", C.c_uint32), ("padded_cap_log2", C.c_uint32), ("merge_ratio", C.c_uint32)]
 
 
 PLANNER_DP = 0
@@ -304,19 +304,22 @@ class DeviceGraph:
         self._spaces = weakref.WeakSet()
 
     def set_tuning(self, enum_min_blocks: int, lane_leaf_max: int, planner: Optional[int] = None,
-                   root_block_min: Optional[int] = None, padded_cap_log2: Optional[int] = None):
+                   root_block_min: Optional[int] = None, padded_cap_log2: Optional[int] = None,
+                   merge_ratio: Optional[int] = None):
         cur = self.tuning()
         planner = cur["planner"] if planner is None else planner
         root_block_min = cur["root_block_min"] if root_block_min is None else root_block_min
         padded_cap_log2 = cur["padded_cap_log2"] if padded_cap_log2 is None else padded_cap_log2
+        merge_ratio = cur["merge_ratio"] if merge_ratio is None else merge_ratio
         _check(_set_tuning(self._h, C.byref(Tuning(enum_min_blocks, lane_leaf_max, planner, root_block_min,
-                                                   padded_cap_log2))), "tuning")
+                                                   padded_cap_log2, merge_ratio))), "tuning")
 
     def tuning(self):
         t = Tuning()
         _check(_get_tuning(self._h, C.byref(t)))
         return {"enum_min_blocks": t.enum_min_blocks, "lane_leaf_max": t.lane_leaf_max, "planner": t.planner,
-                "root_block_min": t.root_block_min, "padded_cap_log2": t.padded_cap_log2}
+                "root_block_min": t.root_block_min, "padded_cap_log2": t.padded_cap_log2,
+                "merge_ratio": t.merge_ratio}
 
     def stream(self) -> int:
         """cudaStream_t (as an int) the library uses for this graph."""
@@ -886,22 +889,23 @@ def run_batch(dg: DeviceGraph, queries: Sequence[HostGraph], time_limit_s: float
 
 def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
              min_blocks=(1, 3, 4, 5), lane_leaf=(32, 96, 256), planners=(PLANNER_DP, PLANNER_GREEDY),
-             root_blocks=(16, 64, 256), run=None):
+             root_blocks=(16, 64, 256), merge_ratios=(0, 2, 8, 32), run=None):
     """Times the caller's batch under every kernel configuration (with the
-    graph's current planner and root-block size), then every planner, then
-    every smallest root-block size with the fastest settings so far, and keeps
-    the fastest on `dg` (device time between CUDA events on the library's
-    stream).  `run(dg, batch)` is the timed call
-    (default: run_batch_packed).  Returns (best, table)."""
+    graph's current planner, root-block size and merge ratio), then every
+    planner, then every smallest root-block size, then every merge/gallop
+    ratio with the fastest settings so far, and keeps the fastest on `dg`
+    (device time between CUDA events on the library's stream).
+    `run(dg, batch)` is the timed call (default: run_batch_packed).  Returns
+    (best, table)."""
     import torch
     run = run or run_batch_packed
     stream = torch.cuda.ExternalStream(dg.stream())
     want = None
     table = []
 
-    def measure(mb, ll, pl, rb):
+    def measure(mb, ll, pl, rb, mr):
         nonlocal want
-        dg.set_tuning(mb, ll, pl, rb)
+        dg.set_tuning(mb, ll, pl, rb, merge_ratio=mr)
         run(dg, batch)  # warm
         ok = batch.status == OK
         if want is None:
@@ -917,20 +921,26 @@ def autotune(dg: DeviceGraph, batch: BatchInput, reps: int = 2,
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
         table.append({"enum_min_blocks": mb, "lane_leaf_max": ll, "planner": pl, "root_block_min": rb,
-                      "ms": min(times)})
+                      "merge_ratio": mr, "ms": min(times)})
 
-    pl0, rb0 = dg.tuning()["planner"], dg.tuning()["root_block_min"]
+    t0 = dg.tuning()
+    pl0, rb0, mr0 = t0["planner"], t0["root_block_min"], t0["merge_ratio"]
     for mb in min_blocks:
         for ll in lane_leaf:
-            measure(mb, ll, pl0, rb0)
+            measure(mb, ll, pl0, rb0, mr0)
     best = min(table, key=lambda r: r["ms"])
     for pl in planners:
         if pl != pl0:
-            measure(best["enum_min_blocks"], best["lane_leaf_max"], pl, rb0)
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], pl, rb0, mr0)
     best = min(table, key=lambda r: r["ms"])
     for rb in root_blocks:
         if rb != rb0:
-            measure(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], rb)
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], rb, mr0)
     best = min(table, key=lambda r: r["ms"])
-    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], best["root_block_min"])
+    for mr in merge_ratios:
+        if mr != mr0:
+            measure(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], best["root_block_min"], mr)
+    best = min(table, key=lambda r: r["ms"])
+    dg.set_tuning(best["enum_min_blocks"], best["lane_leaf_max"], best["planner"], best["root_block_min"],
+                  merge_ratio=best["merge_ratio"])
     return best, table

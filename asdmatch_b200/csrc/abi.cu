@@ -12,8 +12,12 @@ namespace {
 constexpr uint32_t kFull = 0xffffffffu;
 
 // Warp per intersection problem: the shortest list drives, every lane takes
-// one driver element per round and gallops in the other lists from cursors
-// that advance with the driver (leapfrog seek; utility/compute_set_intersection.cpp:177-233).
+// one driver element per round and looks it up in the other lists from cursors
+// that advance with the driver (leapfrog seek; utility/compute_set_intersection.cpp:177-233):
+// a list whose unread part is at most kMergeRatio times the driver's is merged
+// a window of 32 entries at a time, a longer one is galloped by every lane
+// (the reference's merge/gallop switch, :9-30).
+constexpr uint32_t kMergeRatio = 8;
 __global__ void __launch_bounds__(256) intersect_kernel(const uint32_t *__restrict__ values,
                                                         const uint64_t *__restrict__ list_off,
                                                         const uint32_t *__restrict__ list_first, uint32_t nsets,
@@ -56,9 +60,15 @@ __global__ void __launch_bounds__(256) intersect_kernel(const uint32_t *__restri
                 const uint64_t sj = __shfl_sync(kFull, start, j);
                 const uint32_t lj = __shfl_sync(kFull, len, j);
                 const uint32_t *lst = values + sj;
-                const uint32_t q = valid ? gallop_lb(lst, cur[j], lj, x) : lj;
-                ok = ok && q < lj && lst[q] == x;
-                const uint32_t nc = __shfl_sync(kFull, q, lastlane);
+                const uint32_t cj = cur[j];
+                uint32_t nc;
+                if ((uint64_t)(lj - cj) <= (uint64_t)kMergeRatio * (key - p0)) {
+                    ok = warp_merge_member(lst, cj, lj, x, ok, lastlane, lane, nc) && ok;
+                } else {
+                    const uint32_t q = valid ? gallop_lb(lst, cj, lj, x) : lj;
+                    ok = ok && q < lj && lst[q] == x;
+                    nc = __shfl_sync(kFull, q, lastlane);
+                }
                 __syncwarp();
                 if (lane == 0) cur[j] = nc;
                 __syncwarp();
@@ -98,6 +108,7 @@ extern "C" int asdm_graph_set_tuning(asdm_graph *g, const asdm_tuning *t) {
     if (t->planner != ASDM_PLANNER_DP && t->planner != ASDM_PLANNER_GREEDY)
         return fail(ASDM_ERR_INVALID, "planner must be ASDM_PLANNER_DP or ASDM_PLANNER_GREEDY");
     if (t->padded_cap_log2 < 20 || t->padded_cap_log2 > 34) return fail(ASDM_ERR_INVALID, "padded_cap_log2 must be 20..34");
+    if (t->merge_ratio > 1024) return fail(ASDM_ERR_INVALID, "merge_ratio must be <= 1024");
     g->tuning = *t;
     return ASDM_OK;
 }

@@ -97,6 +97,54 @@ __device__ __forceinline__ uint32_t gallop_lb(const uint32_t *__restrict__ a, ui
     return lo;
 }
 
+#ifdef __CUDACC__
+// Warp-cooperative merge probe, the counterpart of galloping for lists of
+// similar length (the reference switches from galloping to a linear merge when
+// the lengths differ by less than 50x, utility/compute_set_intersection.cpp:9-30).
+// Lane i holds x_i; x ascends over lanes 0..last, lanes past `last` hold
+// 0xFFFFFFFF.  Every entry of a[0, cur) is below x_0.  The warp reads a[cur, n)
+// one window of 32 entries at a time (one coalesced 128-byte load) and each
+// lane finds the number of window entries below its x in five shuffle steps.
+// A lane is settled by the first window whose last entry is >= its x.  The
+// loop ends when x_last is settled, or when no lane with `want` set is still
+// unsettled.  Returns whether x_i is in a (meaningful where `want` is set);
+// *ncur gets a position p <= lower_bound(a, x_last) with every a[0, p) below
+// x_last, the cursor of the next round of drivers.
+__device__ __forceinline__ bool warp_merge_member(const uint32_t *__restrict__ a, uint32_t cur, uint32_t n, uint32_t x,
+                                                  bool want, uint32_t last, uint32_t lane, uint32_t &ncur) {
+    constexpr uint32_t full = 0xffffffffu;
+    const uint32_t xl = __shfl_sync(full, x, last);
+    bool hit = false;
+    uint32_t c = cur;
+    ncur = n;
+    while (c < n) {
+        const uint32_t j = c + lane;
+        const uint32_t y = j < n ? a[j] : 0xFFFFFFFFu;
+        uint32_t r = 0;  // entries of the window below x (at most 31 here)
+#pragma unroll
+        for (uint32_t s = 16; s; s >>= 1) {
+            const uint32_t yv = __shfl_sync(full, y, r + s - 1);
+            if (yv < x) r += s;
+        }
+        const uint32_t yr = __shfl_sync(full, y, r);
+        const uint32_t ylast = __shfl_sync(full, y, 31);
+        hit = hit || (want && lane <= last && yr == x);
+        const uint32_t rl = __shfl_sync(full, r, last);
+        if (ylast >= xl) {
+            ncur = c + rl;
+            break;
+        }
+        // every entry of this window is below x_last
+        if (!__any_sync(full, want && x > ylast)) {
+            ncur = min(c + 32, n);
+            break;
+        }
+        c += 32;
+    }
+    return hit;
+}
+#endif
+
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t n, uint32_t x) {
     uint32_t lo = 0, hi = n;
     while (lo < hi) {
@@ -164,7 +212,7 @@ struct PinnedStage {
 };
 
 struct asdm_graph {
-    asdm_tuning tuning{1, 96, ASDM_PLANNER_DP, 64, 33};         // kernel knobs (asdm_graph_set_tuning)
+    asdm_tuning tuning{1, 96, ASDM_PLANNER_DP, 64, 33, 8};         // kernel knobs (asdm_graph_set_tuning)
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;

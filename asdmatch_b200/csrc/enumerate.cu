@@ -97,6 +97,7 @@ struct EnumArgs {
     uint64_t limit_ns;          // 0 = none; else per-warp wall-clock budget
     unsigned long long count_limit;  // 0 = none
     uint32_t lane_leaf_max;     // longest shortest-list a lane evaluates alone at the last level
+    uint32_t merge_ratio;       // a list probe merges (instead of galloping) up to this length ratio
     uint32_t *queue;            // kQueueCap records of kRecWords words
     unsigned long long *qseq;   // kQueueCap slot sequence numbers
     // batches of queries (enum_batch_kernel): one QDesc per query, root tasks
@@ -952,8 +953,13 @@ struct Warp {
     }
 
     // Membership of x (this lane's driver element) in every non-driver list
-    // of level d, galloping from the shared cursors; advances the cursors.
-    __device__ __forceinline__ bool probe(const DLevel &lv, uint32_t dslot, uint32_t x, bool valid, uint32_t lastlane) {
+    // of level d from the shared cursors; advances the cursors.  drem is the
+    // number of driver entries from this round's first to the end of the
+    // range.  A list whose unread part is at most merge_ratio x drem long is
+    // merged with the drivers a window of 32 entries at a time (about
+    // len / drem windows per round); a longer one is galloped by every lane.
+    __device__ __forceinline__ bool probe(const DLevel &lv, uint32_t dslot, uint32_t x, bool valid, uint32_t lastlane,
+                                          uint32_t drem) {
         bool ok = valid;
         for (uint32_t s = 0; s < lv.nback; ++s) {
             const uint32_t sl = lv.back_first + s;
@@ -962,9 +968,14 @@ struct Warp {
             const uint32_t *lst = B[sl].list + sstart[sl];
             const uint32_t len = slen[sl];
             const uint32_t cur = scur[sl];
-            const uint32_t q = valid ? gallop_lb(lst, cur, len, x) : len;
-            ok = ok && q < len && lst[q] == x;
-            const uint32_t nc = __shfl_sync(kFull, q, lastlane);
+            uint32_t nc;
+            if ((uint64_t)(len - cur) <= (uint64_t)a.merge_ratio * drem) {
+                ok = warp_merge_member(lst, cur, len, x, ok, lastlane, lane, nc) && ok;
+            } else {
+                const uint32_t q = valid ? gallop_lb(lst, cur, len, x) : len;
+                ok = ok && q < len && lst[q] == x;
+                nc = __shfl_sync(kFull, q, lastlane);
+            }
             __syncwarp();
             if (lane == 0) scur[sl] = nc;
             __syncwarp();
@@ -989,7 +1000,7 @@ struct Warp {
         const bool valid = p < dlen;
         const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
         const uint32_t lastlane = min(31u, dlen - 1 - p0);
-        bool ok = probe(lv, dslot, x, valid, lastlane);
+        bool ok = probe(lv, dslot, x, valid, lastlane, dlen - p0);
         if (lv.nconf && __any_sync(kFull, ok)) {
             const uint32_t vx = ok ? lv.cand[x] : 0;
             ok = ok && no_conflict(lv, vx);
@@ -1103,7 +1114,7 @@ struct Warp {
                     const uint32_t p = p0 + lane;
                     const bool valid = p < hi;
                     const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
-                    const bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0));
+                    const bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0), hi - p0);
                     total += __popc(__ballot_sync(kFull, ok));
                 }
             }
@@ -1147,7 +1158,7 @@ struct Warp {
                 const uint32_t p = p0 + lane;
                 const bool valid = p < hi;
                 const uint32_t x = valid ? dl[p] : 0xFFFFFFFFu;
-                bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0));
+                bool ok = probe(lv, dslot, x, valid, min(31u, hi - 1 - p0), hi - p0);
                 const uint32_t vx = ok ? lv.cand[x] : 0;
                 ok = ok && no_conflict(lv, vx);
                 const uint32_t mask = __ballot_sync(kFull, ok);
@@ -1918,6 +1929,7 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
         a.limit_ns = opt.time_limit_s > 0 ? (uint64_t)(opt.time_limit_s * 1e9) : 0;
         a.count_limit = opt.count_limit;
         a.lane_leaf_max = G->tuning.lane_leaf_max;
+        a.merge_ratio = G->tuning.merge_ratio;
         if (mode == ASDM_MODE_COUNT) {
             std::vector<TailData> td;
             if ((rc = build_tails({&cs}, {&plan}, td, &d_ps, s))) break;
@@ -2332,6 +2344,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
         a.lane_leaf_max = G->tuning.lane_leaf_max;
+        a.merge_ratio = G->tuning.merge_ratio;
         if (task_pre[L]) {
             // register-budget variant chosen by the tuner (min blocks per SM)
             void (*k)(EnumArgs) = enum_batch_kernel<1>;
@@ -2631,6 +2644,7 @@ extern "C" int asdm_run_plan_count_noalloc(asdm_cs *cs, const asdm_plan *plan, d
     a.limit_ns = time_limit_s > 0 ? (uint64_t)(time_limit_s * 1e9) : 0;
     a.count_limit = count_limit;
     a.lane_leaf_max = G->tuning.lane_leaf_max;
+    a.merge_ratio = G->tuning.merge_ratio;
     if (a.ntasks) {
         const uint32_t smem = 4u * (plan_words(n, nb, nc) + kWarps * warp_words(n, nb));
         ASDM_TRY(launch<ASDM_MODE_COUNT>(a, smem, G->num_sms, s));

@@ -54,6 +54,19 @@ def c4_query_specs():
     return [(C4_QUERY_SIZE, C4_QUERY_SEED + i, 0) for i in range(C4_QUERIES)]
 
 
+C4_PARITY_SEED = 95_000
+C4_PARITY = 40
+C4_EMBED_SEED = 96_000
+
+
+def c4_parity_specs():
+    """(size, seed, density) of the config-4 parity queries: random-walk
+    queries of 4..8 vertices on the config-4 graph, small enough for the
+    reference's local counting to finish, so that its |Vg| x |Vq| CSV can be
+    compared at the graph's full size."""
+    return [(4 + i % 5, C4_PARITY_SEED + i, 0) for i in range(C4_PARITY)]
+
+
 def generator_args(spec):
     """The graph arguments of asdm_gen.out for a spec."""
     return [str(spec["n"]), str(spec["m"]), repr(float(spec["gamma"])), str(spec["nlabels"]),

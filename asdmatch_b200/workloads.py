@@ -24,7 +24,7 @@ import asdmatch_b200 as A
 
 from asdmatch_b200.specs import (C0, C0_QUERY_SEED, C0D, C0D_QUERY_SEED, C1, C1_PER_CLASS, C1_SIZES,  # noqa: F401
                                   C2_QUERIES, C2_QUERY_SEED, C4, C4_QUERY_SEED, DENSE, SPARSE, c1_seed_base,
-                                  c2_seed_size, c4_query_specs)
+                                  c2_seed_size, c4_parity_specs, c4_query_specs)
 
 
 

@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--padded-cap-log2", type=int, default=0,
                     help="candidate-edge build: padded lists up to 2^K entries, counting then filling beyond "
                          "(0: the library default; profiling runs)")
+    ap.add_argument("--merge-ratio", type=int, default=-1,
+                    help="intersection merge/gallop length ratio before tuning (-1: the library default)")
     ap.add_argument("--estimator", default="", help="learned-estimator parameters (.npy); default: the trained "
                                                     "config-1 model shipped with the package, when present")
     ap.add_argument("--learned-max", type=int, default=0, help="largest prefix the estimator is asked about (0 = 6)")
@@ -407,11 +409,12 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     A, W, g, qs, indices, golden, cfg = setup_workload(args.workload, rank, world, args.queries)
     dg = A.DeviceGraph(g)
-    if args.padded_cap_log2 or args.enum_min_blocks or args.root_block_min:
+    if args.padded_cap_log2 or args.enum_min_blocks or args.root_block_min or args.merge_ratio >= 0:
         t = dg.tuning()
         dg.set_tuning(args.enum_min_blocks or t["enum_min_blocks"], t["lane_leaf_max"],
                       root_block_min=args.root_block_min or t["root_block_min"],
-                      padded_cap_log2=args.padded_cap_log2 or t["padded_cap_log2"])
+                      padded_cap_log2=args.padded_cap_log2 or t["padded_cap_log2"],
+                      merge_ratio=args.merge_ratio if args.merge_ratio >= 0 else t["merge_ratio"])
     stream = torch.cuda.ExternalStream(dg.stream(), device=dev)
     Q = len(qs)
     Qall = Q * world if world > 1 else Q
@@ -505,7 +508,8 @@ def main():
                               "enum_idle_warp_ms_per_step": agg["idle_warp_ms"] / args.steps,
                               "enum_root_tasks_per_step": agg["tasks"] / args.steps,
                               "cs_algorithmic_bytes_per_step": agg["cs_bytes"] / args.steps,
-                              "launches": launches // args.steps}))
+                              "launches": launches // args.steps,
+                              "tuning": dg.tuning(), "autotune_table": tune_table}))
         if world > 1:
             dist.destroy_process_group()
         return

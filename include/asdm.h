@@ -126,6 +126,10 @@ typedef struct asdm_tuning {
     uint32_t padded_cap_log2;  /* candidate edges of a group are filled into lists padded to their
                                   label-run lengths when those total at most 2^this entries, else
                                   counted first and filled exactly (20..34, default 33: 32 GiB) */
+    uint32_t merge_ratio;      /* intersection method: a list probed by a round of 32 driver entries
+                                  is merged with them (32-entry windows) while its unread part is at
+                                  most this many times the driver's unread part, else galloped
+                                  (0 = always gallop; 0..1024, default 8) */
 } asdm_tuning;
 /* Order search: exhaustive over connected prefixes where the query is small
  * enough (at most 24 vertices and 4096 connected vertex subsets), else

@@ -28,7 +28,8 @@
 //      at a time, each killed after s seconds.  One line per query on
 //      stdout: "Q <k> ok|timeout|signal <n>|exit <n> <wall seconds>".  Every
 //      child starts from the same untouched state, as a fresh process would.
-//      With -c (LOCAL_COUNT builds) each child writes its CSV to <dir>/q<k>.csv.
+//      With -c (LOCAL_COUNT builds) each child writes its CSV to <dir>/q<k>.csv,
+//      with -e (COLLECT_RESULT builds) its sorted embedding dump to <dir>/q<k>.emb.
 // Build variants select the reference's compile-time modes (config/config.h:38-40):
 //   ref_count : ALL_LEVEL                          (exact counts)
 //   ref_local : ALL_LEVEL + LOCAL_COUNT            (+ |Vg|x|Vq| CSV via -c)
@@ -67,13 +68,14 @@ static double seconds_since(std::chrono::steady_clock::time_point t0) {
 
 // In list mode with -c, each child's CSV path (<dir>/q<k>.csv).
 static std::string g_csv_path;
+static std::string g_emb_path;  // list mode: this child's embedding dump
 
 // One query against the loaded data graph g: the reference's ASDMatch.out
 // sequence after its graph loads (main.cpp:27-147).
 static int run_query(int argc, char **argv, Command &cmd, const std::string &qpath, Graph &g) {
     const std::string cardPath = cmd.getDPStructPath();
     const std::string csDump = option_after(argc, argv, "-w");
-    const std::string embDump = option_after(argc, argv, "-e");
+    const std::string embDump = g_emb_path.empty() ? option_after(argc, argv, "-e") : g_emb_path;
     int memKB = cmd.getMemoryBudget();
     if (memKB == 0) memKB = 16e5;
     const size_t budget = (size_t)1024 * memKB;
@@ -231,6 +233,7 @@ static int run_list(int argc, char **argv, Command &cmd, Graph &g, const std::st
                 const std::string out = outDir + "/q" + std::to_string(next) + ".out";
                 if (!std::freopen(out.c_str(), "w", stdout)) _exit(3);
                 if (!cmd.getCountPath().empty()) g_csv_path = outDir + "/q" + std::to_string(next) + ".csv";
+                if (!option_after(argc, argv, "-e").empty()) g_emb_path = outDir + "/q" + std::to_string(next) + ".emb";
                 const int rc = run_query(argc, argv, cmd, queries[next], g);
                 std::cout.flush();
                 std::fflush(stdout);

@@ -151,6 +151,15 @@ def test_leapfrog_join_matches_numpy():
                 n = int(rng.integers(0, 50)) * (ratio if j == 0 else 1) + (1 if j else 0)
                 lists.append(np.unique(rng.integers(0, 4000, size=n)).astype(np.uint32))
             sets.append(lists)
+    # long lists of similar length (merged over many 32-entry windows) and
+    # lopsided ones (galloped); equal, interleaved and disjoint lists
+    for k, n0, n1, span in ((2, 3000, 2500, 9000), (3, 700, 5000, 20000), (2, 40, 9000, 100000),
+                            (4, 1500, 1600, 4000)):
+        sets.append([np.unique(rng.integers(0, span, size=n0 if j == 0 else n1)).astype(np.uint32)
+                     for j in range(k)])
+    sets.append([np.arange(0, 4000, 2, dtype=np.uint32), np.arange(1, 4001, 2, dtype=np.uint32)])
+    sets.append([np.arange(5000, dtype=np.uint32)] * 3)
+    sets.append([np.arange(0, 3000, dtype=np.uint32), np.arange(3000, 6000, dtype=np.uint32)])
     sets.append([np.zeros(0, np.uint32), np.arange(10, dtype=np.uint32)])
     sets.append([])
     out = A.leapfrog_join(sets)
@@ -235,16 +244,24 @@ def test_every_tuning_gives_the_same_counts(golden, c0d_files, dg_c0d):
             dg_c0d.set_tuning(mb, ll)
             A.run_batch_packed(dg_c0d, b)
             assert b.counts.tolist() == want, (mb, ll)
+    # intersection method: gallop only, merge up to small ratios, merge almost always
+    for mr in (0, 1, 32, 1024):
+        for mb in (1, 5):
+            dg_c0d.set_tuning(mb, 96, merge_ratio=mr)
+            A.run_batch_packed(dg_c0d, b)
+            assert b.counts.tolist() == want, (mb, mr)
+    dg_c0d.set_tuning(1, 96, merge_ratio=8)
     best, table = A.autotune(dg_c0d, b, reps=1, lane_leaf=(96,))
-    # four kernel configurations, then the other planner, then two more root-block sizes
-    assert len(table) == 7 and best in table
+    # four kernel configurations, the other planner, two more root-block sizes, three more merge ratios
+    assert len(table) == 10 and best in table
     assert {r["planner"] for r in table} == {A.PLANNER_DP, A.PLANNER_GREEDY}
     assert {r["root_block_min"] for r in table} == {16, 64, 256}
+    assert {r["merge_ratio"] for r in table} == {0, 2, 8, 32}
     for rb in (1, 4, 256):
         dg_c0d.set_tuning(1, 96, A.PLANNER_DP, rb)
         A.run_batch_packed(dg_c0d, b)
         assert b.counts.tolist() == want, rb
-    dg_c0d.set_tuning(1, 96, A.PLANNER_DP, 64)
+    dg_c0d.set_tuning(1, 96, A.PLANNER_DP, 64, merge_ratio=8)
 
 
 def test_batched_local_counts_match_golden_csv(golden, c0_files, c0d_files, dg_c0, dg_c0d, edge_files):
