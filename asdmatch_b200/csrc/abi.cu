@@ -252,7 +252,11 @@ int build_plan(const asdm_cs &cs, const uint32_t *user_order, asdm_plan &p, cons
 int build_prefix_plan(const asdm_cs &cs, const uint32_t *order, uint32_t depth, asdm_plan &p);
 int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
                     double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out, uint64_t *cycles = nullptr, double query_time_s = 0.0);
+                    uint64_t *const *local_out, uint64_t *cycles = nullptr, double query_time_s = 0.0,
+                    bool settled = false);
+int settle_queries(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<char> &full,
+                   std::vector<uint32_t> &live, uint64_t count_limit, uint64_t *counts, int *status,
+                   asdm_run_stats *agg, uint64_t *const *local_out);
 int plan_batch_learned(const std::vector<asdm_cs *> &css, asdm_estimator *e, uint32_t kmax,
                        std::vector<asdm_plan> &plans);
 }  // namespace asdm
@@ -319,18 +323,53 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
             if (rc == ASDM_ERR_CUDA) break;
             continue;
         }
-        std::vector<asdm_plan> plans(ids.size());
+        // queries the tree program or an overflow bound settles need no plan:
+        // settle first, then plan (cost model, .card or learned) the rest
+        asdm_run_stats gs{};
+        std::vector<uint32_t> open;
+        {
+            std::vector<uint32_t> live;
+            for (uint32_t k = 0; k < ids.size(); ++k)
+                if (group[k]->nonempty) live.push_back(k);  // an empty space counts 0, like the reference's early return
+            std::vector<char> full(ids.size(), 1);
+            std::vector<uint64_t> sc(ids.size(), 0);
+            std::vector<int> sst(ids.size(), ASDM_OK);
+            std::vector<uint64_t *> slo;
+            if (local_out)
+                for (uint32_t id : ids) slo.push_back(local_out[id]);
+            const std::vector<uint32_t> before = live;
+            rc = settle_queries(g, group, full, live, count_limit, sc.data(), sst.data(), &gs,
+                                local_out ? slo.data() : nullptr);
+            if (rc != ASDM_OK) {
+                for (uint32_t id : ids) status[id] = rc;
+                if (worst == ASDM_OK) worst = rc;
+                if (rc == ASDM_ERR_CUDA) break;
+                continue;
+            }
+            std::vector<char> still(ids.size(), 0);
+            for (uint32_t k : live) still[k] = 1;
+            for (uint32_t k : before) {
+                if (still[k]) continue;
+                counts[ids[k]] = sc[k];
+                status[ids[k]] = sst[k];
+                if (sst[k] != ASDM_OK && worst == ASDM_OK) worst = sst[k];
+            }
+            open = live;
+        }
+        std::vector<asdm_cs *> open_cs;
+        for (uint32_t k : open) open_cs.push_back(group[k]);
+        std::vector<asdm_plan> plans(open.size());
         std::vector<asdm_cs *> run_cs;
         std::vector<const asdm_plan *> run_plans;
         std::vector<uint32_t> run_ids;
         int learned_rc = ASDM_OK;
-        if (est) learned_rc = plan_batch_learned(group, est, est_kmax, plans);
-        for (size_t k = 0; k < ids.size(); ++k) {
-            if (!group[k]->nonempty) continue;  // count 0, like the reference's early return
+        if (est && !open_cs.empty()) learned_rc = plan_batch_learned(open_cs, est, est_kmax, plans);
+        for (size_t j = 0; j < open.size(); ++j) {
+            const uint32_t k = open[j];
             int prc;
-            if (!est) prc = build_plan(*group[k], nullptr, plans[k], cards ? cards[ids[k]] : nullptr);
+            if (!est) prc = build_plan(*group[k], nullptr, plans[j], cards ? cards[ids[k]] : nullptr);
             else if (learned_rc != ASDM_OK) prc = learned_rc;
-            else if (plans[k].order.size() != group[k]->q.n) prc = fail(ASDM_ERR_INVALID, "query is not connected");
+            else if (plans[j].order.size() != group[k]->q.n) prc = fail(ASDM_ERR_INVALID, "query is not connected");
             else prc = ASDM_OK;
             if (prc != ASDM_OK) {
                 status[ids[k]] = prc;
@@ -338,7 +377,7 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
                 continue;
             }
             run_cs.push_back(group[k]);
-            run_plans.push_back(&plans[k]);
+            run_plans.push_back(&plans[j]);
             run_ids.push_back(ids[k]);
         }
         std::vector<uint64_t> c(run_ids.size());
@@ -346,9 +385,20 @@ static int run_batch_impl(asdm_graph *g, uint32_t nq, const uint32_t *q_sizes, c
         std::vector<uint64_t *> lo;
         if (local_out)
             for (uint32_t id : run_ids) lo.push_back(local_out[id]);
-        asdm_run_stats gs{};
-        rc = run_batch_count(g, run_cs, run_plans, time_limit_s, count_limit, c.data(), st.data(), &gs,
-                             local_out ? lo.data() : nullptr, nullptr, query_time_s);
+        {
+            asdm_run_stats es{};
+            rc = run_batch_count(g, run_cs, run_plans, time_limit_s, count_limit, c.data(), st.data(), &es,
+                                 local_out ? lo.data() : nullptr, nullptr, query_time_s, /*settled=*/true);
+            gs.count += es.count;
+            gs.intersections += es.intersections;
+            gs.list_bytes += es.list_bytes;
+            gs.tasks += es.tasks;
+            gs.kernel_ms += es.kernel_ms;
+            gs.tails_lane += es.tails_lane;
+            gs.tails_warp += es.tails_warp;
+            gs.busy_warp_ms += es.busy_warp_ms;
+            gs.idle_warp_ms += es.idle_warp_ms;
+        }
         if (stats) {
             stats->count += gs.count;
             stats->intersections += gs.intersections;

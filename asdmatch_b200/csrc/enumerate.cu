@@ -2029,28 +2029,24 @@ int run_plan(asdm_cs &cs, const asdm_plan &plan, const asdm_run_opts &opt, asdm_
 
 // Batched form: one persistent launch counts every query of a group.
 // counts[i] / status[i] receive each query's result.
-int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
-                    double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
-                    uint64_t *const *local_out, uint64_t *cycles, double query_time_s) {
+// Queries settled without enumeration, before any plan is needed: tree
+// queries counted by the tree program (in LOCAL mode the conflict-free ones,
+// with their local counts, a few queries at a time), then queries whose count
+// a device lower bound shows to be at least 2^64 (ASDM_ERR_OVERFLOW).  Only
+// queries with full[i] set (whole queries, not prefixes) take part.  live
+// holds the positions still open on entry and on return; counts and status of
+// the settled ones are written, their device time is added to agg->kernel_ms.
+int settle_queries(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<char> &full,
+                   std::vector<uint32_t> &live, uint64_t count_limit, uint64_t *counts, int *status,
+                   asdm_run_stats *agg, uint64_t *const *local_out) {
     cudaStream_t s = G->stream;
     const uint32_t Q = (uint32_t)cs.size();
-    std::vector<uint32_t> live;  // queries with a non-empty candidate space
-    for (uint32_t i = 0; i < Q; ++i) {
-        counts[i] = 0;
-        status[i] = ASDM_OK;
-        if (cycles) cycles[i] = 0;
-        if (cs[i]->nonempty) live.push_back(i);
-    }
-    if (agg) *agg = asdm_run_stats{};
     if (live.empty()) return ASDM_OK;
-    // tree queries are counted by the tree program (full plans only; prefix
-    // plans count partial matches); in LOCAL mode the conflict-free ones with
-    // their local counts, a few queries at a time
     float tree_ms = 0.f;
     if (local_out) {
         std::vector<uint32_t> tid;
         for (uint32_t i : live)
-            if (plans[i]->order.size() == cs[i]->q.n && tree_countable(cs[i]->q)) tid.push_back(i);
+            if (full[i] && tree_countable(cs[i]->q)) tid.push_back(i);
         std::vector<char> settled(Q, 0);
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
@@ -2114,7 +2110,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         std::vector<asdm_cs *> tcs;
         std::vector<uint32_t> tid;
         for (uint32_t i : live)
-            if (plans[i]->order.size() == cs[i]->q.n && tree_countable_conflicts(cs[i]->q)) {
+            if (full[i] && tree_countable_conflicts(cs[i]->q)) {
                 tcs.push_back(cs[i]);
                 tid.push_back(i);
             }
@@ -2156,7 +2152,7 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
         std::vector<asdm_cs *> ocs;
         std::vector<uint32_t> oid;
         for (uint32_t i : live)
-            if (plans[i]->order.size() == cs[i]->q.n) {
+            if (full[i]) {
                 ocs.push_back(cs[i]);
                 oid.push_back(i);
             }
@@ -2188,6 +2184,29 @@ int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::
             if (agg) agg->kernel_ms += bms;
             if (live.empty()) return ASDM_OK;
         }
+    }
+    return ASDM_OK;
+}
+
+int run_batch_count(asdm_graph *G, const std::vector<asdm_cs *> &cs, const std::vector<const asdm_plan *> &plans,
+                    double time_limit_s, uint64_t count_limit, uint64_t *counts, int *status, asdm_run_stats *agg,
+                    uint64_t *const *local_out, uint64_t *cycles, double query_time_s, bool settled) {
+    cudaStream_t s = G->stream;
+    const uint32_t Q = (uint32_t)cs.size();
+    std::vector<uint32_t> live;  // queries with a non-empty candidate space
+    for (uint32_t i = 0; i < Q; ++i) {
+        counts[i] = 0;
+        status[i] = ASDM_OK;
+        if (cycles) cycles[i] = 0;
+        if (cs[i]->nonempty) live.push_back(i);
+    }
+    if (agg) *agg = asdm_run_stats{};
+    if (live.empty()) return ASDM_OK;
+    if (!settled) {
+        std::vector<char> full(Q, 0);
+        for (uint32_t i = 0; i < Q; ++i) full[i] = plans[i]->order.size() == cs[i]->q.n;
+        ASDM_TRY(settle_queries(G, cs, full, live, count_limit, counts, status, agg, local_out));
+        if (live.empty()) return ASDM_OK;
     }
     const uint32_t L = (uint32_t)live.size();
     // host images of all plans, then one upload
