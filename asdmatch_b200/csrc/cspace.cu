@@ -45,6 +45,35 @@ __device__ __forceinline__ uint32_t find_segment(const uint64_t *__restrict__ pr
     return lo;
 }
 
+// The same for a warp whose lanes hold ascending items (item = base + lane;
+// lanes past the end pass valid = false, and every lane must call): the
+// warp's first item is located once, 32 probes per round, and only a lane
+// whose item lies past that segment searches on from there.  Segments here
+// are long (a query vertex's candidates), so most warps need one search.
+__device__ __forceinline__ uint32_t warp_find_segment(const uint64_t *__restrict__ prefix, uint32_t nseg,
+                                                      uint64_t base, uint64_t item, bool valid, uint32_t lane) {
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t p = lo + lane * step;
+        const uint32_t m = __ballot_sync(0xffffffffu, p < hi && prefix[p] <= base);
+        const uint32_t nlo = lo + (31 - __clz(m)) * step;
+        hi = min(hi, nlo + step);
+        lo = nlo;
+    }
+    const uint32_t p = lo + lane;
+    uint32_t s = lo + (31 - __clz(__ballot_sync(0xffffffffu, p < hi && prefix[p] <= base)));
+    if (valid && s + 1 < nseg && prefix[s + 1] <= item) {
+        uint32_t l2 = s + 1, h2 = nseg;
+        while (h2 - l2 > 1) {
+            const uint32_t mid = (l2 + h2) >> 1;
+            if (prefix[mid] <= item) l2 = mid; else h2 = mid;
+        }
+        s = l2;
+    }
+    return s;
+}
+
 // ---- K1: label + degree + NLC filter --------------------------------------
 // One segment per (query, query vertex) of a group; a segment's items are
 // the ranks 0 .. |V_l(u)| - 1 of u's label, padded to a multiple of 32 so
@@ -452,8 +481,8 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
         const uint64_t item = pos;
         uint32_t b = 0, e = 0;
         const uint2 *cm = nullptr;
+        const uint32_t ei = warp_find_segment(item_base, nedges, base, item, pos < total, lane);
         if (pos < total) {
-            const uint32_t ei = find_segment(item_base, nedges, item);
             const EdgeDesc d = edges[ei];
             if (rstart) {
                 b = rstart[item];
@@ -527,8 +556,8 @@ __global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint64_t item = base + lane;
         uint64_t len = 0;
+        const uint32_t ei = warp_find_segment(item_base, nedges, base, item, item < total, lane);
         if (item < total) {
-            const uint32_t ei = find_segment(item_base, nedges, item);
             s_cm[wid][lane] = edges[ei].cmem;
             len = cnt[item];
             s_rs[wid][lane] = rstart[item];
@@ -584,10 +613,12 @@ __global__ void __launch_bounds__(kBlock) k3_bound(DevGraph g, const EdgeDesc *_
                                                    uint32_t *__restrict__ ub,
                                                    uint32_t *__restrict__ rstart) {
     const uint64_t total = item_base[nedges];
-    for (uint64_t pos = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
-         pos += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t item = pos;
-        const uint32_t ei = find_segment(item_base, nedges, item);
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total;
+         base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t item = base + lane;
+        const uint32_t ei = warp_find_segment(item_base, nedges, base, item, item < total, lane);
+        if (item >= total) continue;
         const EdgeDesc d = edges[ei];
         const uint32_t i = (uint32_t)(item - item_base[ei]);
         uint32_t b = 0, e = 0;
@@ -614,8 +645,8 @@ __global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ u
         const uint64_t my = base + lane;
         const uint32_t c = my < nitems ? cnt[my] : 0u;
         const uint64_t from = my < nitems ? upos[my] : 0, to = my < nitems ? wpos[my] : 0;
+        const uint32_t ei = warp_find_segment(item_base, nedges, base, my, my < nitems, lane);
         if (my < nitems) {
-            const uint32_t ei = find_segment(item_base, nedges, my);
             const uint64_t first = item_base[ei];
             const uint64_t rel = to - wpos[first];
             if (rel > 0xFFFFFFFFull) atomicExch(bad, 1u);
@@ -638,8 +669,12 @@ __global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ u
 __global__ void k3_offsets(const uint64_t *__restrict__ item_base, uint32_t nedges, const uint64_t *__restrict__ wpos,
                            uint32_t *__restrict__ eoff, uint64_t *__restrict__ edge_start, uint32_t *__restrict__ bad) {
     const uint64_t total = item_base[nedges];
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t ei = find_segment(item_base, nedges, i);
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total;
+         base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = base + lane;
+        const uint32_t ei = warp_find_segment(item_base, nedges, base, i, i < total, lane);
+        if (i >= total) continue;
         const uint64_t rel = wpos[i] - wpos[item_base[ei]];
         if (rel > 0xFFFFFFFFull) atomicExch(bad, 1u);
         eoff[i] = (uint32_t)rel;

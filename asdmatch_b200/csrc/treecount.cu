@@ -870,12 +870,28 @@ __global__ void bound_level(const BoundSeg *__restrict__ segs, uint32_t nseg, un
         BoundSeg sg{};
         uint32_t i = 0;
         bool alive = valid;
-        if (valid) {
-            uint32_t lo = 0, hi = nseg;
+        // the segment of t (the last one starting at or before it): the warp's
+        // first item is located once, 32 probes per round; a lane whose item
+        // lies past that segment searches on from there
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 32) {
+            const uint32_t step = (hi - lo + 31) / 32;
+            const uint32_t p = lo + lane * step;
+            const uint32_t m = __ballot_sync(0xffffffffu, p < hi && segs[p].start <= base);
+            const uint32_t nlo = lo + (31 - __clz(m)) * step;
+            hi = min(hi, nlo + step);
+            lo = nlo;
+        }
+        lo += 31 - __clz(__ballot_sync(0xffffffffu, lo + lane < hi && segs[lo + lane].start <= base));
+        if (valid && lo + 1 < nseg && segs[lo + 1].start <= t) {
+            hi = nseg;
+            ++lo;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
                 if (segs[mid].start <= t) lo = mid; else hi = mid;
             }
+        }
+        if (valid) {
             sg = segs[lo];
             i = (uint32_t)(t - sg.start);
             if (sg.cls_k > 1) alive = vertex_class(sg.cand[i], sg.cls_k) == sg.cls_c;
