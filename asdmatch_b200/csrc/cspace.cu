@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(kBlock) k3_edges(DevGraph g, const EdgeDesc *_
 // in flight whatever the run lengths.  In: cnt = run lengths, rstart = run
 // starts (k3_bound), upos = padded positions; out: each item's hits packed in
 // order at the front of its padded region, cnt = their number.
-__global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__restrict__ edges,
+__global__ void __launch_bounds__(kBlock, 6) k3_flat(DevGraph g, const EdgeDesc *__restrict__ edges,
                                                   const uint64_t *__restrict__ item_base, uint32_t nedges,
                                                   uint32_t *__restrict__ cnt, const uint64_t *__restrict__ upos,
                                                   const uint32_t *__restrict__ rstart, uint32_t *__restrict__ padded,
@@ -575,20 +575,21 @@ __global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__
         __syncwarp();
         const uint64_t S = s_pre[wid][32];
         scanned += S;
-        for (uint64_t j0 = 0; j0 < S; j0 += 32) {
-            const uint64_t j = j0 + lane;
-            const bool valid = j < S;
-            // owner: the last item whose run starts at or before j (empty
-            // runs share their start with the next item and come first)
+        // owner of entry j: the last item whose run starts at or before j
+        // (empty runs share their start with the next item and come first)
+        auto owner = [&](uint64_t j) {
             uint32_t lo = 0, hi = 32;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
                 if (s_pre[wid][mid] <= j) lo = mid; else hi = mid;
             }
-            const uint32_t it = lo;
-            const uint64_t first = s_pre[wid][it];
-            uint32_t idx = kNone;
-            if (valid) idx = cand_index(s_cm[wid][it], g.nbr_rank[s_rs[wid][it] + (uint32_t)(j - first)]);
+            return lo;
+        };
+        // one round's hits of the entries j0 .. j0+31 (idx = kNone for a miss)
+        // packed behind their item's earlier hits
+        auto emit = [&](uint64_t j0, uint32_t it, uint64_t first, uint32_t idx) {
+            const uint64_t j = j0 + lane;
+            const bool valid = j < S;
             const uint32_t mask = __ballot_sync(0xffffffffu, idx != kNone);
             // the item's lanes in this round are contiguous, from lane f
             const uint32_t f = first > j0 ? (uint32_t)(first - j0) : 0u;
@@ -600,6 +601,20 @@ __global__ void __launch_bounds__(kBlock) k3_flat(DevGraph g, const EdgeDesc *__
             __syncwarp();
             if (last) s_hits[wid][it] = done + __popc(mine & ((2u << lane) - 1u));
             __syncwarp();
+        };
+        // two rounds at a time: both rounds' rank and membership loads are in
+        // flight together (the rounds' outputs are packed in order after)
+        for (uint64_t j0 = 0; j0 < S; j0 += 64) {
+            const uint64_t ja = j0 + lane, jb = ja + 32;
+            const bool va = ja < S, vb = jb < S;
+            const uint32_t ita = owner(ja), itb = owner(jb);
+            const uint64_t fa = s_pre[wid][ita], fb = s_pre[wid][itb];
+            const uint32_t ra = va ? g.nbr_rank[s_rs[wid][ita] + (uint32_t)(ja - fa)] : 0u;
+            const uint32_t rb = vb ? g.nbr_rank[s_rs[wid][itb] + (uint32_t)(jb - fb)] : 0u;
+            const uint32_t xa = va ? cand_index(s_cm[wid][ita], ra) : kNone;
+            const uint32_t xb = vb ? cand_index(s_cm[wid][itb], rb) : kNone;
+            emit(j0, ita, fa, xa);
+            if (j0 + 32 < S) emit(j0 + 32, itb, fb, xb);
         }
         if (item < total) cnt[item] = s_hits[wid][lane];
         __syncwarp();
