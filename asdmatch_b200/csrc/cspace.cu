@@ -668,15 +668,28 @@ __global__ void __launch_bounds__(kBlock) k3_pack(const uint64_t *__restrict__ u
             cnt[my] = (uint32_t)rel;
             if (my == first) edge_start[ei] = to;
         }
-        if (c <= kLongRun)
-            for (uint32_t k = 0; k < c; ++k) elist[to + k] = padded[from + k];
-        uint32_t todo = __ballot_sync(0xffffffffu, c > kLongRun);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t cc = __shfl_sync(0xffffffffu, c, src);
-            const uint64_t f = __shfl_sync(0xffffffffu, from, src), t = __shfl_sync(0xffffffffu, to, src);
-            for (uint32_t k = lane; k < cc; k += 32) elist[t + k] = padded[f + k];
+        // the 32 items' dense lists are one contiguous range from lane 0's
+        // position: the warp copies it a lane per entry (coalesced stores),
+        // each entry read from its owner item's padded list
+        uint64_t pre = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= (uint32_t)o) pre += y;
+        }
+        const uint64_t total = __shfl_sync(0xffffffffu, pre, 31), to0 = __shfl_sync(0xffffffffu, to, 0);
+        for (uint64_t t0 = 0; t0 < total; t0 += 32) {
+            const uint64_t t = t0 + lane;
+            // owner: the first lane whose inclusive prefix passes t
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step; step >>= 1) {
+                const uint64_t v = __shfl_sync(0xffffffffu, pre, o + step - 1);
+                if (v <= t) o += step;
+            }
+            const uint64_t f = __shfl_sync(0xffffffffu, from, o);
+            const uint64_t ex = __shfl_sync(0xffffffffu, pre - c, o);
+            if (t < total) elist[to0 + t] = padded[f + (t - ex)];
         }
     }
 }
