@@ -143,3 +143,32 @@ def test_oracle_tree_bound_is_the_count_without_far_pairs(golden, c0_files, tmp_
         assert int(v) == rec["count"], (rec["index"], v, rec["count"])
         equal += 1
     assert equal >= 40, (equal, len(recs))
+
+
+def test_oracle_matches_reference_on_the_config4_graph(tmp_path):
+    """At the config-4 graph's full size (1M vertices, 10M edges): the oracle's
+    local-count CSVs and sorted embedding dumps equal the reference's
+    (tests/golden/c4_batch.json, made with oracle/_ref) on the smallest
+    finished queries of the parity and embed sets."""
+    import json
+    from asdmatch_b200 import workloads as W
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c4_batch.json")) as fh:
+        data = json.load(fh)
+    g = W.graph(W.C4)
+    dpath = str(tmp_path / "data.graph")
+    g.write(dpath)
+    specs = W.c4_parity_specs()
+    parity = sorted((r for r in data["parity"] if r["count"] is not None), key=lambda r: r["count"])[:2]
+    embed = sorted((r for r in data["embed"] if r["count"] is not None), key=lambda r: r["count"])[:2]
+    for r in parity:
+        qpath = str(tmp_path / "p.graph")
+        W.from_specs(g, [specs[r["index"]]])[0].write(qpath)
+        csv = str(tmp_path / "l.csv")
+        count, _ = O.oracle_run(qpath, dpath, O.MODE_LOCAL, csv=csv)
+        assert count == r["count"] and O.sha256_file(csv) == r["csv_sha256"], r["index"]
+    for r in embed:
+        qpath = str(tmp_path / "e.graph")
+        W.from_specs(g, [(r["size"], r["seed"], r["density"])])[0].write(qpath)
+        emb = str(tmp_path / "e.txt")
+        count, _ = O.oracle_run(qpath, dpath, O.MODE_EMBED, emb=emb)
+        assert count == r["count"] and O.sha256_file(emb) == r["emb_sha256"], r["index"]
