@@ -172,3 +172,23 @@ def test_oracle_matches_reference_on_the_config4_graph(tmp_path):
         emb = str(tmp_path / "e.txt")
         count, _ = O.oracle_run(qpath, dpath, O.MODE_EMBED, emb=emb)
         assert count == r["count"] and O.sha256_file(emb) == r["emb_sha256"], r["index"]
+
+
+def test_oracle_counts_match_reference_on_the_config1_graph(tmp_path):
+    """At the config-1 graph's full size (3.77M vertices, 16.5M edges): the
+    oracle's backtracking count equals the reference's (tests/golden/c2_batch.json,
+    made with oracle/_ref) on the two config-2 queries with the smallest
+    reference counts, one of them outside the tree program's reach."""
+    import json
+    from asdmatch_b200 import workloads as W
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_batch.json")) as fh:
+        data = json.load(fh)
+    recs = sorted((r for r in data["queries"] if r.get("count") is not None), key=lambda r: r["count"])[:2]
+    g = W.graph(W.C1)
+    dpath = str(tmp_path / "data.graph")
+    g.write(dpath)
+    for r in recs:
+        qpath = str(tmp_path / "q.graph")
+        W.c2_candidate(g, r["index"])[2].write(qpath)
+        count, _ = O.oracle_run(qpath, dpath, O.MODE_COUNT)
+        assert count == r["count"], r["index"]
